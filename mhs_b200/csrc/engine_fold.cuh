@@ -1,0 +1,428 @@
+// The folded image of a source whose smeared slip reaches above z = 0
+// (mhs/kernels/fold.py): at receivers in a band below the surface the lifted
+// Mindlin image is replaced by the mirror element's full-space field plus the
+// Boussinesq field of the pair's normal surface traction, integrated on a
+// polar grid centred under the receiver.
+//
+// The grid is rebuilt here from the same rules (radial breaks, composite
+// Gauss panels, angular sectors) so the quadrature nodes are the same nodes.
+#pragma once
+
+#include "engine_kernels.cuh"
+
+namespace mhs {
+
+// Mirror element's slip columns (fold.py:79).
+MHS_FI double mirror_slip_sign(int m) { return m == 2 ? 1.0 : -1.0; }
+
+// Source folded when its shallowest vertex is within FOLD_SOURCE_DEPTH_EPS eps
+// of the surface (fold.py:84-87).
+MHS_FI bool fold_straddles(const double* tri, double eps) {
+  double zmax = tri[2];
+  if (tri[5] > zmax) zmax = tri[5];
+  if (tri[8] > zmax) zmax = tri[8];
+  return -zmax < cst::FOLD_SOURCE_DEPTH_EPS * eps;
+}
+
+// Surface disk holding the source's sharp features: centre and radius
+// (fold.py:95-107).
+MHS_HD void fold_crease(const double* tri, double eps, double* centre, double* radius) {
+  double dep[3];
+  for (int i = 0; i < 3; ++i) dep[i] = -tri[3 * i + 2];
+  bool top[3];
+  int nt = 0;
+  for (int i = 0; i < 3; ++i) {
+    top[i] = dep[i] < cst::FOLD_SOURCE_DEPTH_EPS * eps;
+    nt += top[i];
+  }
+  if (nt == 0) {
+    double dmin = dep[0];
+    for (int i = 1; i < 3; ++i)
+      if (dep[i] < dmin) dmin = dep[i];
+    for (int i = 0; i < 3; ++i) {
+      top[i] = dep[i] == dmin;
+      nt += top[i];
+    }
+  }
+  double cx = 0.0, cy = 0.0;
+  for (int i = 0; i < 3; ++i)
+    if (top[i]) {
+      cx += tri[3 * i];
+      cy += tri[3 * i + 1];
+    }
+  cx /= nt;
+  cy /= nt;
+  double spread = 0.0, dtop = -INFINITY;
+  for (int i = 0; i < 3; ++i)
+    if (top[i]) {
+      const double dx = tri[3 * i] - cx, dy = tri[3 * i + 1] - cy;
+      const double r = sqrt(dx * dx + dy * dy);
+      if (r > spread) spread = r;
+      if (dep[i] > dtop) dtop = dep[i];
+    }
+  centre[0] = cx;
+  centre[1] = cy;
+  *radius = (spread + cst::FOLD_CREASE_MARGIN_EPS * eps) + dtop;
+}
+
+// Receiver takes the folded image of this source (fold.py:110-118).
+MHS_FI bool fold_band(const double* x, const double* centre, double eps) {
+  const double depth = -x[2];
+  const double reach = hypot(x[0] - centre[0], x[1] - centre[1]);
+  return depth < cst::FOLD_BAND_DEPTH_EPS * eps && reach < cst::FOLD_REACH_EPS * eps;
+}
+
+// Largest vertex-to-vertex distance (fold.py:344-345).
+MHS_HD double tri_diameter(const double* tri) {
+  double d = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double a = tri[3 * i] - tri[3 * j], b = tri[3 * i + 1] - tri[3 * j + 1],
+                   c = tri[3 * i + 2] - tri[3 * j + 2];
+      const double r = sqrt(a * a + b * b + c * c);
+      if (r > d) d = r;
+    }
+  return d;
+}
+
+// ------------------------------------------------ Boussinesq point load
+// Unit normal point load on the surface of the body z <= 0: stress (6
+// unique components xx, yy, zz, xy, xz, yz) at depth zeta and offset
+// (dx, dy) = receiver - load (fold.py:132-166).
+MHS_HD void point_stress6(double dx, double dy, double zeta, double nu, double* S) {
+  const double r2 = dx * dx + dy * dy;
+  const double rho = sqrt(r2 + zeta * zeta);
+  const double rho3 = rho * rho * rho;
+  const double rho5 = rho3 * rho * rho;
+  const double a = 1.0 / (rho * (rho + zeta));
+  const double c = 1.0 - 2.0 * nu;
+  const double s_th = c * (-a + zeta / rho3);
+  const double s_r_th = 2.0 * c * a - 3.0 * zeta * r2 / rho5 - c * zeta / rho3;
+  const double r = sqrt(r2);
+  const double ex = r > 0.0 ? dx / r : 0.0, ey = r > 0.0 ? dy / r : 0.0;
+  const double pref = 1.0 / (2.0 * cst::PI);
+  S[0] = pref * (s_th + s_r_th * ex * ex);
+  S[1] = pref * (s_th + s_r_th * ey * ey);
+  S[2] = -pref * 3.0 * (zeta * zeta * zeta) / rho5;
+  S[3] = pref * s_r_th * ex * ey;
+  const double t_rz = pref * 3.0 * r * zeta * zeta / rho5;
+  S[4] = t_rz * ex;
+  S[5] = t_rz * ey;
+}
+
+MHS_HD void point_disp3(double dx, double dy, double zeta, double mu, double nu, double* u) {
+  const double r2 = dx * dx + dy * dy;
+  const double rho = sqrt(r2 + zeta * zeta);
+  const double rho3 = rho * rho * rho;
+  const double pref = 1.0 / (4.0 * cst::PI * mu);
+  const double ur = pref * (zeta / rho3 - (1.0 - 2.0 * nu) / (rho * (rho + zeta)));
+  u[0] = ur * dx;
+  u[1] = ur * dy;
+  u[2] = -pref * (2.0 * (1.0 - nu) / rho + zeta * zeta / rho3);
+}
+
+// Love's on-axis field of unit pressure over a disk of radius a
+// (fold.py:185-210): diag(srr, srr, szz) and the vertical displacement.
+MHS_HD void disk_stress(double a, double zeta, double nu, double* srr, double* szz) {
+  const double rho = sqrt(a * a + zeta * zeta);
+  const double z3 = (zeta * zeta * zeta) / (rho * rho * rho);
+  *szz = -(1.0 - z3);
+  *srr = -0.5 * ((1.0 + 2.0 * nu) - 2.0 * (1.0 + nu) * zeta / rho + z3);
+}
+
+MHS_HD double disk_disp_z(double a, double zeta, double mu, double nu) {
+  const double rho = sqrt(a * a + zeta * zeta);
+  return -(0.5 / mu) * (2.0 * (1.0 - nu) * (rho - zeta) + zeta - zeta * zeta / rho);
+}
+
+// ---------------------------------------------------------- polar grid
+constexpr int FOLD_MAX_BREAKS = 192;
+
+// numpy.linspace(a, b, num)[i]: i * step + a, the last point exactly b.
+MHS_FI double linspace_at(double a, double b, int num, int i) {
+  if (i == num - 1) return b;
+  const double step = (b - a) / (double)(num - 1);
+#if defined(__CUDA_ARCH__)
+  return __dadd_rn(__dmul_rn((double)i, step), a);
+#else
+  return (double)i * step + a;
+#endif
+}
+
+// One-sided angular half-width of the circles r in [ra, rb] inside the disk
+// of `radius` about the crease centre at distance rho_s (fold.py:251-258).
+MHS_HD double fold_halfwidth(double ra, double rb, double rho_s, double radius) {
+  if (rb < rho_s - radius || ra > rho_s + radius) return 0.0;
+  if (rho_s <= radius) return cst::PI;
+  double q = radius / rho_s;
+  if (q > 1.0) q = 1.0;
+  return asin(q);
+}
+
+// Angular rule of one radial panel: up to four linspace pieces, each
+// composite 4-point Gauss over its intervals (fold.py:261-287).
+struct AngRule {
+  int npiece;
+  double a[4], b[4];
+  int m[4];        // intervals per piece
+  int n;           // total nodes = FOLD_N_ANGULAR * sum(m)
+};
+
+MHS_HD void fold_angular(double theta_c, double w_fine, double w_med, double rb, double eps,
+                         AngRule& A) {
+  const int n = cst::FOLD_N_ANGULAR;
+  const double two_pi = 2.0 * cst::PI;
+  A.npiece = 0;
+  A.n = 0;
+  if (w_fine >= cst::PI || w_med >= cst::PI) {
+    const double sp = w_fine >= cst::PI ? cst::FOLD_FINE_SPACING_EPS : cst::FOLD_MEDIUM_SPACING_EPS;
+    int m = (int)ceil(two_pi * rb / ((double)n * sp * eps));
+    if (m < 8) m = 8;
+    A.a[0] = 0.0;
+    A.b[0] = two_pi;
+    A.m[0] = m;
+    A.npiece = 1;
+    A.n = n * m;
+    return;
+  }
+  double pa[4], pb[4];
+  int pm[4], np = 0;
+  int mid_first = -1;
+  if (w_fine > 0.0) {
+    int m = (int)ceil(2.0 * w_fine * rb / ((double)n * cst::FOLD_FINE_SPACING_EPS * eps));
+    if (m < 1) m = 1;
+    pa[np] = theta_c - w_fine;
+    pb[np] = theta_c + w_fine;
+    pm[np] = m;
+    mid_first = np;
+    ++np;
+  }
+  if (w_med > w_fine) {
+    int m = (int)ceil((w_med - w_fine) * rb / ((double)n * cst::FOLD_MEDIUM_SPACING_EPS * eps));
+    if (m < 1) m = 1;
+    // insert the left flank before the fine sector, append the right one
+    for (int i = np; i > 0; --i) {
+      pa[i] = pa[i - 1];
+      pb[i] = pb[i - 1];
+      pm[i] = pm[i - 1];
+    }
+    pa[0] = theta_c - w_med;
+    pb[0] = theta_c - w_fine;
+    pm[0] = m;
+    ++np;
+    pa[np] = theta_c + w_fine;
+    pb[np] = theta_c + w_med;
+    pm[np] = m;
+    ++np;
+  }
+  (void)mid_first;
+  const double start = w_med > 0.0 ? theta_c + w_med : 0.0;
+  pa[np] = start;
+  pb[np] = (start + two_pi) - 2.0 * w_med;
+  pm[np] = imax(1, cst::FOLD_N_COARSE / n);
+  ++np;
+  for (int i = 0; i < np; ++i) {
+    // a piece is used when its last break lies beyond its first
+    if (!(pb[i] > pa[i])) continue;
+    A.a[A.npiece] = pa[i];
+    A.b[A.npiece] = pb[i];
+    A.m[A.npiece] = pm[i];
+    A.n += n * pm[i];
+    ++A.npiece;
+  }
+}
+
+// Sorted, de-duplicated radial breaks of the polar grid about the receiver
+// foot (fold.py:290-318).  Returns the count (or -1 past FOLD_MAX_BREAKS)
+// and R1, the grid's outer radius.
+MHS_HD int fold_breaks(double rho_s, double zeta, double r_f, double eps, double diam,
+                       double* br, double* R1out) {
+  double geo[64];
+  int ng = 0;
+  geo[ng++] = 0.0;
+  if (0.0 < zeta && zeta < 0.5 * eps) {
+    const double zs[4] = {0.5 * zeta, zeta, 2.0 * zeta, 4.0 * zeta};
+    for (int i = 0; i < 4; ++i)
+      if (zs[i] < 0.5 * eps) geo[ng++] = zs[i];
+  }
+  const double r1_target = (rho_s + 4.0 * r_f) + cst::FOLD_R1_MARGIN_DIAM * diam;
+  double r = 0.5 * eps;
+  while (true) {
+    if (ng >= 64) return -1;
+    geo[ng++] = r;
+    if (r >= r1_target) break;
+    r *= 2.0;
+  }
+  const double R1 = geo[ng - 1];
+  const double lo_m = rho_s - 4.0 * r_f, hi_m = rho_s + 4.0 * r_f;
+  const double lo_f = rho_s - r_f, hi_f = rho_s + r_f;
+  int nb = 0;
+  for (int i = 0; i < ng; ++i)
+    if (geo[i] < lo_m || geo[i] > hi_m) br[nb++] = geo[i];
+  const double a0s[3] = {lo_m > 0.0 ? lo_m : 0.0, lo_f > 0.0 ? lo_f : 0.0, hi_f < R1 ? hi_f : R1};
+  const double b0s[3] = {lo_f > 0.0 ? lo_f : 0.0, hi_f < R1 ? hi_f : R1, hi_m < R1 ? hi_m : R1};
+  const double ws[3] = {cst::FOLD_MEDIUM_SUBPANEL_EPS, cst::FOLD_FINE_SUBPANEL_EPS,
+                        cst::FOLD_MEDIUM_SUBPANEL_EPS};
+  for (int s = 0; s < 3; ++s) {
+    const double a0 = a0s[s], b0 = b0s[s];
+    if (!(b0 > a0)) continue;
+    int m = (int)ceil((b0 - a0) / (ws[s] * eps));
+    if (m < 1) m = 1;
+    if (nb + m + 1 > FOLD_MAX_BREAKS) return -1;
+    for (int i = 0; i <= m; ++i) br[nb++] = linspace_at(a0, b0, m + 1, i);
+  }
+  // sort (insertion) and drop exact duplicates
+  for (int i = 1; i < nb; ++i) {
+    const double v = br[i];
+    int j = i - 1;
+    while (j >= 0 && br[j] > v) {
+      br[j + 1] = br[j];
+      --j;
+    }
+    br[j + 1] = v;
+  }
+  int nu = 0;
+  const double cap = R1 + 1e-12 * R1;
+  for (int i = 0; i < nb; ++i) {
+    if (nu > 0 && br[i] == br[nu - 1]) continue;
+    if (!(br[i] <= cap)) continue;
+    br[nu++] = br[i];
+  }
+  *R1out = R1;
+  return nu;
+}
+
+// Everything a band pair's grid walk needs besides the breaks.
+struct FoldPair {
+  double xh0, xh1, zeta;    // receiver foot and depth
+  double rho_s, theta_c;    // crease centre seen from the foot
+  double r_f, eps, R1;
+};
+
+MHS_HD void fold_pair_setup(const double* x, const double* centre, double r_f, double eps,
+                            FoldPair& fp) {
+  fp.xh0 = x[0];
+  fp.xh1 = x[1];
+  fp.zeta = -x[2] > 0.0 ? -x[2] : 0.0;
+  const double cx = centre[0] - x[0], cy = centre[1] - x[1];
+  fp.rho_s = hypot(cx, cy);
+  fp.theta_c = atan2(cy, cx);
+  fp.r_f = r_f;
+  fp.eps = eps;
+}
+
+// Angular rule of panel [ra, rb].
+MHS_FI void fold_panel_rule(const FoldPair& fp, double ra, double rb, AngRule& A) {
+  fold_angular(fp.theta_c, fold_halfwidth(ra, rb, fp.rho_s, fp.r_f),
+               fold_halfwidth(ra, rb, fp.rho_s, 4.0 * fp.r_f), rb, fp.eps, A);
+}
+
+// Node j (0 <= j < A.n) of an angular rule: angle and weight.
+MHS_HD void fold_ang_node(const AngRule& A, const double* glx4, const double* glw4, int j,
+                          double* theta, double* wt) {
+  int p = 0;
+  while (j >= cst::FOLD_N_ANGULAR * A.m[p]) {
+    j -= cst::FOLD_N_ANGULAR * A.m[p];
+    ++p;
+  }
+  const int iv = j / cst::FOLD_N_ANGULAR, nd = j % cst::FOLD_N_ANGULAR;
+  const double a = linspace_at(A.a[p], A.b[p], A.m[p] + 1, iv);
+  const double b = linspace_at(A.a[p], A.b[p], A.m[p] + 1, iv + 1);
+  const double u = 0.5 * (glx4[nd] + 1.0), wu = 0.5 * glw4[nd];
+  *theta = a + (b - a) * u;
+  *wt = (b - a) * wu;
+}
+
+// Surface load at horizontal point (px, py): twice the element's elastic
+// sigma_zz on z = 0 per node and slip component (fold.py:214-228).
+template <int P>
+MHS_HD void fold_surface_load(const Frame& f, const QuadRule& r12, const QuadRule& r8, double px,
+                              double py, double eps, const Material& m, double* s /*K x 3*/) {
+  constexpr int K = n_nodes(P);
+  double H[K * 27], E[K];
+  const double x[3] = {px, py, 0.0};
+  direct_eval<P, W_H | W_E>(f, r12, r8, x, eps, m, nullptr, H, E);
+  double ezz[3];
+  for (int j = 0; j < 3; ++j) ezz[j] = m.lam * f.n[j] + (j == 2 ? 2.0 * m.mu * f.n[2] : 0.0);
+  for (int k = 0; k < K; ++k)
+    for (int j = 0; j < 3; ++j) s[3 * k + j] = 2.0 * (H[27 * k + 9 * 2 + 3 * 2 + j] - E[k] * ezz[j]);
+}
+
+// Scalar reference walk of one band pair's Boussinesq correction, for the
+// host test build and for small launches: H[k][a][b][m] (WANT_H) or
+// U[k][i][m].  Returns 0, or -1 if the grid overflowed its capacity.
+template <int P, bool WANT_H>
+MHS_HD int fold_boussinesq_scalar(const Frame& f, const QuadRule& r12, const QuadRule& r8,
+                                  const double* tri, const double* x, double eps,
+                                  const Material& m, const double* glx, const double* glw,
+                                  double* out) {
+  constexpr int K = n_nodes(P);
+  double centre[2], r_f;
+  fold_crease(tri, eps, centre, &r_f);
+  const double diam = tri_diameter(tri);
+  FoldPair fp;
+  fold_pair_setup(x, centre, r_f, eps, fp);
+  double br[FOLD_MAX_BREAKS];
+  const int nb = fold_breaks(fp.rho_s, fp.zeta, r_f, eps, diam, br, &fp.R1);
+  if (nb < 0) return -1;
+  double sh[3 * K];
+  fold_surface_load<P>(f, r12, r8, x[0], x[1], eps, m, sh);
+  const double* gx6 = glx + gl_offset(cst::FOLD_N_RADIAL);
+  const double* gw6 = glw + gl_offset(cst::FOLD_N_RADIAL);
+  const double* gx4 = glx + gl_offset(cst::FOLD_N_ANGULAR);
+  const double* gw4 = glw + gl_offset(cst::FOLD_N_ANGULAR);
+  constexpr int NC = WANT_H ? 6 : 3;
+  double acc[NC][3 * K];
+  for (int c = 0; c < NC; ++c)
+    for (int j = 0; j < 3 * K; ++j) acc[c][j] = 0.0;
+  for (int pi = 0; pi + 1 < nb; ++pi) {
+    const double ra = br[pi], rb = br[pi + 1];
+    if (rb - ra < 1e-9 * eps) continue;
+    AngRule A;
+    fold_panel_rule(fp, ra, rb, A);
+    for (int ir = 0; ir < cst::FOLD_N_RADIAL; ++ir) {
+      const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
+      const double wr = (rb - ra) * (0.5 * gw6[ir]);
+      for (int j = 0; j < A.n; ++j) {
+        double th, wt;
+        fold_ang_node(A, gx4, gw4, j, &th, &wt);
+        const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
+        const double w = wr * wt * R;
+        double s[3 * K];
+        fold_surface_load<P>(f, r12, r8, px, py, eps, m, s);
+        double B[NC];
+        if (WANT_H) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, B);
+        else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, B);
+        for (int c = 0; c < NC; ++c)
+          for (int jj = 0; jj < 3 * K; ++jj) acc[c][jj] += (w * B[c]) * (s[jj] - sh[jj]);
+      }
+    }
+  }
+  if (WANT_H) {
+    double srr, szz;
+    disk_stress(fp.R1, fp.zeta, m.nu_f, &srr, &szz);
+    const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    for (int k = 0; k < K; ++k)
+      for (int mm = 0; mm < 3; ++mm) {
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) out[27 * k + 9 * a + 3 * b + mm] = 0.0;
+        for (int c = 0; c < 6; ++c) {
+          const double v = acc[c][3 * k + mm];
+          out[27 * k + 9 * ia[c] + 3 * ib[c] + mm] = v;
+          out[27 * k + 9 * ib[c] + 3 * ia[c] + mm] = v;
+        }
+        out[27 * k + 9 * 0 + 3 * 0 + mm] += sh[3 * k + mm] * srr;
+        out[27 * k + 9 * 1 + 3 * 1 + mm] += sh[3 * k + mm] * srr;
+        out[27 * k + 9 * 2 + 3 * 2 + mm] += sh[3 * k + mm] * szz;
+      }
+  } else {
+    const double uz = disk_disp_z(fp.R1, fp.zeta, m.mu, m.nu_f);
+    for (int k = 0; k < K; ++k)
+      for (int mm = 0; mm < 3; ++mm)
+        for (int i = 0; i < 3; ++i)
+          out[9 * k + 3 * i + mm] = acc[i][3 * k + mm] + (i == 2 ? sh[3 * k + mm] * uz : 0.0);
+  }
+  return 0;
+}
+
+}  // namespace mhs

@@ -1,0 +1,528 @@
+// Per-(observer, source) influence tensors from the weighted moment tables:
+// the direct full-space Kelvin-Cortez kernels U / H / E, the half-space image
+// R-family (closed form on the reflected element) and Q-family (per-observer
+// Gauss quadrature).  Output layouts, per node k:
+//   U[k][i][j]     displacement i from unit Cartesian slip j
+//   H[k][a][b][j]  total stress (a, b) from unit Cartesian slip j
+//   E[k]           blob weight of the eigenstress
+#pragma once
+
+#include "engine_moments.cuh"
+
+namespace mhs {
+
+enum : int { W_U = 1, W_H = 2, W_E = 4 };
+
+// Spec of the direct term for a readout mask.
+template <int P, int WANT> struct DirectSpec {
+  static constexpr Spec spec = (WANT & W_U) ? SpecU<P>::spec
+                               : (WANT & W_H) ? SpecH<P>::spec
+                                              : SpecE<P>::spec;
+};
+
+// Component of a rank-r moment tensor in the element's own frame (basis
+// e1, e2, nhat): with (ca, cb, cc) the counts of each basis index the lift
+// (mhs/fullspace/kernels.py:90-123) reduces to one table entry,
+// (-1)^(ca+cb) z^cc W_n(ca, cb).
+template <class S>
+MHS_FI double lift_local(const double* W, int s, int ca, int cb, int cc, const double* zp) {
+  const double v = zp[cc] * W[S::spec.w_off[s] + tri_idx(ca, cb)];
+  return ((ca + cb) & 1) ? -v : v;
+}
+
+// Rotate a rank-2 tensor from the local frame: out[a][b] = R[a][x] R[b][y] in[x][y],
+// R[a][x] = basis_x[a].
+MHS_HD void rotate2(const Frame& f, const double in[3][3], double* out) {
+  const double* B[3] = {f.e1, f.e2, f.n};
+  double t[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int y = 0; y < 3; ++y) t[a][y] = B[0][a] * in[0][y] + B[1][a] * in[1][y] + B[2][a] * in[2][y];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) out[3 * a + b] = t[a][0] * B[0][b] + t[a][1] * B[1][b] + t[a][2] * B[2][b];
+}
+
+MHS_HD void rotate3(const Frame& f, const double in[3][3][3], double* out) {
+  const double* B[3] = {f.e1, f.e2, f.n};
+  double t1[3][3][3], t2[3][3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int y = 0; y < 3; ++y)
+      for (int z = 0; z < 3; ++z)
+        t1[a][y][z] = B[0][a] * in[0][y][z] + B[1][a] * in[1][y][z] + B[2][a] * in[2][y][z];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int z = 0; z < 3; ++z)
+        t2[a][b][z] = t1[a][0][z] * B[0][b] + t1[a][1][z] * B[1][b] + t1[a][2][z] * B[2][b];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int c = 0; c < 3; ++c)
+        out[9 * a + 3 * b + c] = t2[a][b][0] * B[0][c] + t2[a][b][1] * B[1][c] + t2[a][b][2] * B[2][c];
+}
+
+// Slip -> displacement (mhs/fullspace/kernels.py:148-163), evaluated in the
+// element frame where the normal is e3, then rotated.
+template <class S>
+MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, const Material& m,
+                     double* U) {
+  double zp[4] = {1.0, z, z * z, z * z * z};
+  const int s3 = nslot(3), s5 = nslot(5);
+  const double V3[3] = {-W[S::spec.w_off[s3] + tri_idx(1, 0)], -W[S::spec.w_off[s3] + tri_idx(0, 1)],
+                        z * W[S::spec.w_off[s3]]};
+  const double V5[3] = {-W[S::spec.w_off[s5] + tri_idx(1, 0)], -W[S::spec.w_off[s5] + tri_idx(0, 1)],
+                        z * W[S::spec.w_off[s5]]};
+  const double e2 = eps * eps;
+  const double f6 = 6.0 * m.one_m_nu * e2;
+  double G1[3][3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) {
+        const int ca = (i == 0) + (j == 0) + (k == 0), cb = (i == 1) + (j == 1) + (k == 1);
+        const double T = lift_local<S>(W, s5, ca, cb, 3 - ca - cb, zp);
+        double g = (i == j ? -m.c34 * V3[k] : 0.0);
+        g = g + (i == k ? V3[j] : 0.0);
+        g = g + (j == k ? V3[i] : 0.0);
+        g = g - 3.0 * T;
+        g = g - (i == j ? f6 * V5[k] : 0.0);
+        G1[i][j][k] = g * m.C1;
+      }
+  double Ul[3][3];
+  for (int i = 0; i < 3; ++i) {
+    const double tr = G1[i][0][0] + G1[i][1][1] + G1[i][2][2];
+    for (int j = 0; j < 3; ++j)
+      Ul[i][j] = -(m.mu * G1[i][j][2] + (j == 2 ? m.lam_d * tr : 0.0) + m.mu * G1[i][2][j]);
+  }
+  rotate2(f, Ul, U);
+}
+
+// Slip -> total stress (mhs/fullspace/kernels.py:182-210), in the element frame.
+template <class S>
+MHS_HD void kernel_H(const Frame& f, const double* W, double z, double eps, const Material& m,
+                     double* H) {
+  double zp[5] = {1.0, z, z * z, z * z * z, z * z * z * z};
+  const int s3 = nslot(3), s5 = nslot(5), s7 = nslot(7);
+  const double I3 = W[S::spec.w_off[s3]];
+  const double I5 = W[S::spec.w_off[s5]];
+  const double e2 = eps * eps;
+  const double f2 = 2.0 * m.one_m_nu * e2;
+  double T25[3][3], T27[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const int ca = (i == 0) + (j == 0), cb = (i == 1) + (j == 1);
+      T25[i][j] = lift_local<S>(W, s5, ca, cb, 2 - ca - cb, zp);
+      T27[i][j] = lift_local<S>(W, s7, ca, cb, 2 - ca - cb, zp);
+    }
+  // D2[r][p][s][q] / C1
+  double D2[3][3][3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int p = 0; p < 3; ++p)
+      for (int s = 0; s < 3; ++s)
+        for (int q = 0; q < 3; ++q) {
+          const double drp = r == p, dsq = s == q, drs = r == s, dpq = p == q, dps = p == s,
+                       drq = r == q;
+          const int ca = (r == 0) + (p == 0) + (s == 0) + (q == 0);
+          const int cb = (r == 1) + (p == 1) + (s == 1) + (q == 1);
+          const double T47 = lift_local<S>(W, s7, ca, cb, 4 - ca - cb, zp);
+          double d = -m.c34 * (drp * dsq * I3 - 3.0 * (drp * T25[s][q]));
+          d += drs * dpq * I3 - 3.0 * (drs * T25[p][q]);
+          d += dps * drq * I3 - 3.0 * (dps * T25[r][q]);
+          d += -3.0 * ((drq * T25[p][s] + dpq * T25[r][s]) + dsq * T25[r][p]);
+          d += 15.0 * T47;
+          d += f2 * (-3.0 * (drp * dsq * I5) + 15.0 * (drp * T27[s][q]));
+          D2[r][p][s][q] = d * m.C1;
+        }
+  double B[3][3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int s = 0; s < 3; ++s) {
+      const double trD = D2[r][0][s][0] + D2[r][1][s][1] + D2[r][2][s][2];
+      for (int j = 0; j < 3; ++j)
+        B[r][s][j] = (j == 2 ? m.lam_d * trD : 0.0) + m.mu * D2[r][j][s][2] + m.mu * D2[r][2][s][j];
+    }
+  double Hl[3][3][3];
+  for (int j = 0; j < 3; ++j) {
+    const double trB = B[0][0][j] + B[1][1][j] + B[2][2][j];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        Hl[a][b][j] = -((a == b ? m.lam_d * trB : 0.0) + m.mu * (B[a][b][j] + B[b][a][j]));
+  }
+  rotate3(f, Hl, H);
+}
+
+// ----------------------------------------------------------- direct term
+// One source triangle at one observer, all K nodes: near field by the
+// closed-form recursion (sqrt(|x - c|^2 + eps^2) <= D_STAR L), far field by
+// the 12x12 (8x8 beyond D_STAR_DISTANT L) product rule
+// (mhs/fullspace/moments.py:551-601, mhs/fullspace/kernels.py:126-215).
+// R_FAR is the arithmetic type of the far-field quadrature.
+template <int P, int WANT, class R_FAR = double>
+MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
+                        const double* x, double eps, const Material& m,
+                        double* U, double* H, double* E) {
+  using S = DirectSpec<P, WANT>;
+  constexpr Spec sp = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = sp.w_off[NS];
+  const double d0 = x[0] - f.c[0], d1 = x[1] - f.c[1], d2 = x[2] - f.c[2];
+  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
+  double z, X0, X1;
+  to_plane(f, x, z, X0, X1);
+  const double h2 = z * z + eps * eps;
+  const double e4 = 15.0 * (eps * eps) * (eps * eps) / (8.0 * cst::PI);
+  if (D <= cst::D_STAR * f.L) {
+    MomentTable<S> T;
+    closed_moments<S>(f, X0, X1, h2, T);
+    double c[K][ntri(P)];
+    shape_coeffs<P>(f, X0, X1, c);
+#pragma unroll 1
+    for (int k = 0; k < K; ++k) {
+      double W[NW];
+      weight_closed<S, P>(T, c, k, W);
+      if (WANT & W_U) kernel_U<S>(f, W, z, eps, m, U + 9 * k);
+      if (WANT & W_H) kernel_H<S>(f, W, z, eps, m, H + 27 * k);
+      if (WANT & W_E) E[k] = e4 * W[sp.w_off[nslot(7)]];
+    }
+  } else {
+    const QuadRule& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
+    double W[K * NW];
+    weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
+#pragma unroll 1
+    for (int k = 0; k < K; ++k) {
+      if (WANT & W_U) kernel_U<S>(f, W + k * NW, z, eps, m, U + 9 * k);
+      if (WANT & W_H) kernel_H<S>(f, W + k * NW, z, eps, m, H + 27 * k);
+      if (WANT & W_E) E[k] = e4 * W[k * NW + sp.w_off[nslot(7)]];
+    }
+  }
+}
+
+// ------------------------------------------------------------ image data
+// Per-material image coefficients (built on the host from the generated
+// rationals): R records c(z) = cz[r][0] + z cz[r][1] + z^2 cz[r][2], scale
+// included; Q records a single number each, scale applied after the sum
+// (mhs/kernels/image.py:95-104, 257-297).
+struct ImageCoef {
+  const double* r_dg;    // [MHS_R_NDG][3]
+  const double* r_ddg;   // [MHS_R_NDDG][3]
+  const double* q_dg;    // [MHS_Q_NDG]
+  const double* q_ddg;   // [MHS_Q_NDDG]
+};
+
+// View of the packed coefficient block (host_prep.h: image_coef).
+MHS_HD ImageCoef image_coef_view(const double* base) {
+  ImageCoef c;
+  c.r_dg = base;
+  c.r_ddg = c.r_dg + 3 * MHS_R_NDG;
+  c.q_dg = c.r_ddg + 3 * MHS_R_NDDG;
+  c.q_ddg = c.q_dg + MHS_Q_NDG;
+  return c;
+}
+
+// Basis-product coefficients G_abc(alpha, beta): the coefficient of
+// x^alpha y^beta w^gamma in prod over the a+b+c Cartesian slots of
+// (e1_i x + e2_i y + n_i w), i.e. the geometry the lift sums per (alpha, beta)
+// group (mhs/fullspace/kernels.py:63-87), one polynomial per (a, b, c).
+constexpr int G_RMAX = 5;
+MHS_FI constexpr int abc_idx(int a, int b, int c) {
+  return (a + b + c) * (a + b + c + 1) * (a + b + c + 2) / 6 + tri_idx(b, c);
+}
+MHS_FI constexpr int g_rank_off(int r) {  // sum_{r' < r} ntri(r')^2
+  int s = 0;
+  for (int i = 0; i < r; ++i) s += ntri(i) * ntri(i);
+  return s;
+}
+MHS_FI constexpr int g_off(int a, int b, int c) {
+  return g_rank_off(a + b + c) + tri_idx(b, c) * ntri(a + b + c);
+}
+constexpr int G_SIZE = g_rank_off(G_RMAX + 1);
+
+MHS_HD void build_basis_products(const Frame& f, double* G) {
+  G[0] = 1.0;
+  for (int r = 1; r <= G_RMAX; ++r)
+    for (int b = 0; b <= r; ++b)
+      for (int c = 0; b + c <= r; ++c) {
+        const int a = r - b - c;
+        int pa = a, pb = b, pc = c, comp;
+        if (c > 0) { pc = c - 1; comp = 2; }
+        else if (b > 0) { pb = b - 1; comp = 1; }
+        else { pa = a - 1; comp = 0; }
+        const double* src = G + g_off(pa, pb, pc);
+        double* dst = G + g_off(a, b, c);
+        const double ux = f.e1[comp], uy = f.e2[comp], uw = f.n[comp];
+        for (int al = 0; al <= r; ++al)
+          for (int be = 0; al + be <= r; ++be) {
+            double v = 0.0;
+            if (al >= 1) v += ux * src[tri_idx(al - 1, be)];
+            if (be >= 1) v += uy * src[tri_idx(al, be - 1)];
+            if (al + be <= r - 1) v += uw * src[tri_idx(al, be)];
+            dst[tri_idx(al, be)] = v;
+          }
+      }
+}
+
+// Traction-operator contraction of DG (slip -> displacement) with the real
+// element's normal (mhs/kernels/image.py:127-137).
+MHS_HD void contract_dg(const double* DG, const double* nrm, const Material& m, double* U) {
+  for (int i = 0; i < 3; ++i) {
+    const double tr = DG[9 * i + 0] + DG[9 * i + 4] + DG[9 * i + 8];
+    for (int k = 0; k < 3; ++k) {
+      double s1 = 0.0, s2 = 0.0;
+      for (int l = 0; l < 3; ++l) {
+        s1 += nrm[l] * DG[9 * i + 3 * k + l];
+        s2 += nrm[l] * DG[9 * i + 3 * l + k];
+      }
+      U[3 * i + k] = m.mu * s1 + m.mu * s2 + m.lam * nrm[k] * tr;
+    }
+  }
+}
+
+// DDG (i, j, p, m) -> displacement gradient -> symmetric Hooke stress
+// (mhs/kernels/image.py:138-161).
+MHS_HD void contract_ddg(const double* DDG, const double* nrm, const Material& m, double* H) {
+  double S[3][3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int p = 0; p < 3; ++p) {
+      const double trm = DDG[27 * i + 9 * 0 + 3 * p + 0] + DDG[27 * i + 9 * 1 + 3 * p + 1] +
+                         DDG[27 * i + 9 * 2 + 3 * p + 2];
+      for (int k = 0; k < 3; ++k) {
+        double s1 = 0.0, s2 = 0.0;
+        for (int l = 0; l < 3; ++l) {
+          s1 += nrm[l] * DDG[27 * i + 9 * k + 3 * p + l];
+          s2 += nrm[l] * DDG[27 * i + 9 * l + 3 * p + k];
+        }
+        S[i][p][k] = m.mu * s1 + m.mu * s2 + m.lam * nrm[k] * trm;
+      }
+    }
+  for (int k = 0; k < 3; ++k) {
+    double e[3][3];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) e[a][b] = 0.5 * (S[a][b][k] + S[b][a][k]);
+    const double tr = e[0][0] + e[1][1] + e[2][2];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double v = 2.0 * m.mu * e[a][b];
+        if (a == b) v += m.lam * tr;
+        H[9 * a + 3 * b + k] = v;
+      }
+  }
+}
+
+// --------------------------------------------------------- image R-family
+// The closed-form R-family on the reflected element (mhs/kernels/image.py:
+// 435-497): weighted tables of the image frame, Cartesian monomial moments
+// D1^a D2^b D3^c / R2^n from the basis products G, then the generated records.
+template <int P, int WANT, class R_FAR = double>
+MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
+                         const QuadRule& r12, const QuadRule& r8, const double* x, double eps,
+                         const Material& m, const ImageCoef& ic, double* U, double* H) {
+  using S = SpecImg<P>;
+  constexpr Spec sp = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = sp.w_off[NS];
+  const double d0 = x[0] - fi.c[0], d1 = x[1] - fi.c[1], d2 = x[2] - fi.c[2];
+  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
+  double zp, X0, X1;
+  to_plane(fi, x, zp, X0, X1);
+  const double h2 = zp * zp + eps * eps;
+  const double zo = x[2];   // absolute depth of the observer
+  double zpow[G_RMAX + 1];
+  zpow[0] = 1.0;
+  for (int i = 1; i <= G_RMAX; ++i) zpow[i] = zpow[i - 1] * zp;
+  double Wall[K * NW];
+  if (D <= cst::D_STAR * fi.L) {
+    MomentTable<S> T;
+    closed_moments<S>(fi, X0, X1, h2, T);
+    double c[K][ntri(P)];
+    shape_coeffs<P>(fi, X0, X1, c);
+    for (int k = 0; k < K; ++k) weight_closed<S, P>(T, c, k, Wall + k * NW);
+  } else {
+    const QuadRule& q = (D > cst::D_STAR_DISTANT * fi.L) ? r8 : r12;
+    weight_far<S, P, R_FAR>(q, X0, X1, h2, Wall);
+  }
+#pragma unroll 1
+  for (int k = 0; k < K; ++k) {
+    const double* W = Wall + k * NW;
+    // Cartesian monomial moments
+    double Tm[MHS_R_NMONO];
+#pragma unroll 1
+    for (int mi = 0; mi < MHS_R_NMONO; ++mi) {
+      const int a = MHS_TAB(mhs_r_mono)[mi][0], b = MHS_TAB(mhs_r_mono)[mi][1],
+                c = MHS_TAB(mhs_r_mono)[mi][2], n = MHS_TAB(mhs_r_mono)[mi][3];
+      const int r = a + b + c, s = nslot(n);
+      const double* g = G + g_off(a, b, c);
+      const double* Wn = W + sp.w_off[s];
+      double acc = 0.0;
+      for (int t = 0; t <= r; ++t) {
+        double part = 0.0;
+        for (int al = 0; al <= t; ++al) part += g[tri_idx(al, t - al)] * Wn[tri_idx(al, t - al)];
+        const double v = zpow[r - t] * part;
+        acc += (t & 1) ? -v : v;
+      }
+      Tm[mi] = acc;
+    }
+    if (WANT & W_U) {
+      double DG[27];
+      for (int i = 0; i < 27; ++i) DG[i] = 0.0;
+#pragma unroll 1
+      for (int r = 0; r < MHS_R_NDG; ++r) {
+        const int mi = MHS_TAB(mhs_r_dg_idx)[r][0], slot = MHS_TAB(mhs_r_dg_idx)[r][1];
+        const double* cz = ic.r_dg + 3 * r;
+        DG[slot] += (cz[0] + zo * (cz[1] + zo * cz[2])) * Tm[mi];
+      }
+      contract_dg(DG, nrm, m, U + 9 * k);
+    }
+    if (WANT & W_H) {
+      double DDG[81];
+      for (int i = 0; i < 81; ++i) DDG[i] = 0.0;
+#pragma unroll 1
+      for (int r = 0; r < MHS_R_NDDG; ++r) {
+        const int mi = MHS_TAB(mhs_r_ddg_idx)[r][0], slot = MHS_TAB(mhs_r_ddg_idx)[r][1];
+        const double* cz = ic.r_ddg + 3 * r;
+        DDG[slot] += (cz[0] + zo * (cz[1] + zo * cz[2])) * Tm[mi];
+      }
+      contract_ddg(DDG, nrm, m, H + 27 * k);
+    }
+  }
+}
+
+// --------------------------------------------------------- image Q-family
+// Exact distance from a point to a closed triangle (mhs/kernels/image.py:
+// 170-208), used by the Q-family order law.
+MHS_HD double triangle_distance(const double* x, const double* t) {
+  const double* a = t;
+  const double* b = t + 3;
+  const double* c = t + 6;
+  double ab[3], ac[3], ap[3], nr[3];
+  for (int j = 0; j < 3; ++j) {
+    ab[j] = b[j] - a[j];
+    ac[j] = c[j] - a[j];
+    ap[j] = x[j] - a[j];
+  }
+  cross3(ab, ac, nr);
+  const double d20 = dot3(ap, ab), d21 = dot3(ap, ac);
+  const double d00 = dot3(ab, ab), d01 = dot3(ab, ac), d11 = dot3(ac, ac);
+  const double den = d00 * d11 - d01 * d01;
+  const double v = (d11 * d20 - d01 * d21) / den;
+  const double w = (d00 * d21 - d01 * d20) / den;
+  const double u = 1.0 - v - w;
+  if (u >= 0.0 && v >= 0.0 && w >= 0.0) return fabs(dot3(ap, nr)) / norm3(nr);
+  double best = INFINITY;
+  const double* P0[3] = {a, b, c};
+  const double* P1[3] = {b, c, a};
+  for (int e = 0; e < 3; ++e) {
+    double ev[3], d[3];
+    for (int j = 0; j < 3; ++j) {
+      ev[j] = P1[e][j] - P0[e][j];
+      d[j] = x[j] - P0[e][j];
+    }
+    double tt = dot3(d, ev) / dot3(ev, ev);
+    tt = tt < 0.0 ? 0.0 : (tt > 1.0 ? 1.0 : tt);
+    double q[3];
+    for (int j = 0; j < 3; ++j) q[j] = x[j] - (P0[e][j] + tt * ev[j]);
+    const double dist = norm3(q);
+    if (dist < best) best = dist;
+  }
+  return best;
+}
+
+// Gauss order per observer: clip(ceil(C L / sqrt(delta^2 + eps^2)) + order)
+// with delta the distance to the image triangle (image.py:211-254).
+MHS_HD int q_gauss_order(const double* x, const double* tri_img, double eps, double L, int order) {
+  const double delta = triangle_distance(x, tri_img);
+  const double scale = sqrt(delta * delta + eps * eps);
+  double nq = ceil(cst::IMAGE_Q_BUDGET_C * L / scale) + (double)order;
+  if (nq < cst::IMAGE_Q_GAUSS_MIN) nq = cst::IMAGE_Q_GAUSS_MIN;
+  if (nq > cst::IMAGE_Q_GAUSS_MAX) nq = cst::IMAGE_Q_GAUSS_MAX;
+  return (int)nq;
+}
+
+// A Q-family rule on the REAL element: Cartesian nodes y, weights wN[k] =
+// area weight x N_k (image.py:325-339).
+struct QRule {
+  int nq;
+  const double* y;    // nq x 3
+  const double* wN;   // nq x K
+};
+
+template <int P>
+MHS_HD void build_qrule(const Frame& f, const double* glx, const double* glw, int n,
+                        double* y, double* wN) {
+  constexpr int K = n_nodes(P);
+  const double* x = glx + gl_offset(n);
+  const double* w = glw + gl_offset(n);
+  int q = 0;
+  for (int i = 0; i < n; ++i) {
+    const double gi = 0.5 * (x[i] + 1.0), wi = 0.5 * w[i];
+    for (int j = 0; j < n; ++j, ++q) {
+      const double gj = 0.5 * (x[j] + 1.0), wj = 0.5 * w[j];
+      const double x1 = gi, x2 = gj * (1.0 - gi);
+      const double ww = wi * wj * (1.0 - gi);
+      const double l0 = 1.0 - x1 - x2;
+      for (int c = 0; c < 3; ++c) y[3 * q + c] = (l0 * f.v[0][c] + x1 * f.v[1][c]) + x2 * f.v[2][c];
+      const double e0 = (l0 * f.p[0][0] + x1 * f.p[1][0]) + x2 * f.p[2][0];
+      const double e1 = (l0 * f.p[0][1] + x1 * f.p[1][1]) + x2 * f.p[2][1];
+      double N[K];
+      shape_at<P>(f, e0, e1, N);
+      const double wq = ww * (2.0 * f.area);
+      for (int k = 0; k < K; ++k) wN[q * K + k] = wq * N[k];
+    }
+  }
+}
+
+// Q-family moments by quadrature, contracted (image.py:315-432).
+template <int P, int WANT>
+MHS_HD void image_q_eval(const QRule& q, const double* nrm, const double* x, double eps,
+                         const Material& m, const ImageCoef& ic, double* U, double* H) {
+  constexpr int K = n_nodes(P);
+  double basis[MHS_Q_NMONO][K];
+  for (int i = 0; i < MHS_Q_NMONO; ++i)
+    for (int k = 0; k < K; ++k) basis[i][k] = 0.0;
+  const double e2 = eps * eps;
+#pragma unroll 1
+  for (int t = 0; t < q.nq; ++t) {
+    const double d1 = x[0] - q.y[3 * t + 0];
+    const double d2 = x[1] - q.y[3 * t + 1];
+    const double d3 = x[2] + q.y[3 * t + 2];
+    const double r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
+    const double ir = 1.0 / r2, iq = 1.0 / (r2 - d3);
+    double p1[5], p2[5], p3[5], pr[8], pq[5];
+    p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
+    for (int i = 2; i < 5; ++i) {
+      p1[i] = p1[i - 1] * d1;
+      p2[i] = p2[i - 1] * d2;
+      p3[i] = p3[i - 1] * d3;
+      pq[i] = pq[i - 1] * iq;
+    }
+    for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
+    const double* wN = q.wN + t * K;
+#pragma unroll 1
+    for (int mi = 0; mi < MHS_Q_NMONO; ++mi) {
+      const int* e = MHS_TAB(mhs_q_mono)[mi];
+      double v = 1.0;
+      bool first = true;
+      if (e[0]) { v = p1[e[0]]; first = false; }
+      if (e[1]) { v = first ? p2[e[1]] : v * p2[e[1]]; first = false; }
+      if (e[2]) { v = first ? p3[e[2]] : v * p3[e[2]]; first = false; }
+      if (e[3]) { v = first ? pr[e[3]] : v * pr[e[3]]; first = false; }
+      if (e[4]) { v = first ? pq[e[4]] : v * pq[e[4]]; first = false; }
+      for (int k = 0; k < K; ++k) basis[mi][k] += v * wN[k];
+    }
+  }
+#pragma unroll 1
+  for (int k = 0; k < K; ++k) {
+    if (WANT & W_U) {
+      double DG[27];
+      for (int i = 0; i < 27; ++i) DG[i] = 0.0;
+      for (int r = 0; r < MHS_Q_NDG; ++r)
+        DG[MHS_TAB(mhs_q_dg_idx)[r][1]] += ic.q_dg[r] * basis[MHS_TAB(mhs_q_dg_idx)[r][0]][k];
+      for (int i = 0; i < 27; ++i) DG[i] *= m.scale_c;
+      contract_dg(DG, nrm, m, U + 9 * k);
+    }
+    if (WANT & W_H) {
+      double DDG[81];
+      for (int i = 0; i < 81; ++i) DDG[i] = 0.0;
+      for (int r = 0; r < MHS_Q_NDDG; ++r)
+        DDG[MHS_TAB(mhs_q_ddg_idx)[r][1]] += ic.q_ddg[r] * basis[MHS_TAB(mhs_q_ddg_idx)[r][0]][k];
+      for (int i = 0; i < 81; ++i) DDG[i] *= m.scale_c;
+      contract_ddg(DDG, nrm, m, H + 27 * k);
+    }
+  }
+}
+
+}  // namespace mhs

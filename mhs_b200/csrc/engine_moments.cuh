@@ -1,0 +1,474 @@
+// Weighted moment tables of one triangle at one observer:
+//
+//   W_k[n](a, b) = int_T N_k(y) xi_1^a xi_2^b / R_eps^n dS,
+//   R_eps^2 = xi_1^2 + xi_2^2 + z^2 + eps^2,
+//
+// by the divergence-theorem recursion (near field) or a collapsed Gauss
+// product rule (far field), exactly the split of mhs/fullspace/moments.py:
+// 515-606.  One thread evaluates one (observer, triangle) pair.
+#pragma once
+
+#include "engine_base.cuh"
+
+namespace mhs {
+
+// 1/i for the series denominators.
+MHS_FI double inv_int(int i) { return 1.0 / (double)i; }
+
+MHS_FI double ipow(double x, int e) {
+  double r = 1.0;
+  const int n = e < 0 ? -e : e;
+  for (int i = 0; i < n; ++i) r *= x;
+  return e < 0 ? 1.0 / r : r;
+}
+
+// ------------------------------------------------------ edge primitives
+// P[m][k] = int_{ua}^{ub} u^k / (u^2 + rho^2)^(m/2) du for the (m, k) of the
+// spec, cancellation-free: the small-|u| binomial series where both ends sit
+// within rho/2 of the foot, the large-|u| series where both lie beyond 2 rho
+// on one side, the closed-form difference forms otherwise
+// (mhs/fullspace/primitives.py:131-504; rho > 0 always since eps > 0).
+
+template <class S>
+MHS_HD void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
+  constexpr Spec sp = S::spec;
+  const double Ra = sqrt(ua * ua + rho2);
+  const double Rb = sqrt(ub * ub + rho2);
+  const double dR = (ub - ua) * (ub + ua) / (Ra + Rb);   // R_b - R_a
+  double J[MS], Kk[MS];
+  // Delta J_1: log1p forms on one side, the product form across the foot
+  if (sp.Jneed[1]) {
+    if (ua >= 0.0) J[1] = log1p(((ub - ua) + dR) / (ua + Ra));
+    else if (ub <= 0.0) J[1] = log1p(((ub - ua) - dR) / (Rb - ub));
+    else J[1] = log(((ub + Rb) * (Ra - ua)) / rho2);
+  }
+  if (sp.Jneed[2]) {
+    if (ua * ub > 0.0) J[2] = ((ub - ua) * (ub + ua)) / ((Ra * Rb) * (ub * Ra + ua * Rb));
+    else J[2] = (ub / Rb - ua / Ra) / rho2;
+  }
+  if (sp.Jneed[3]) {  // m = 5 from m = 3
+    const double iRa = 1.0 / Ra, iRb = 1.0 / Rb;
+    const double duRm = ub * (iRb * iRb * iRb) - ua * (iRa * iRa * iRa);
+    J[3] = (duRm + 2.0 * J[2]) / (3.0 * rho2);
+  }
+  if (sp.Jneed[4]) {  // m = 7 from m = 5
+    const double iRa = 1.0 / Ra, iRb = 1.0 / Rb;
+    const double a2 = iRa * iRa, b2 = iRb * iRb;
+    const double duRm = ub * (b2 * b2 * iRb) - ua * (a2 * a2 * iRa);
+    J[4] = (duRm + 4.0 * J[3]) / (5.0 * rho2);
+  }
+  if (sp.Jneed[0]) {  // m = -1
+    const double duR = 0.5 * (ub - ua) * (Ra + Rb) + 0.5 * (ua + ub) * dR;
+    J[0] = 0.5 * (duR + rho2 * J[1]);
+  }
+  // Delta K_m = Delta R^(2-m) / (2-m), factored through dR
+  if (sp.Kneed[0]) Kk[0] = dR * ((Rb * Rb + Ra * Rb) + Ra * Ra) / 3.0;
+  if (sp.Kneed[1]) Kk[1] = dR;
+  if (sp.Kneed[2]) Kk[2] = dR / (Ra * Rb);
+  if (sp.Kneed[3]) {
+    const double ab = Ra * Rb;
+    Kk[3] = dR * ((Rb * Rb + Ra * Rb) + Ra * Ra) / (3.0 * (ab * ab * ab));
+  }
+  if (sp.Kneed[4]) {
+    const double ab = Ra * Rb, a2 = Ra * Ra, b2 = Rb * Rb;
+    const double s = (((b2 * b2 + Ra * (b2 * Rb)) + a2 * b2) + (a2 * Ra) * Rb) + a2 * a2;
+    Kk[4] = dR * s / (5.0 * (ab * ab * ab * ab * ab));
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+#pragma unroll
+    for (int j = 0; j < MS; ++j) {
+      if (!sp.Pneed[j][k]) continue;
+      if (k == 0) P[j][0] = J[j];
+      else if (k == 1) P[j][1] = Kk[j];
+      else P[j][k] = P[j - 1][k - 2] - rho2 * P[j][k - 2];
+    }
+}
+
+template <class S>
+MHS_HD void edge_small(double ua, double ub, double rho, double P[MS][8]) {
+  constexpr Spec sp = S::spec;
+  constexpr int PWMAX = sp.kmax + 2 * (cst::SERIES_TERMS - 1) + 1;
+  const double ya = ua / rho, yb = ub / rho;
+  const bool same = ua * ub > 0.0;
+  // E[pw] = (yb^pw - ya^pw) / pw; the same-sign recurrence
+  // D_{pw+1} = yb D_pw + ya^pw (yb - ya) has no cancellation.
+  double E[PWMAX + 1];
+  const double dy = yb - ya;
+  double yap = ya, ybp = yb, D = dy;
+#pragma unroll
+  for (int pw = 1; pw <= PWMAX; ++pw) {
+    E[pw] = D * inv_int(pw);
+    if (same) D = yb * D + yap * dy;
+    yap *= ya;
+    ybp *= yb;
+    if (!same) D = ybp - yap;
+  }
+#pragma unroll
+  for (int j = 0; j < MS; ++j) {
+    if (sp.edge[j] < 0) continue;
+    const int m = 2 * j - 1;
+    const double* bh = MHS_TAB(mhs_binom_half)[j];
+#pragma unroll
+    for (int k = 0; k <= sp.edge[j]; ++k) {
+      double acc = 0.0;
+#pragma unroll
+      for (int t = 0; t < cst::SERIES_TERMS; ++t) acc += bh[t] * E[k + 2 * t + 1];
+      P[j][k] = ipow(rho, k + 1 - m) * acc;
+    }
+  }
+}
+
+// Exponent range q = k - m + 1 - 2 t of the large-|u| series over a spec.
+constexpr int series_qhi(const Spec& sp) {
+  int q = -999;
+  for (int j = 0; j < MS; ++j)
+    if (sp.edge[j] >= 0) q = imax(q, sp.edge[j] - (2 * j - 1) + 1);
+  return q;
+}
+constexpr int series_qlo(const Spec& sp) {
+  int q = 999;
+  for (int j = 0; j < MS; ++j)
+    if (sp.edge[j] >= 0) q = imin(q, 0 - (2 * j - 1) + 1);
+  return q - 2 * (cst::SERIES_TERMS - 1);
+}
+constexpr int spec_max_need0(const Spec& sp) {
+  int d = 0;
+  for (int s = 0; s < NS; ++s) d = imax(d, sp.need0[s]);
+  return d;
+}
+
+template <class S>
+MHS_HD void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
+  constexpr Spec sp = S::spec;
+  // exponent range q = k - m + 1 - 2 t over the spec
+  constexpr int QHI = series_qhi(sp);
+  constexpr int QLO = series_qlo(sp);
+  constexpr int NQ = QHI - QLO + 1;
+  const bool neg = ua < 0.0;
+  const double a = neg ? -ub : ua, b = neg ? -ua : ub;
+  const double r = b / a;
+  const double log_r = log1p((b - a) / a);
+  const bool close = r < 2.0;
+  const double x = rho2 / (a * a);
+  // dq[q] = [t^q / q]_1^r (log r at q = 0).  Near r = 1 the geometric sums
+  // (r - 1) sum r^i and (1 - 1/r) sum r^-i replace expm1 without cancellation.
+  double dq[NQ];
+  const double rm1 = (b - a) / a;     // r - 1
+  const double omt = (b - a) / b;     // 1 - 1/r
+  const double t = a / b;             // 1/r
+  if constexpr (QHI >= 0) dq[0 - QLO] = log_r;
+  if constexpr (QHI >= 1) dq[1 - QLO] = close ? rm1 : r - 1.0;
+  if constexpr (QHI >= 2) dq[2 - QLO] = (close ? rm1 * (1.0 + r) : r * r - 1.0) * 0.5;
+  static_assert(QHI <= 2, "large-u series exponent above 2");
+  {
+    double gsum = 0.0, tk = 1.0;
+#pragma unroll
+    for (int k = 1; k <= -QLO; ++k) {
+      gsum += tk;
+      tk *= t;
+      if (-k <= QHI) dq[-k - QLO] = (close ? omt * gsum : 1.0 - tk) * inv_int(k);
+    }
+  }
+  double xj[cst::SERIES_TERMS];
+  xj[0] = 1.0;
+#pragma unroll
+  for (int i = 1; i < cst::SERIES_TERMS; ++i) xj[i] = xj[i - 1] * x;
+#pragma unroll
+  for (int j = 0; j < MS; ++j) {
+    if (sp.edge[j] < 0) continue;
+    const int m = 2 * j - 1;
+    const double* bh = MHS_TAB(mhs_binom_half)[j];
+#pragma unroll
+    for (int k = 0; k <= sp.edge[j]; ++k) {
+      const int s = k - m + 1;
+      double acc = 0.0;
+#pragma unroll
+      for (int i = 0; i < cst::SERIES_TERMS; ++i) acc += (bh[i] * xj[i]) * dq[s - 2 * i - QLO];
+      const double v = ipow(a, s) * acc;
+      P[j][k] = (neg && (k & 1)) ? -v : v;
+    }
+  }
+}
+
+template <class S>
+MHS_HD void edge_table(double ua, double ub, double rho2, double P[MS][8]) {
+  const double rho = sqrt(rho2);
+  const double aua = fabs(ua), aub = fabs(ub);
+  const double umax = aua > aub ? aua : aub;
+  const double umin = aua < aub ? aua : aub;
+  if (umax <= cst::SMALL_U_OVER_RHO * rho) edge_small<S>(ua, ub, rho, P);
+  else if (ua * ub > 0.0 && umin >= cst::SERIES_U_OVER_RHO * rho) edge_large<S>(ua, ub, rho2, P);
+  else edge_closed<S>(ua, ub, rho2, P);
+}
+
+// ------------------------------------------------- closed-form moment table
+// M_n^(a,b)(x) = int_T xi_1^a xi_2^b / R_eps^n dS for the closed degrees of
+// the spec, seeded by the solid angle and the vertical identity and filled
+// by the horizontal recursion (mhs/fullspace/moments.py:171-355).
+template <class S>
+struct MomentTable {
+  static constexpr Spec sp = S::spec;
+  double M[sp.m_off[NS] > 0 ? sp.m_off[NS] : 1];
+  MHS_FI double& at(int s, int a, int b) { return M[sp.m_off[s] + tri_idx(a, b)]; }
+  MHS_FI double at(int s, int a, int b) const { return M[sp.m_off[s] + tri_idx(a, b)]; }
+};
+
+// Van Oosterom-Strackee solid angle of the triangle seen from the point at
+// in-plane offset -X, height h; the vertices are given relative to the foot
+// (pa[i] = p_i - X), so the point sits at (0, 0, h) in the local frame.
+MHS_HD double solid_angle_local(const double pr[3][2], double h) {
+  double r[3][3];
+  for (int i = 0; i < 3; ++i) {
+    r[i][0] = pr[i][0];
+    r[i][1] = pr[i][1];
+    r[i][2] = -h;
+  }
+  const double R1 = norm3(r[0]), R2 = norm3(r[1]), R3 = norm3(r[2]);
+  double cx[3];
+  cross3(r[1], r[2], cx);
+  const double numer = dot3(r[0], cx);
+  const double denom = R1 * R2 * R3 + R3 * dot3(r[0], r[1]) + R1 * dot3(r[1], r[2]) +
+                       R2 * dot3(r[0], r[2]);
+  return 2.0 * atan2(numer, denom);
+}
+
+template <class S>
+MHS_HD void closed_moments(const Frame& f, double X0, double X1, double h2, MomentTable<S>& T) {
+  constexpr Spec sp = S::spec;
+  constexpr int NB = sp.b_off[MS] > 0 ? sp.b_off[MS] : 1;
+  double BN1[NB], BN2[NB], BD[MS];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    BN1[i] = 0.0;
+    BN2[i] = 0.0;
+  }
+#pragma unroll
+  for (int j = 0; j < MS; ++j) BD[j] = 0.0;
+  double pr[3][2];
+  for (int k = 0; k < 3; ++k) {
+    pr[k][0] = f.p[k][0] - X0;
+    pr[k][1] = f.p[k][1] - X1;
+  }
+#pragma unroll 1
+  for (int e = 0; e < 3; ++e) {
+    const int e2 = e == 2 ? 0 : e + 1;
+    const double pa0 = pr[e][0], pa1 = pr[e][1], pb0 = pr[e2][0], pb1 = pr[e2][1];
+    const double ev0 = pb0 - pa0, ev1 = pb1 - pa1;
+    const double L = sqrt(ev0 * ev0 + ev1 * ev1);
+    const double s1 = ev0 / L, s2 = ev1 / L;   // edge tangent t
+    const double c1 = s2, c2 = -s1;            // outward normal (t_y, -t_x)
+    const double dp = pa0 * c1 + pa1 * c2;
+    const double ua = pa0 * s1 + pa1 * s2;
+    const double ub = pb0 * s1 + pb1 * s2;
+    const double rho2 = dp * dp + h2;
+    double P[MS][8];
+    edge_table<S>(ua, ub, rho2, P);
+#pragma unroll
+    for (int j = 0; j < MS; ++j)
+      if (sp.edge[j] >= 0) BD[j] += dp * P[j][0];
+    // xi_1^a xi_2^b along the edge as a polynomial in u:
+    // xi_1 = dp c1 + u s1, xi_2 = dp c2 + u s2.
+    constexpr int KM = sp.kmax;
+    double pa_[KM + 1];   // xi_1^a
+    pa_[0] = 1.0;
+#pragma unroll
+    for (int i = 1; i <= KM; ++i) pa_[i] = 0.0;
+    const double l0 = dp * c1, l1 = s1, m0 = dp * c2, m1 = s2;
+#pragma unroll
+    for (int a = 0; a <= KM; ++a) {
+      double pb_[KM + 1];
+#pragma unroll
+      for (int i = 0; i <= KM; ++i) pb_[i] = pa_[i];
+#pragma unroll
+      for (int b = 0; a + b <= KM; ++b) {
+        // pb_ holds xi_1^a xi_2^b (degree a + b)
+#pragma unroll
+        for (int j = 0; j < MS; ++j) {
+          if (sp.edge[j] < a + b) continue;
+          double val = 0.0;
+#pragma unroll
+          for (int i = 0; i <= a + b; ++i) val += pb_[i] * P[j][i];
+          BN1[sp.b_off[j] + tri_idx(a, b)] += c1 * val;
+          BN2[sp.b_off[j] + tri_idx(a, b)] += c2 * val;
+        }
+        if (a + b < KM) {  // multiply by xi_2
+#pragma unroll
+          for (int i = KM; i >= 1; --i) pb_[i] = pb_[i] * m0 + pb_[i - 1] * m1;
+          pb_[0] = pb_[0] * m0;
+        }
+      }
+      if (a < KM) {  // multiply by xi_1
+#pragma unroll
+        for (int i = KM; i >= 1; --i) pa_[i] = pa_[i] * l0 + pa_[i - 1] * l1;
+        pa_[0] = pa_[0] * l0;
+      }
+    }
+  }
+  const double h = sqrt(h2);
+  const double I3 = -solid_angle_local(pr, h) / h;
+#pragma unroll
+  for (int i = 0; i < sp.m_off[NS]; ++i) T.M[i] = 0.0;
+  T.at(nslot(3), 0, 0) = I3;
+  // upward seeds I_{n+2} = (E_n + (n-2) I_n) / (n h^2)
+#pragma unroll
+  for (int n = 3; n + 2 <= 9; n += 2) {
+    if (sp.deg[nslot(n + 2)] < 0) break;
+    T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) / (n * h2);
+  }
+  // downward seeds I_n = (E_n - n h^2 I_{n+2}) / (2 - n)
+#pragma unroll
+  for (int n = 1; n >= -1; n -= 2) {
+    if (sp.deg[nslot(n)] < 0) break;
+    const double corr = n * h2 * T.at(nslot(n + 2), 0, 0);
+    T.at(nslot(n), 0, 0) = (BD[nslot(n)] - corr) / (2.0 - n);
+  }
+  // horizontal recursion, ascending n
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int d = sp.deg[s];
+    if (d <= 0) continue;
+    const int n = slot_n(s), mj = s - 1;   // m = n - 2
+    const double inv = 1.0 / (double)(n - 2);
+#pragma unroll
+    for (int q = 1; q <= d; ++q)
+#pragma unroll
+      for (int a = q; a >= 0; --a) {
+        const int b = q - a;
+        double val;
+        if (a >= 1) {
+          val = -BN1[sp.b_off[mj] + tri_idx(a - 1, b)];
+          if (a >= 2) val = val + (a - 1) * T.at(s - 1, a - 2, b);
+        } else {
+          val = -BN2[sp.b_off[mj] + tri_idx(0, b - 1)];
+          if (b >= 2) val = val + (b - 1) * T.at(s - 1, 0, b - 2);
+        }
+        T.at(s, a, b) = val * inv;
+      }
+  }
+}
+
+// W_k[n](a, b) = sum_{a'+b'<=P} c_k(a', b') M_n(a + a', b + b'), at the
+// constant-slip degrees (mhs/fullspace/moments.py:370-398).
+template <class S, int P>
+MHS_HD void weight_closed(const MomentTable<S>& T, const double c[][ntri(P)], int k, double* W) {
+  constexpr Spec sp = S::spec;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int d = sp.need0[s];
+    if (d < 0) continue;
+#pragma unroll
+    for (int a = 0; a <= d; ++a)
+#pragma unroll
+      for (int b = 0; a + b <= d; ++b) {
+        double acc = 0.0;
+#pragma unroll
+        for (int ap = 0; ap <= P; ++ap)
+#pragma unroll
+          for (int bp = 0; ap + bp <= P; ++bp)
+            acc += c[k][tri_idx(ap, bp)] * T.at(s, a + ap, b + bp);
+        W[sp.w_off[s] + tri_idx(a, b)] = acc;
+      }
+  }
+}
+
+// ----------------------------------------------------- far-field quadrature
+// Collapsed Gauss product rule on the reference triangle, mapped onto the
+// element: nodes eta (centroid frame), weights wq (area measure) and N_k at
+// the nodes (mhs/fullspace/moments.py:401-446).  Built once per source.
+struct QuadRule {
+  int nq;
+  const double* eta0;
+  const double* eta1;
+  const double* wq;
+  const double* Nq;   // nq x K, node-major
+};
+
+// Fill a rule for order n from the 1-D Gauss-Legendre table (x in [-1, 1]).
+template <int P>
+MHS_HD void build_rule(const Frame& f, const double* glx, const double* glw, int n,
+                       double* eta0, double* eta1, double* wq, double* Nq) {
+  constexpr int K = n_nodes(P);
+  const double* x = glx + gl_offset(n);
+  const double* w = glw + gl_offset(n);
+  int q = 0;
+  for (int i = 0; i < n; ++i) {
+    const double gi = 0.5 * (x[i] + 1.0), wi = 0.5 * w[i];
+    for (int j = 0; j < n; ++j, ++q) {
+      const double gj = 0.5 * (x[j] + 1.0), wj = 0.5 * w[j];
+      const double x1 = gi, x2 = gj * (1.0 - gi);
+      const double ww = wi * wj * (1.0 - gi);
+      const double l0 = 1.0 - x1 - x2;
+      const double e0 = (l0 * f.p[0][0] + x1 * f.p[1][0]) + x2 * f.p[2][0];
+      const double e1 = (l0 * f.p[0][1] + x1 * f.p[1][1]) + x2 * f.p[2][1];
+      eta0[q] = e0;
+      eta1[q] = e1;
+      wq[q] = ww * (2.0 * f.area);
+      shape_at<P>(f, e0, e1, Nq + q * K);
+    }
+  }
+}
+
+// W_k[n](a, b) by quadrature of N_k xi_1^a xi_2^b R^-n at the constant-slip
+// degrees (mhs/fullspace/moments.py:427-498).  R is float or double: the
+// mixed-precision form runs this in float with float accumulation.
+template <class S, int P, class R>
+MHS_HD void weight_far(const QuadRule& q, double X0, double X1, double h2, double* Wout) {
+  constexpr Spec sp = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = sp.w_off[NS];
+  constexpr int DM = spec_max_need0(sp);
+  R acc[K][NW];
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int i = 0; i < NW; ++i) acc[k][i] = R(0);
+  const R x0 = R(X0), x1 = R(X1), hh = R(h2);
+#pragma unroll 1
+  for (int t = 0; t < q.nq; ++t) {
+    const R xi0 = R(q.eta0[t]) - x0, xi1 = R(q.eta1[t]) - x1;
+    const R R2 = xi0 * xi0 + xi1 * xi1 + hh;
+    const R inv = R(1) / sqrt(R2);
+    const R inv2 = inv * inv;
+    R rp[NS];   // R^-n for odd n
+    {
+      R cur = inv;
+#pragma unroll
+      for (int s = 1; s < NS; ++s) {
+        rp[s] = cur;
+        cur = cur * inv2;
+      }
+    }
+    R p0[DM + 1], p1[DM + 1];
+    p0[0] = R(1);
+    p1[0] = R(1);
+#pragma unroll
+    for (int i = 1; i <= DM; ++i) {
+      p0[i] = p0[i - 1] * xi0;
+      p1[i] = p1[i - 1] * xi1;
+    }
+    const R wq = R(q.wq[t]);
+    R Nk[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) Nk[k] = R(q.Nq[t * K + k]);
+#pragma unroll
+    for (int a = 0; a <= DM; ++a)
+#pragma unroll
+      for (int b = 0; a + b <= DM; ++b) {
+        const R mono = (a && b) ? wq * p0[a] * p1[b] : a ? wq * p0[a] : b ? wq * p1[b] : wq;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          if (sp.need0[s] < a + b) continue;
+          const R v = mono * rp[s];
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k][sp.w_off[s] + tri_idx(a, b)] += v * Nk[k];
+        }
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int i = 0; i < NW; ++i) Wout[k * NW + i] = double(acc[k][i]);
+}
+
+}  // namespace mhs
