@@ -1,0 +1,114 @@
+/* C ABI of the B200 Green's-function assembler.
+ *
+ * One entry point fills one matrix on one CUDA device, asynchronously on the
+ * caller's stream.  Every pointer in mhs_request is DEVICE memory owned by
+ * the caller; the library allocates nothing per call (it keeps a small
+ * per-device table of Gauss-Legendre rules, built on first use).  Scratch
+ * comes from the caller's workspace, sized by mhs_workspace_bytes.
+ *
+ * The request mirrors mhs's internal assembly seam (mhs/kernels/assemble.py:
+ * 190-366), which sees only C-contiguous float64 arrays and plain floats:
+ * obs (N, 3), tris (S, 3, 3), eps (S,), mu, lam, a preallocated output,
+ * order, ids (S, 6) for shared columns, fold, plus receiver normals for
+ * traction and receiver/source bases for interaction.  Validation of user
+ * input (shapes, z <= 0, eps > 0, the byte ceiling) happens in the caller,
+ * as in mhs/matrices.py:75-227; the library re-checks what would make a
+ * launch unsafe and returns an error code instead.
+ */
+#ifndef MHS_B200_H
+#define MHS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Output kinds, each one of mhs's public matrix functions. */
+enum mhs_kind {
+  MHS_DISP = 0,          /* disp_matrix          (N, 3, n_dof, 3)    matrices.py:231 */
+  MHS_STRESS = 1,        /* stress_matrix        (N, 3, 3, n_dof, 3) matrices.py:251 */
+  MHS_TOTAL_STRESS = 2,  /* total_stress_matrix  (N, 3, 3, n_dof, 3) matrices.py:494 */
+  MHS_EIGENSTRESS = 3,   /* eigenstress_matrix   (N, 3, 3, n_dof, 3) matrices.py:518 */
+  MHS_STRAIN = 4,        /* elastic_strain_matrix(N, 3, 3, n_dof, 3) matrices.py:546 */
+  MHS_TRACTION = 5,      /* traction_matrix      (N, 3, n_dof, 3)    matrices.py:298 */
+  MHS_INTERACTION = 6    /* interaction_matrix   (N, n_dof, n_a, n_b) matrices.py:378 */
+};
+
+enum mhs_precision {
+  MHS_FP64 = 0,   /* every term in float64 */
+  MHS_MIXED = 1   /* far-field quadrature bulk in float32, the rest float64 */
+};
+
+enum mhs_status_code {
+  MHS_OK = 0,
+  MHS_ERR_ARG = 1,        /* invalid request field */
+  MHS_ERR_WORKSPACE = 2,  /* workspace too small */
+  MHS_ERR_CUDA = 3,       /* a CUDA call failed */
+  MHS_ERR_DEVICE = 4      /* a device-side check failed (see mhs_read_status) */
+};
+
+/* Device-side status bits (mhs_read_status). */
+#define MHS_DEV_FOLD_GRID_OVERFLOW 1
+
+typedef struct mhs_request {
+  int kind;                  /* enum mhs_kind */
+  int order;                 /* 0, 1, 2 (P0, P1, P2) */
+  int fold;                  /* 1: fold surface-reaching sources (default) */
+  int subtract_eigenstress;  /* STRESS/STRAIN/TRACTION/INTERACTION */
+  int precision;             /* enum mhs_precision */
+  int out_f32;               /* 1: output stored as float32 */
+  int64_t n_obs, n_src;
+  const double* obs;         /* (n_obs, 3) */
+  const double* tris;        /* (n_src, 3, 3) */
+  const double* eps;         /* (n_src,) */
+  double mu, lam;
+  const double* normals;     /* TRACTION / INTERACTION: (n_obs, 3) unit */
+  const double* rec_basis;   /* INTERACTION: (n_obs, n_a, 3) */
+  const double* src_basis;   /* INTERACTION: (n_src, n_b, 3), or (n_cols, n_b, 3) with ids */
+  int n_a, n_b;
+  /* continuous layout: per-column gather plan built by mhs_column_plan */
+  const int64_t* ids;        /* (n_src, 6) or NULL (discontinuous) */
+  int64_t n_cols;
+  const int32_t* col_ptr;    /* (n_cols + 1,) */
+  const int32_t* col_ent;    /* (n_src * 6,) entries s * 6 + k, ascending s per column */
+  void* out;                 /* output, C-contiguous, zero not required */
+  void* workspace;
+  size_t workspace_bytes;
+} mhs_request;
+
+/* Bytes of workspace a request needs: *min_bytes for one observer row per
+ * pass, *good_bytes for the whole request in one pass (capped at 2 GiB). */
+int mhs_workspace_bytes(const mhs_request* req, size_t* min_bytes, size_t* good_bytes);
+
+/* Assemble req->out on `stream` (a cudaStream_t; NULL = legacy default).
+ * Returns MHS_OK once every kernel is queued; device-side checks are read
+ * later with mhs_read_status.  Replaces mhs.kernels.assemble's
+ * assemble_halfspace_disp / _total_stress / _traction, assemble_interaction
+ * and assemble_eigenstress (assemble.py:190-366) plus the eigenstress
+ * subtraction and strain readout of matrices.py:287-294 and :572-579. */
+int mhs_assemble(const mhs_request* req, void* stream);
+
+/* Synchronise `stream` and return the device status bits of the last
+ * request that used `workspace` (0 = clean), clearing them. */
+int mhs_read_status(void* workspace, void* stream, int* bits);
+
+/* Host helper: the per-column gather plan of a continuous layout from its
+ * (n_src, 6) ids (mhs/shared.py:175-273), entries in ascending source order
+ * so the sum runs in the order mhs's scatter-add does (assemble.py:69-93).
+ * col_ptr has n_cols + 1 entries, col_ent n_src * 6. */
+int mhs_column_plan(const int64_t* ids_host, int64_t n_src, int64_t n_cols, int32_t* col_ptr,
+                    int32_t* col_ent);
+
+/* Last error message of this thread. */
+const char* mhs_last_error(void);
+
+/* Library version string. */
+const char* mhs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MHS_B200_H */

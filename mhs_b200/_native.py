@@ -1,0 +1,91 @@
+"""ctypes binding of the CUDA library ``libmhs_b200.so`` (the C ABI in
+``include/mhs_b200.h``).  The library is built in-tree by ``build.py``; if it
+is missing the package refuses to run rather than falling back to anything
+else."""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+LIB_PATH = pathlib.Path(__file__).resolve().with_name("libmhs_b200.so")
+
+# enum mhs_kind
+DISP, STRESS, TOTAL_STRESS, EIGENSTRESS, STRAIN, TRACTION, INTERACTION = range(7)
+# enum mhs_precision
+FP64, MIXED = 0, 1
+# device status bits
+DEV_FOLD_GRID_OVERFLOW = 1
+
+
+class Request(ctypes.Structure):
+    """Mirror of ``struct mhs_request``."""
+
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("order", ctypes.c_int),
+        ("fold", ctypes.c_int),
+        ("subtract_eigenstress", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("out_f32", ctypes.c_int),
+        ("n_obs", ctypes.c_int64),
+        ("n_src", ctypes.c_int64),
+        ("obs", ctypes.c_void_p),
+        ("tris", ctypes.c_void_p),
+        ("eps", ctypes.c_void_p),
+        ("mu", ctypes.c_double),
+        ("lam", ctypes.c_double),
+        ("normals", ctypes.c_void_p),
+        ("rec_basis", ctypes.c_void_p),
+        ("src_basis", ctypes.c_void_p),
+        ("n_a", ctypes.c_int),
+        ("n_b", ctypes.c_int),
+        ("ids", ctypes.c_void_p),
+        ("n_cols", ctypes.c_int64),
+        ("col_ptr", ctypes.c_void_p),
+        ("col_ent", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("workspace", ctypes.c_void_p),
+        ("workspace_bytes", ctypes.c_size_t),
+    ]
+
+
+#: Symbols the header declares; a test checks the library exports each.
+EXPORTS = ("mhs_workspace_bytes", "mhs_assemble", "mhs_read_status", "mhs_column_plan",
+           "mhs_last_error", "mhs_version")
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH.name} is not built: run `python -c \"import __graft_entry__ as g; "
+            f"g.build()\"` (or mhs_b200.build.build()) first. There is no CPU fallback.")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    R = ctypes.POINTER(Request)
+    lib.mhs_workspace_bytes.argtypes = [R, ctypes.POINTER(ctypes.c_size_t),
+                                        ctypes.POINTER(ctypes.c_size_t)]
+    lib.mhs_workspace_bytes.restype = ctypes.c_int
+    lib.mhs_assemble.argtypes = [R, ctypes.c_void_p]
+    lib.mhs_assemble.restype = ctypes.c_int
+    lib.mhs_read_status.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    lib.mhs_read_status.restype = ctypes.c_int
+    lib.mhs_column_plan.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                    ctypes.c_void_p, ctypes.c_void_p]
+    lib.mhs_column_plan.restype = ctypes.c_int
+    lib.mhs_last_error.argtypes = []
+    lib.mhs_last_error.restype = ctypes.c_char_p
+    lib.mhs_version.argtypes = []
+    lib.mhs_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = load().mhs_last_error().decode(errors="replace")
+        raise RuntimeError(f"mhs_b200 native call failed (code {rc}): {msg}")

@@ -20,14 +20,18 @@
 namespace mhs {
 namespace tab_h {
 #define MHS_TBL static const
+#define MHS_TBLC static const
 #include "tables.inc"
 #undef MHS_TBL
+#undef MHS_TBLC
 }  // namespace tab_h
 #if defined(__CUDACC__)
 namespace tab_d {
 #define MHS_TBL static __constant__ const
+#define MHS_TBLC static __device__ const
 #include "tables.inc"
 #undef MHS_TBL
+#undef MHS_TBLC
 }  // namespace tab_d
 #endif
 }  // namespace mhs
@@ -112,7 +116,7 @@ struct Spec {
 // at degree D consumes M_{n-2} at degree D-2 down to the lowest odd n, and
 // the vertical seeds need I_3 and every I_m between (mhs/fullspace/
 // moments.py:94-116, restated).
-constexpr Spec make_spec(int d1, int d3, int d5, int d7, int d9, int order) {
+MHS_FI constexpr Spec make_spec(int d1, int d3, int d5, int d7, int d9, int order) {
   Spec s{};
   s.order = order;
   const int in0[NS] = {-1, d1, d3, d5, d7, d9};

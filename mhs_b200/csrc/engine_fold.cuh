@@ -165,8 +165,18 @@ struct AngRule {
   int npiece;
   double a[4], b[4];
   int m[4];        // intervals per piece
-  int n;           // total nodes = FOLD_N_ANGULAR * sum(m)
+  int n;           // total nodes = FOLD_N_ANGULAR * sum(m); -1 past the cap
 };
+
+// Intervals per angular piece beyond which a grid is refused (a source
+// millions of eps across); keeps every count inside int range.
+constexpr double FOLD_MAX_INTERVALS = 1 << 20;
+
+// ceil(v) as an int, or -1 when v is not a finite count below the cap.
+MHS_FI int fold_count(double v) {
+  const double c = ceil(v);
+  return (c >= 0.0 && c <= FOLD_MAX_INTERVALS) ? (int)c : -1;
+}
 
 MHS_HD void fold_angular(double theta_c, double w_fine, double w_med, double rb, double eps,
                          AngRule& A) {
@@ -176,7 +186,8 @@ MHS_HD void fold_angular(double theta_c, double w_fine, double w_med, double rb,
   A.n = 0;
   if (w_fine >= cst::PI || w_med >= cst::PI) {
     const double sp = w_fine >= cst::PI ? cst::FOLD_FINE_SPACING_EPS : cst::FOLD_MEDIUM_SPACING_EPS;
-    int m = (int)ceil(two_pi * rb / ((double)n * sp * eps));
+    int m = fold_count(two_pi * rb / ((double)n * sp * eps));
+    if (m < 0) { A.n = -1; return; }
     if (m < 8) m = 8;
     A.a[0] = 0.0;
     A.b[0] = two_pi;
@@ -189,7 +200,8 @@ MHS_HD void fold_angular(double theta_c, double w_fine, double w_med, double rb,
   int pm[4], np = 0;
   int mid_first = -1;
   if (w_fine > 0.0) {
-    int m = (int)ceil(2.0 * w_fine * rb / ((double)n * cst::FOLD_FINE_SPACING_EPS * eps));
+    int m = fold_count(2.0 * w_fine * rb / ((double)n * cst::FOLD_FINE_SPACING_EPS * eps));
+    if (m < 0) { A.n = -1; return; }
     if (m < 1) m = 1;
     pa[np] = theta_c - w_fine;
     pb[np] = theta_c + w_fine;
@@ -198,7 +210,8 @@ MHS_HD void fold_angular(double theta_c, double w_fine, double w_med, double rb,
     ++np;
   }
   if (w_med > w_fine) {
-    int m = (int)ceil((w_med - w_fine) * rb / ((double)n * cst::FOLD_MEDIUM_SPACING_EPS * eps));
+    int m = fold_count((w_med - w_fine) * rb / ((double)n * cst::FOLD_MEDIUM_SPACING_EPS * eps));
+    if (m < 0) { A.n = -1; return; }
     if (m < 1) m = 1;
     // insert the left flank before the fine sector, append the right one
     for (int i = np; i > 0; --i) {
@@ -266,7 +279,9 @@ MHS_HD int fold_breaks(double rho_s, double zeta, double r_f, double eps, double
   for (int s = 0; s < 3; ++s) {
     const double a0 = a0s[s], b0 = b0s[s];
     if (!(b0 > a0)) continue;
-    int m = (int)ceil((b0 - a0) / (ws[s] * eps));
+    const double md = ceil((b0 - a0) / (ws[s] * eps));
+    if (!(md <= (double)FOLD_MAX_BREAKS)) return -1;
+    int m = (int)md;
     if (m < 1) m = 1;
     if (nb + m + 1 > FOLD_MAX_BREAKS) return -1;
     for (int i = 0; i <= m; ++i) br[nb++] = linspace_at(a0, b0, m + 1, i);
@@ -380,6 +395,7 @@ MHS_HD int fold_boussinesq_scalar(const Frame& f, const QuadRule& r12, const Qua
     if (rb - ra < 1e-9 * eps) continue;
     AngRule A;
     fold_panel_rule(fp, ra, rb, A);
+    if (A.n < 0) return -1;
     for (int ir = 0; ir < cst::FOLD_N_RADIAL; ++ir) {
       const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
       const double wr = (rb - ra) * (0.5 * gw6[ir]);

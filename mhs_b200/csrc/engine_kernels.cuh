@@ -26,7 +26,8 @@ template <int P, int WANT> struct DirectSpec {
 // (-1)^(ca+cb) z^cc W_n(ca, cb).
 template <class S>
 MHS_FI double lift_local(const double* W, int s, int ca, int cb, int cc, const double* zp) {
-  const double v = zp[cc] * W[S::spec.w_off[s] + tri_idx(ca, cb)];
+  constexpr Spec sp = S::spec;
+  const double v = zp[cc] * W[sp.w_off[s] + tri_idx(ca, cb)];
   return ((ca + cb) & 1) ? -v : v;
 }
 
@@ -65,10 +66,10 @@ MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, cons
                      double* U) {
   double zp[4] = {1.0, z, z * z, z * z * z};
   const int s3 = nslot(3), s5 = nslot(5);
-  const double V3[3] = {-W[S::spec.w_off[s3] + tri_idx(1, 0)], -W[S::spec.w_off[s3] + tri_idx(0, 1)],
-                        z * W[S::spec.w_off[s3]]};
-  const double V5[3] = {-W[S::spec.w_off[s5] + tri_idx(1, 0)], -W[S::spec.w_off[s5] + tri_idx(0, 1)],
-                        z * W[S::spec.w_off[s5]]};
+  constexpr Spec sp = S::spec;
+  constexpr int o3 = sp.w_off[nslot(3)], o5 = sp.w_off[nslot(5)];
+  const double V3[3] = {-W[o3 + tri_idx(1, 0)], -W[o3 + tri_idx(0, 1)], z * W[o3]};
+  const double V5[3] = {-W[o5 + tri_idx(1, 0)], -W[o5 + tri_idx(0, 1)], z * W[o5]};
   const double e2 = eps * eps;
   const double f6 = 6.0 * m.one_m_nu * e2;
   double G1[3][3][3];
@@ -99,8 +100,9 @@ MHS_HD void kernel_H(const Frame& f, const double* W, double z, double eps, cons
                      double* H) {
   double zp[5] = {1.0, z, z * z, z * z * z, z * z * z * z};
   const int s3 = nslot(3), s5 = nslot(5), s7 = nslot(7);
-  const double I3 = W[S::spec.w_off[s3]];
-  const double I5 = W[S::spec.w_off[s5]];
+  constexpr Spec sp = S::spec;
+  const double I3 = W[sp.w_off[nslot(3)]];
+  const double I5 = W[sp.w_off[nslot(5)]];
   const double e2 = eps * eps;
   const double f2 = 2.0 * m.one_m_nu * e2;
   double T25[3][3], T27[3][3];

@@ -120,19 +120,19 @@ MHS_HD void edge_small(double ua, double ub, double rho, double P[MS][8]) {
 }
 
 // Exponent range q = k - m + 1 - 2 t of the large-|u| series over a spec.
-constexpr int series_qhi(const Spec& sp) {
+MHS_FI constexpr int series_qhi(const Spec& sp) {
   int q = -999;
   for (int j = 0; j < MS; ++j)
     if (sp.edge[j] >= 0) q = imax(q, sp.edge[j] - (2 * j - 1) + 1);
   return q;
 }
-constexpr int series_qlo(const Spec& sp) {
+MHS_FI constexpr int series_qlo(const Spec& sp) {
   int q = 999;
   for (int j = 0; j < MS; ++j)
     if (sp.edge[j] >= 0) q = imin(q, 0 - (2 * j - 1) + 1);
   return q - 2 * (cst::SERIES_TERMS - 1);
 }
-constexpr int spec_max_need0(const Spec& sp) {
+MHS_FI constexpr int spec_max_need0(const Spec& sp) {
   int d = 0;
   for (int s = 0; s < NS; ++s) d = imax(d, sp.need0[s]);
   return d;
@@ -208,10 +208,15 @@ MHS_HD void edge_table(double ua, double ub, double rho2, double P[MS][8]) {
 // by the horizontal recursion (mhs/fullspace/moments.py:171-355).
 template <class S>
 struct MomentTable {
-  static constexpr Spec sp = S::spec;
-  double M[sp.m_off[NS] > 0 ? sp.m_off[NS] : 1];
-  MHS_FI double& at(int s, int a, int b) { return M[sp.m_off[s] + tri_idx(a, b)]; }
-  MHS_FI double at(int s, int a, int b) const { return M[sp.m_off[s] + tri_idx(a, b)]; }
+  double M[S::spec.m_off[NS] > 0 ? S::spec.m_off[NS] : 1];
+  MHS_FI double& at(int s, int a, int b) {
+    constexpr Spec sp = S::spec;
+    return M[sp.m_off[s] + tri_idx(a, b)];
+  }
+  MHS_FI double at(int s, int a, int b) const {
+    constexpr Spec sp = S::spec;
+    return M[sp.m_off[s] + tri_idx(a, b)];
+  }
 };
 
 // Van Oosterom-Strackee solid angle of the triangle seen from the point at

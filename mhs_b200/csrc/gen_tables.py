@@ -66,7 +66,8 @@ def main(src: str) -> None:
     lines = ["// GENERATED by gen_tables.py -- do not edit by hand.",
              "// Image-family coefficients re-laid out from mhs's generated table",
              "// (mhs/kernels/_image_table.py); binomial series constants exact.",
-             "// Included once per address space: MHS_TBL is the storage qualifier.", ""]
+             "// Included once per address space: MHS_TBL is the storage qualifier of",
+             "// the kernel-time tables, MHS_TBLC of the per-material coefficients.", ""]
 
     # ---------------- R family ----------------
     rmono = set()
@@ -104,7 +105,7 @@ def main(src: str) -> None:
         lines += [f"  {{{m}, {s}}}," for m, s, _ in rows]
         lines.append("};")
         lines.append(f"// c[pz][pnu]: coefficient of z^pz nu^pnu")
-        lines.append(f"MHS_TBL double mhs_r_{name.lower()}_c[MHS_R_N{name}][3][3] = {{")
+        lines.append(f"MHS_TBLC double mhs_r_{name.lower()}_c[MHS_R_N{name}][3][3] = {{")
         for _, _, c in rows:
             lines.append("  {" + ", ".join(
                 "{" + ", ".join(_num(v) for v in row) + "}" for row in c) + "},")
@@ -139,7 +140,7 @@ def main(src: str) -> None:
         lines.append(f"MHS_TBL short mhs_q_{name.lower()}_idx[MHS_Q_N{name}][2] = {{")
         lines += [f"  {{{m}, {s}}}," for m, s, _ in rows]
         lines.append("};")
-        lines.append(f"MHS_TBL double mhs_q_{name.lower()}_c[MHS_Q_N{name}][3] = {{")
+        lines.append(f"MHS_TBLC double mhs_q_{name.lower()}_c[MHS_Q_N{name}][3] = {{")
         lines += ["  {" + ", ".join(_num(v) for v in c) + "}," for _, _, c in rows]
         lines.append("};")
 

@@ -1,0 +1,966 @@
+// CUDA kernels and C ABI of the B200 Green's-function assembler.
+//
+// One request runs as a short pipeline on the caller's stream, per chunk of
+// observers:
+//   k_coef   per-material image coefficients (once per request)
+//   k_prep   per-source frames, reflected frames, basis products, fold data
+//   k_pair   one thread per (observer, source): direct term + image R-family,
+//            per-source quadrature rules staged in shared memory
+//   k_imageq one thread per (observer, source): image Q-family
+//   k_band   per straddling source, the ordered list of band receivers
+//   k_fold   one warp per band pair: mirror element + Boussinesq surface
+//            quadrature over the receiver's polar grid, 32 nodes per step
+//   k_final  one thread per (observer, output column): eigenstress,
+//            traction / interaction contraction, continuous-layout gather,
+//            and the store in the caller's layout
+// Per-pair tensors travel between stages in an element-major scratch table
+// (workspace), so every stage writes disjoint rows and no result depends on
+// atomics or scheduling order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/mhs_b200.h"
+#include "engine_fold.cuh"
+#include "host_prep.h"
+
+using namespace mhs;
+
+namespace {
+
+// ------------------------------------------------------------ device data
+__device__ double d_glx[GL_TABLE];
+__device__ double d_glw[GL_TABLE];
+
+struct SrcPrep {
+  Frame f;        // element
+  Frame fi;       // reflected element (image R-family and fold mirror)
+  double eps;
+  double centre[2], r_f, diam;
+  int straddle;   // folded (fold requested and the source reaches the band)
+  int pad;
+};
+
+constexpr int TB = 128;          // threads per block for pair-parallel kernels
+constexpr int FOLD_WARPS = 4;    // band pairs per fold block (one source)
+constexpr int QFLOOR = cst::IMAGE_Q_GAUSS_MIN;
+
+enum : int { KD_DISP = 0, KD_HE = 1, KD_E = 2 };   // what the stages compute
+
+MHS_FI constexpr int kind_class(int kind) {
+  return kind == MHS_DISP ? KD_DISP : (kind == MHS_EIGENSTRESS ? KD_E : KD_HE);
+}
+MHS_FI constexpr int comps_of(int kc) { return kc == KD_DISP ? 9 : (kc == KD_HE ? 27 : 0); }
+// Scratch row per (observer, source, node): tensor comps, phi, phi_mirror.
+MHS_FI constexpr int row_of(int kc) { return comps_of(kc) + 2; }
+
+// --------------------------------------------------------------- helpers
+__device__ __forceinline__ void atomic_status(int* st, int bits) { atomicOr(st, bits); }
+
+// One node of the collapsed Gauss product rule of order n (q = i * n + j).
+template <int P>
+__device__ __forceinline__ void rule_node(const Frame& f, int n, int q, double& e0, double& e1,
+                                          double& wq, double* N) {
+  const double* x = d_glx + gl_offset(n);
+  const double* w = d_glw + gl_offset(n);
+  const int i = q / n, j = q % n;
+  const double gi = 0.5 * (x[i] + 1.0), wi = 0.5 * w[i];
+  const double gj = 0.5 * (x[j] + 1.0), wj = 0.5 * w[j];
+  const double x1 = gi, x2 = gj * (1.0 - gi);
+  const double ww = wi * wj * (1.0 - gi);
+  const double l0 = 1.0 - x1 - x2;
+  e0 = (l0 * f.p[0][0] + x1 * f.p[1][0]) + x2 * f.p[2][0];
+  e1 = (l0 * f.p[0][1] + x1 * f.p[1][1]) + x2 * f.p[2][1];
+  wq = ww * (2.0 * f.area);
+  shape_at<P>(f, e0, e1, N);
+}
+
+// Shared-memory far-field rules of one frame (orders 12 and 8).
+template <int P>
+struct SmemRules {
+  static constexpr int K = n_nodes(P);
+  static constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
+  static constexpr int N8 = cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
+  double e0[N12 + N8], e1[N12 + N8], wq[N12 + N8], Nq[(N12 + N8) * K];
+  __device__ void build(const Frame& f, int tid, int nthr) {
+    for (int t = tid; t < N12 + N8; t += nthr) {
+      const int n = t < N12 ? cst::FAR_GAUSS_N : cst::FAR_GAUSS_N_DISTANT;
+      const int q = t < N12 ? t : t - N12;
+      rule_node<P>(f, n, q, e0[t], e1[t], wq[t], Nq + t * K);
+    }
+  }
+  __device__ QuadRule r12() const { return QuadRule{N12, e0, e1, wq, Nq}; }
+  __device__ QuadRule r8() const { return QuadRule{N8, e0 + N12, e1 + N12, wq + N12, Nq + N12 * K}; }
+};
+
+// ---------------------------------------------------------------- k_coef
+__global__ void k_coef(double mu, double lam, double* out) {
+  const Material m = make_material(mu, lam);
+  const double nu = m.nu_i, s = m.scale_c;
+  const double nup[3] = {1.0, nu, nu * nu};
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double* r_dg = out;
+  double* r_ddg = r_dg + 3 * MHS_R_NDG;
+  double* q_dg = r_ddg + 3 * MHS_R_NDDG;
+  double* q_ddg = q_dg + MHS_Q_NDG;
+  if (t < MHS_R_NDG)
+    for (int pz = 0; pz < 3; ++pz) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += tab_d::mhs_r_dg_c[t][pz][k] * nup[k];
+      r_dg[3 * t + pz] = v * s;
+    }
+  if (t < MHS_R_NDDG)
+    for (int pz = 0; pz < 3; ++pz) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += tab_d::mhs_r_ddg_c[t][pz][k] * nup[k];
+      r_ddg[3 * t + pz] = v * s;
+    }
+  if (t < MHS_Q_NDG) {
+    double v = 0.0;
+    for (int k = 0; k < 3; ++k) v += tab_d::mhs_q_dg_c[t][k] * nup[k];
+    q_dg[t] = v;
+  }
+  if (t < MHS_Q_NDDG) {
+    double v = 0.0;
+    for (int k = 0; k < 3; ++k) v += tab_d::mhs_q_ddg_c[t][k] * nup[k];
+    q_ddg[t] = v;
+  }
+}
+
+// ---------------------------------------------------------------- k_prep
+__global__ void k_prep(int64_t n_src, const double* __restrict__ tris,
+                       const double* __restrict__ eps, int fold, int want_g,
+                       SrcPrep* __restrict__ prep, double* __restrict__ G) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n_src) return;
+  SrcPrep p;
+  const double* t = tris + 9 * s;
+  double ti[9];
+  for (int i = 0; i < 9; ++i) ti[i] = (i % 3 == 2) ? -t[i] : t[i];
+  make_frame(t, p.f);
+  make_frame(ti, p.fi);
+  p.eps = eps[s];
+  fold_crease(t, p.eps, p.centre, &p.r_f);
+  p.diam = tri_diameter(t);
+  p.straddle = (fold && fold_straddles(t, p.eps)) ? 1 : 0;
+  p.pad = 0;
+  prep[s] = p;
+  if (want_g) build_basis_products(p.fi, G + s * G_SIZE);
+}
+
+// ---------------------------------------------------------------- k_pair
+// Direct term and image R-family of one (observer, source) pair.
+template <int P, int KC>
+__global__ void __launch_bounds__(TB)
+k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
+       const SrcPrep* __restrict__ prep, const double* __restrict__ Gall,
+       const double* __restrict__ coef, double mu, double lam, double* __restrict__ T) {
+  constexpr int K = n_nodes(P);
+  constexpr int NR = row_of(KC);
+  constexpr bool IMG = KC != KD_E;
+  const int64_t s = blockIdx.y;
+  __shared__ SrcPrep sp;
+  __shared__ SmemRules<P> rd;
+  __shared__ SmemRules<IMG ? P : 0> ri;
+  __shared__ double sG[IMG ? G_SIZE : 1];
+  if (threadIdx.x == 0) sp = prep[s];
+  __syncthreads();
+  rd.build(sp.f, threadIdx.x, TB);
+  if (IMG) {
+    ri.build(sp.fi, threadIdx.x, TB);
+    for (int i = threadIdx.x; i < G_SIZE; i += TB) sG[i] = Gall[s * G_SIZE + i];
+  }
+  __syncthreads();
+  const int64_t oc = blockIdx.x * (int64_t)TB + threadIdx.x;
+  if (oc >= n_chunk) return;
+  const int64_t o = lo + oc;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  const Material m = make_material(mu, lam);
+  const double eps = sp.eps;
+  double* row = T + ((oc * n_src + s) * K) * NR;
+  if constexpr (KC == KD_E) {
+    double E[K];
+    direct_eval<P, W_E>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
+    for (int k = 0; k < K; ++k) {
+      row[k * NR + 0] = E[k];
+      row[k * NR + 1] = 0.0;
+    }
+    return;
+  } else {
+    constexpr int C = comps_of(KC);
+    double A[K * C], E[K];
+    if constexpr (KC == KD_DISP)
+      direct_eval<P, W_U>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
+    else
+      direct_eval<P, W_H | W_E>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
+    const bool band = sp.straddle && fold_band(x, sp.centre, eps);
+    if (!band) {
+      double B[K * C];
+      const ImageCoef ic = image_coef_view(coef);
+      if constexpr (KC == KD_DISP)
+        image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
+      else
+        image_r_eval<P, W_H>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, nullptr, B);
+      for (int i = 0; i < K * C; ++i) A[i] += B[i];
+    }
+    for (int k = 0; k < K; ++k) {
+      for (int c = 0; c < C; ++c) row[k * NR + c] = A[k * C + c];
+      row[k * NR + C] = (KC == KD_HE) ? E[k] : 0.0;
+      row[k * NR + C + 1] = 0.0;
+    }
+  }
+}
+
+// -------------------------------------------------------------- k_imageq
+// Image Q-family of one pair, added to the scratch row.  The floor order
+// (8 x 8 points, almost every pair) reads a shared-memory rule; higher
+// orders generate their nodes on the fly.
+template <int P>
+struct QRuleSmem {
+  static constexpr int K = n_nodes(P);
+  const double* y;
+  const double* wN;
+  int nq;
+  __device__ int count() const { return nq; }
+  __device__ void node(int t, double* yy, double* w) const {
+    yy[0] = y[3 * t];
+    yy[1] = y[3 * t + 1];
+    yy[2] = y[3 * t + 2];
+    for (int k = 0; k < K; ++k) w[k] = wN[t * K + k];
+  }
+};
+
+template <int P>
+struct QRuleFly {
+  static constexpr int K = n_nodes(P);
+  const Frame* f;
+  int n;
+  __device__ int count() const { return n * n; }
+  __device__ void node(int t, double* yy, double* w) const {
+    double e0, e1, wq, N[K];
+    rule_node<P>(*f, n, t, e0, e1, wq, N);
+    // Cartesian node on the real element: barycentric (l0, x1, x2) @ tri
+    const double* x = d_glx + gl_offset(n);
+    const int i = t / n, j = t % n;
+    const double gi = 0.5 * (x[i] + 1.0), gj = 0.5 * (x[j] + 1.0);
+    const double x1 = gi, x2 = gj * (1.0 - gi), l0 = 1.0 - x1 - x2;
+    for (int c = 0; c < 3; ++c) yy[c] = (l0 * f->v[0][c] + x1 * f->v[1][c]) + x2 * f->v[2][c];
+    for (int k = 0; k < K; ++k) w[k] = wq * N[k];
+  }
+};
+
+template <int P, int WANT, class Rule>
+__device__ void image_q_rule(const Rule& q, const double* nrm, const double* x, double eps,
+                             const Material& m, const ImageCoef& ic, double* U, double* H) {
+  constexpr int K = n_nodes(P);
+  double basis[MHS_Q_NMONO][K];
+  for (int i = 0; i < MHS_Q_NMONO; ++i)
+    for (int k = 0; k < K; ++k) basis[i][k] = 0.0;
+  const double e2 = eps * eps;
+  const int nq = q.count();
+  for (int t = 0; t < nq; ++t) {
+    double y[3], wN[K];
+    q.node(t, y, wN);
+    const double d1 = x[0] - y[0];
+    const double d2 = x[1] - y[1];
+    const double d3 = x[2] + y[2];
+    const double r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
+    const double ir = 1.0 / r2, iq = 1.0 / (r2 - d3);
+    double p1[5], p2[5], p3[5], pr[8], pq[5];
+    p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
+#pragma unroll
+    for (int i = 2; i < 5; ++i) {
+      p1[i] = p1[i - 1] * d1;
+      p2[i] = p2[i - 1] * d2;
+      p3[i] = p3[i - 1] * d3;
+      pq[i] = pq[i - 1] * iq;
+    }
+#pragma unroll
+    for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
+#pragma unroll 4
+    for (int mi = 0; mi < MHS_Q_NMONO; ++mi) {
+      const int* e = tab_d::mhs_q_mono[mi];
+      double v = 1.0;
+      bool first = true;
+      if (e[0]) { v = p1[e[0]]; first = false; }
+      if (e[1]) { v = first ? p2[e[1]] : v * p2[e[1]]; first = false; }
+      if (e[2]) { v = first ? p3[e[2]] : v * p3[e[2]]; first = false; }
+      if (e[3]) { v = first ? pr[e[3]] : v * pr[e[3]]; first = false; }
+      if (e[4]) { v = first ? pq[e[4]] : v * pq[e[4]]; first = false; }
+      for (int k = 0; k < K; ++k) basis[mi][k] += v * wN[k];
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    if (WANT & W_U) {
+      double DG[27];
+      for (int i = 0; i < 27; ++i) DG[i] = 0.0;
+      for (int r = 0; r < MHS_Q_NDG; ++r)
+        DG[tab_d::mhs_q_dg_idx[r][1]] += ic.q_dg[r] * basis[tab_d::mhs_q_dg_idx[r][0]][k];
+      for (int i = 0; i < 27; ++i) DG[i] *= m.scale_c;
+      contract_dg(DG, nrm, m, U + 9 * k);
+    }
+    if (WANT & W_H) {
+      double DDG[81];
+      for (int i = 0; i < 81; ++i) DDG[i] = 0.0;
+      for (int r = 0; r < MHS_Q_NDDG; ++r)
+        DDG[tab_d::mhs_q_ddg_idx[r][1]] += ic.q_ddg[r] * basis[tab_d::mhs_q_ddg_idx[r][0]][k];
+      for (int i = 0; i < 81; ++i) DDG[i] *= m.scale_c;
+      contract_ddg(DDG, nrm, m, H + 27 * k);
+    }
+  }
+}
+
+template <int P, int KC>
+__global__ void __launch_bounds__(TB)
+k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
+         const SrcPrep* __restrict__ prep, const double* __restrict__ coef, double mu, double lam,
+         double* __restrict__ T) {
+  constexpr int K = n_nodes(P);
+  constexpr int NR = row_of(KC);
+  constexpr int C = comps_of(KC);
+  const int64_t s = blockIdx.y;
+  __shared__ SrcPrep sp;
+  __shared__ double qy[QFLOOR * QFLOOR * 3];
+  __shared__ double qw[QFLOOR * QFLOOR * K];
+  if (threadIdx.x == 0) sp = prep[s];
+  __syncthreads();
+  {
+    QRuleFly<P> fly{&sp.f, QFLOOR};
+    for (int t = threadIdx.x; t < QFLOOR * QFLOOR; t += TB) fly.node(t, qy + 3 * t, qw + K * t);
+  }
+  __syncthreads();
+  const int64_t oc = blockIdx.x * (int64_t)TB + threadIdx.x;
+  if (oc >= n_chunk) return;
+  const int64_t o = lo + oc;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  const double eps = sp.eps;
+  if (sp.straddle && fold_band(x, sp.centre, eps)) return;
+  const Material m = make_material(mu, lam);
+  const ImageCoef ic = image_coef_view(coef);
+  double ti[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) ti[3 * i + j] = sp.fi.v[i][j];
+  const int n = q_gauss_order(x, ti, eps, sp.f.L, P);
+  double B[K * C];
+  constexpr int WANT = KC == KD_DISP ? W_U : W_H;
+  if (n == QFLOOR) {
+    QRuleSmem<P> r{qy, qw, QFLOOR * QFLOOR};
+    image_q_rule<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
+  } else {
+    QRuleFly<P> r{&sp.f, n};
+    image_q_rule<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
+  }
+  double* row = T + ((oc * n_src + s) * K) * NR;
+  for (int k = 0; k < K; ++k)
+    for (int c = 0; c < C; ++c) row[k * NR + c] += B[k * C + c];
+}
+
+// ---------------------------------------------------------------- k_band
+// Ordered list of the band receivers of each straddling source, in slots
+// [s * n_chunk, s * n_chunk + cnt[s]).
+__global__ void __launch_bounds__(256)
+k_band(int64_t lo, int64_t n_chunk, const double* __restrict__ obs,
+       const SrcPrep* __restrict__ prep, int* __restrict__ cnt, int* __restrict__ list) {
+  const int64_t s = blockIdx.x;
+  __shared__ int warp_n[8];
+  __shared__ int base;
+  const SrcPrep& p = prep[s];
+  if (!p.straddle) {
+    if (threadIdx.x == 0) cnt[s] = 0;
+    return;
+  }
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t t0 = 0; t0 < n_chunk; t0 += 256) {
+    const int64_t oc = t0 + threadIdx.x;
+    bool pred = false;
+    if (oc < n_chunk) {
+      const double x[3] = {obs[3 * (lo + oc)], obs[3 * (lo + oc) + 1], obs[3 * (lo + oc) + 2]};
+      pred = fold_band(x, p.centre, p.eps);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, pred);
+    if (lane == 0) warp_n[wid] = __popc(bal);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < wid; ++w) off += warp_n[w];
+    if (pred) list[s * n_chunk + off + __popc(bal & ((1u << lane) - 1u))] = (int)oc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int w = 0; w < 8; ++w) tot += warp_n[w];
+      base += tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) cnt[s] = base;
+}
+
+// ---------------------------------------------------------------- k_fold
+template <int P, int KC>
+struct FoldShared {
+  static constexpr int K = n_nodes(P);
+  static constexpr int NC = KC == KD_HE ? 6 : 3;
+  static constexpr int NJ = 3 * K;
+  static constexpr int NOUT = NC * NJ;
+  SrcPrep sp;
+  SmemRules<P> rd;       // element (surface load)
+  SmemRules<P> rm;       // mirror element (its full-space field)
+  double brk[FOLD_WARPS][FOLD_MAX_BREAKS];
+  double sh_load[FOLD_WARPS][NJ];
+  double sB[FOLD_WARPS][32][NC];
+  double sS[FOLD_WARPS][32][NJ + 1];
+  double sR1[FOLD_WARPS];
+  double outv[FOLD_WARPS][NOUT];
+  int sbrk_n[FOLD_WARPS];
+};
+
+// One warp per band pair.  Lanes evaluate 32 grid nodes at a time (each a
+// full-space H + E of the source at a surface point); the weighted
+// point-load tensor and the load difference go through shared memory and
+// each lane accumulates a fixed subset of the (component x node x slip)
+// products, so the sum has a fixed order.
+template <int P, int KC>
+__global__ void __launch_bounds__(32 * FOLD_WARPS)
+k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
+       const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
+       const int* __restrict__ list, double mu, double lam, double* __restrict__ T,
+       int* __restrict__ status) {
+  constexpr int K = n_nodes(P);
+  constexpr int NR = row_of(KC);
+  constexpr int C = comps_of(KC);
+  constexpr bool WH = KC == KD_HE;
+  constexpr int NC = WH ? 6 : 3;          // point-load components
+  constexpr int NJ = 3 * K;               // load components (node x slip)
+  constexpr int NOUT = NC * NJ;
+  constexpr int PER_LANE = (NOUT + 31) / 32;
+  const int64_t s = blockIdx.y;
+  const int n_band = cnt[s];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if ((int64_t)blockIdx.x * FOLD_WARPS >= n_band) return;
+  extern __shared__ __align__(16) unsigned char fold_smem[];
+  FoldShared<P, KC>& sh = *reinterpret_cast<FoldShared<P, KC>*>(fold_smem);
+  SrcPrep& sp = sh.sp;
+  SmemRules<P>& rd = sh.rd;
+  SmemRules<P>& rm = sh.rm;
+  auto& brk = sh.brk;
+  auto& sh_load = sh.sh_load;
+  auto& sB = sh.sB;
+  auto& sS = sh.sS;
+  auto& sbrk_n = sh.sbrk_n;
+  auto& sR1 = sh.sR1;
+  auto& outv = sh.outv;
+  if (threadIdx.x == 0) sp = prep[s];
+  __syncthreads();
+  rd.build(sp.f, threadIdx.x, 32 * FOLD_WARPS);
+  rm.build(sp.fi, threadIdx.x, 32 * FOLD_WARPS);
+  __syncthreads();
+  const int bi = blockIdx.x * FOLD_WARPS + wid;
+  if (bi >= n_band) return;
+  const int64_t oc = list[s * n_chunk + bi];
+  const int64_t o = lo + oc;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  const Material m = make_material(mu, lam);
+  const double eps = sp.eps;
+  double* row = T + ((oc * n_src + s) * K) * NR;
+  const QuadRule r12 = rd.r12(), r8 = rd.r8();
+  if constexpr (KC == KD_E) {
+    if (lane == 0) {
+      double E[K];
+      direct_eval<P, W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, nullptr, E);
+      for (int k = 0; k < K; ++k) row[k * NR + 1] = E[k];
+    }
+    return;
+  } else {
+    FoldPair fp;
+    fold_pair_setup(x, sp.centre, sp.r_f, eps, fp);
+    if (lane == 0) {
+      double R1;
+      sbrk_n[wid] = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, brk[wid], &R1);
+      sR1[wid] = R1;
+      double sl[NJ];
+      fold_surface_load<P>(sp.f, r12, r8, x[0], x[1], eps, m, sl);
+      for (int j = 0; j < NJ; ++j) sh_load[wid][j] = sl[j];
+    }
+    __syncwarp();
+    const int nb = sbrk_n[wid];
+    if (nb < 0) {
+      if (lane == 0) atomic_status(status, MHS_DEV_FOLD_GRID_OVERFLOW);
+      return;
+    }
+    fp.R1 = sR1[wid];
+    const double* gx6 = d_glx + gl_offset(cst::FOLD_N_RADIAL);
+    const double* gw6 = d_glw + gl_offset(cst::FOLD_N_RADIAL);
+    const double* gx4 = d_glx + gl_offset(cst::FOLD_N_ANGULAR);
+    const double* gw4 = d_glw + gl_offset(cst::FOLD_N_ANGULAR);
+    double acc[PER_LANE];
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) acc[i] = 0.0;
+    for (int pi = 0; pi + 1 < nb; ++pi) {
+      const double ra = brk[wid][pi], rb = brk[wid][pi + 1];
+      if (rb - ra < 1e-9 * eps) continue;
+      AngRule A;
+      fold_panel_rule(fp, ra, rb, A);
+      if (A.n < 0) {  // uniform across the warp: every lane built the same rule
+        if (lane == 0) atomic_status(status, MHS_DEV_FOLD_GRID_OVERFLOW);
+        return;
+      }
+      const int npts = cst::FOLD_N_RADIAL * A.n;
+      for (int b0 = 0; b0 < npts; b0 += 32) {
+        const int t = b0 + lane;
+        double Bv[NC], sv[NJ];
+        if (t < npts) {
+          const int ir = t / A.n, j = t % A.n;
+          const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
+          const double wr = (rb - ra) * (0.5 * gw6[ir]);
+          double th, wt;
+          fold_ang_node(A, gx4, gw4, j, &th, &wt);
+          const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
+          const double w = wr * wt * R;
+          fold_surface_load<P>(sp.f, r12, r8, px, py, eps, m, sv);
+          if (WH) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, Bv);
+          else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, Bv);
+          for (int c = 0; c < NC; ++c) sB[wid][lane][c] = w * Bv[c];
+          for (int jj = 0; jj < NJ; ++jj) sS[wid][lane][jj] = sv[jj] - sh_load[wid][jj];
+        } else {
+          for (int c = 0; c < NC; ++c) sB[wid][lane][c] = 0.0;
+          for (int jj = 0; jj < NJ; ++jj) sS[wid][lane][jj] = 0.0;
+        }
+        __syncwarp();
+        const int nvalid = min(32, npts - b0);
+#pragma unroll
+        for (int i = 0; i < PER_LANE; ++i) {
+          const int oi = lane + 32 * i;
+          if (oi < NOUT) {
+            const int c = oi / NJ, jj = oi % NJ;
+            double a = acc[i];
+            for (int u = 0; u < nvalid; ++u) a += sB[wid][u][c] * sS[wid][u][jj];
+            acc[i] = a;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    // gather the lane partials into the scratch row
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) {
+      const int oi = lane + 32 * i;
+      if (oi < NOUT) outv[wid][oi] = acc[i];
+    }
+    __syncwarp();
+    if (lane == 0) {
+      double Mv[K * C], E[K];
+      if constexpr (WH) {
+        direct_eval<P, W_H | W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, Mv, E);
+        double srr, szz;
+        disk_stress(fp.R1, fp.zeta, m.nu_f, &srr, &szz);
+        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+        for (int k = 0; k < K; ++k)
+          for (int mm = 0; mm < 3; ++mm) {
+            double Hb[3][3];
+            for (int c = 0; c < 6; ++c) {
+              const double v = outv[wid][c * NJ + 3 * k + mm];
+              Hb[ia[c]][ib[c]] = v;
+              Hb[ib[c]][ia[c]] = v;
+            }
+            const double shv = sh_load[wid][3 * k + mm];
+            Hb[0][0] += shv * srr;
+            Hb[1][1] += shv * srr;
+            Hb[2][2] += shv * szz;
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b)
+                row[k * NR + 9 * a + 3 * b + mm] +=
+                    Mv[27 * k + 9 * a + 3 * b + mm] * mirror_slip_sign(mm) + Hb[a][b];
+          }
+        for (int k = 0; k < K; ++k) row[k * NR + C + 1] = E[k];
+      } else {
+        direct_eval<P, W_U>(sp.fi, rm.r12(), rm.r8(), x, eps, m, Mv, nullptr, nullptr);
+        const double uz = disk_disp_z(fp.R1, fp.zeta, m.mu, m.nu_f);
+        for (int k = 0; k < K; ++k)
+          for (int mm = 0; mm < 3; ++mm)
+            for (int i = 0; i < 3; ++i) {
+              const double v = outv[wid][i * NJ + 3 * k + mm] +
+                               (i == 2 ? sh_load[wid][3 * k + mm] * uz : 0.0);
+              row[k * NR + 3 * i + mm] += Mv[9 * k + 3 * i + mm] * mirror_slip_sign(mm) + v;
+            }
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------- k_final
+struct FinalArgs {
+  int kind, subtract, out_f32, n_a, n_b;
+  int64_t lo, n_chunk, n_src, n_obs, n_dof;
+  const double* normals;
+  const double* rec_basis;
+  const double* src_basis;
+  const int32_t* col_ptr;
+  const int32_t* col_ent;
+  double mu, lam;
+  void* out;
+};
+
+// Eigenstress C:sym(slip (x) n) of one row: phi C(n) + phi_m C(n_m) sign.
+__device__ __forceinline__ double eig_comp(const SrcPrep& p, double phi, double phim, double mu,
+                                           double lam, int a, int b, int m) {
+  const double* n = p.f.n;
+  const double* nm = p.fi.n;
+  const double c = (a == b ? lam * n[m] : 0.0) + mu * ((a == m ? n[b] : 0.0) + (b == m ? n[a] : 0.0));
+  const double cm = (a == b ? lam * nm[m] : 0.0) + mu * ((a == m ? nm[b] : 0.0) + (b == m ? nm[a] : 0.0));
+  return phi * c + phim * (cm * mirror_slip_sign(m));
+}
+
+template <class OUT>
+__device__ __forceinline__ void store(void* out, int64_t i, double v) {
+  reinterpret_cast<OUT*>(out)[i] = (OUT)v;
+}
+
+// Value of output component `comp` of one (observer, source, node) row.
+template <int KC>
+__device__ void row_values(const FinalArgs& a, const SrcPrep& p, const double* row, int64_t o,
+                           int64_t scol, double* v, int nv) {
+  constexpr int C = comps_of(KC);
+  const double phi = row[C], phim = row[C + 1];
+  const double mu = a.mu, lam = a.lam;
+  switch (a.kind) {
+    case MHS_DISP:
+      for (int i = 0; i < 9; ++i) v[i] = row[i];
+      break;
+    case MHS_TOTAL_STRESS:
+      for (int i = 0; i < 27; ++i) v[i] = row[i];
+      break;
+    case MHS_EIGENSTRESS:
+      for (int aa = 0; aa < 3; ++aa)
+        for (int b = 0; b < 3; ++b)
+          for (int m = 0; m < 3; ++m) v[9 * aa + 3 * b + m] = eig_comp(p, row[0], row[1], mu, lam, aa, b, m);
+      break;
+    case MHS_STRESS:
+    case MHS_STRAIN:
+      for (int aa = 0; aa < 3; ++aa)
+        for (int b = 0; b < 3; ++b)
+          for (int m = 0; m < 3; ++m) {
+            double s = row[9 * aa + 3 * b + m];
+            if (a.subtract) s -= eig_comp(p, phi, phim, mu, lam, aa, b, m);
+            v[9 * aa + 3 * b + m] = s;
+          }
+      if (a.kind == MHS_STRAIN)
+        for (int m = 0; m < 3; ++m) {
+          const double tr = v[m] + v[12 + m] + v[24 + m];
+          const double tre = tr / (3.0 * lam + 2.0 * mu);
+          for (int d = 0; d < 3; ++d) v[12 * d + m] -= lam * tre;
+          for (int i = 0; i < 9; ++i) v[3 * i + m] /= (2.0 * mu);
+        }
+      break;
+    default: {  // traction / interaction
+      const double* n = a.normals + 3 * o;
+      double t[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int m = 0; m < 3; ++m) {
+          double s = row[9 * i + 3 * 0 + m] * n[0] + row[9 * i + 3 * 1 + m] * n[1] + row[9 * i + 3 * 2 + m] * n[2];
+          if (a.subtract) {
+            double e = 0.0;
+            for (int j = 0; j < 3; ++j) e += eig_comp(p, phi, phim, mu, lam, i, j, m) * n[j];
+            s -= e;
+          }
+          t[i][m] = s;
+        }
+      if (a.kind == MHS_TRACTION) {
+        for (int i = 0; i < 3; ++i)
+          for (int m = 0; m < 3; ++m) v[3 * i + m] = t[i][m];
+      } else {
+        const double* rb = a.rec_basis + o * a.n_a * 3;
+        const double* sb = a.src_basis + scol * a.n_b * 3;
+        for (int ia = 0; ia < a.n_a; ++ia)
+          for (int ib = 0; ib < a.n_b; ++ib) {
+            double acc = 0.0;
+            for (int i = 0; i < 3; ++i)
+              for (int m = 0; m < 3; ++m) acc += rb[3 * ia + i] * t[i][m] * sb[3 * ib + m];
+            v[ia * a.n_b + ib] = acc;
+          }
+      }
+    }
+  }
+}
+
+template <int P, int KC, class OUT, bool CONT>
+__global__ void __launch_bounds__(TB)
+k_final(FinalArgs a, const SrcPrep* __restrict__ prep, const double* __restrict__ T) {
+  constexpr int K = n_nodes(P);
+  constexpr int NR = row_of(KC);
+  const int64_t col = blockIdx.x * (int64_t)TB + threadIdx.x;
+  const int64_t oc = blockIdx.y;
+  if (col >= a.n_dof) return;
+  const int64_t o = a.lo + oc;
+  int nv;
+  switch (a.kind) {
+    case MHS_DISP:
+    case MHS_TRACTION: nv = 9; break;
+    case MHS_INTERACTION: nv = a.n_a * a.n_b; break;
+    default: nv = 27;
+  }
+  double v[27];
+  if (!CONT) {
+    const int64_t s = col / K;
+    const double* row = T + (oc * a.n_src * K + col) * NR;
+    row_values<KC>(a, prep[s], row, o, s, v, nv);
+  } else {
+    for (int i = 0; i < nv; ++i) v[i] = 0.0;
+    for (int e = a.col_ptr[col]; e < a.col_ptr[col + 1]; ++e) {
+      const int ent = a.col_ent[e];
+      const int64_t s = ent / 6;
+      const double* row = T + (oc * a.n_src * K + ent) * NR;
+      double w[27];
+      row_values<KC>(a, prep[s], row, o, col, w, nv);
+      for (int i = 0; i < nv; ++i) v[i] += w[i];
+    }
+  }
+  // store in the caller's layout
+  switch (a.kind) {
+    case MHS_DISP:
+    case MHS_TRACTION:  // (N, 3, n_dof, 3)
+      for (int i = 0; i < 3; ++i)
+        for (int m = 0; m < 3; ++m)
+          store<OUT>(a.out, ((o * 3 + i) * a.n_dof + col) * 3 + m, v[3 * i + m]);
+      break;
+    case MHS_INTERACTION:  // (N, n_dof, n_a, n_b)
+      for (int i = 0; i < nv; ++i) store<OUT>(a.out, (o * a.n_dof + col) * nv + i, v[i]);
+      break;
+    default:  // (N, 3, 3, n_dof, 3)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          for (int m = 0; m < 3; ++m)
+            store<OUT>(a.out, (((o * 3 + i) * 3 + j) * a.n_dof + col) * 3 + m, v[9 * i + 3 * j + m]);
+  }
+}
+
+// ----------------------------------------------------------------- host
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUDA_TRY(x)                                                            \
+  do {                                                                         \
+    cudaError_t e_ = (x);                                                      \
+    if (e_ != cudaSuccess) return fail(MHS_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+std::mutex g_init_mu;
+std::vector<int> g_init_done;
+
+int ensure_device_tables() {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if ((int)g_init_done.size() <= dev) g_init_done.resize(dev + 1, 0);
+  if (g_init_done[dev]) return MHS_OK;
+  std::vector<double> x(GL_TABLE), w(GL_TABLE);
+  gauss_table(x.data(), w.data());
+  CUDA_TRY(cudaMemcpyToSymbol(d_glx, x.data(), sizeof(double) * GL_TABLE));
+  CUDA_TRY(cudaMemcpyToSymbol(d_glw, w.data(), sizeof(double) * GL_TABLE));
+  g_init_done[dev] = 1;
+  return MHS_OK;
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Layout {
+  size_t status, coef, prep, G, cnt, list, T, total;
+  int64_t chunk;
+};
+
+// Workspace carve-up for a chunk of `chunk` observers.
+Layout plan(const mhs_request* r, int64_t chunk) {
+  const int kc = kind_class(r->kind);
+  const int K = n_nodes(r->order);
+  Layout L;
+  size_t off = 0;
+  L.status = off; off = align_up(off + 256);
+  L.coef = off; off = align_up(off + sizeof(double) * IMAGE_COEF_SIZE);
+  L.prep = off; off = align_up(off + sizeof(SrcPrep) * (size_t)r->n_src);
+  L.G = off;
+  if (kc != KD_E) off = align_up(off + sizeof(double) * G_SIZE * (size_t)r->n_src);
+  L.cnt = off; off = align_up(off + sizeof(int) * (size_t)r->n_src);
+  L.list = off; off = align_up(off + sizeof(int) * (size_t)r->n_src * (size_t)chunk);
+  L.T = off; off = align_up(off + sizeof(double) * (size_t)chunk * r->n_src * K * row_of(kc));
+  L.total = off;
+  L.chunk = chunk;
+  return L;
+}
+
+int check_request(const mhs_request* r) {
+  if (!r) return fail(MHS_ERR_ARG, "null request");
+  if (r->kind < MHS_DISP || r->kind > MHS_INTERACTION) return fail(MHS_ERR_ARG, "bad kind %d", r->kind);
+  if (r->order < 0 || r->order > 2) return fail(MHS_ERR_ARG, "order must be 0, 1 or 2");
+  if (r->n_obs <= 0 || r->n_src <= 0) return fail(MHS_ERR_ARG, "empty request");
+  if (r->n_src > 65535) return fail(MHS_ERR_ARG, "n_src %lld above 65535", (long long)r->n_src);
+  if (!r->obs || !r->tris || !r->eps || !r->out) return fail(MHS_ERR_ARG, "null array");
+  if (!(r->mu > 0.0)) return fail(MHS_ERR_ARG, "mu must be positive");
+  if ((r->kind == MHS_TRACTION || r->kind == MHS_INTERACTION) && !r->normals)
+    return fail(MHS_ERR_ARG, "normals required");
+  if (r->kind == MHS_INTERACTION &&
+      (!r->rec_basis || !r->src_basis || r->n_a < 1 || r->n_a > 3 || r->n_b < 1 || r->n_b > 3))
+    return fail(MHS_ERR_ARG, "interaction bases");
+  if (r->ids && (r->order != 2 || !r->col_ptr || !r->col_ent || r->n_cols <= 0))
+    return fail(MHS_ERR_ARG, "continuous layout needs order 2 and a column plan");
+  if (r->precision != MHS_FP64 && r->precision != MHS_MIXED) return fail(MHS_ERR_ARG, "precision");
+  return MHS_OK;
+}
+
+template <int P, int KC>
+int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
+  char* ws = (char*)r->workspace;
+  int* status = (int*)(ws + L.status);
+  double* coef = (double*)(ws + L.coef);
+  SrcPrep* prep = (SrcPrep*)(ws + L.prep);
+  double* G = (double*)(ws + L.G);
+  int* cnt = (int*)(ws + L.cnt);
+  int* list = (int*)(ws + L.list);
+  double* T = (double*)(ws + L.T);
+  constexpr int K = n_nodes(P);
+  k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(r->mu, r->lam, coef);
+  k_prep<<<(unsigned)((r->n_src + 127) / 128), 128, 0, st>>>(r->n_src, r->tris, r->eps, r->fold,
+                                                              KC != KD_E, prep, G);
+  const bool cont = r->ids != nullptr;
+  const int64_t n_dof = cont ? r->n_cols : r->n_src * K;
+  for (int64_t lo = 0; lo < r->n_obs; lo += L.chunk) {
+    const int64_t nc = std::min<int64_t>(L.chunk, r->n_obs - lo);
+    dim3 g((unsigned)((nc + TB - 1) / TB), (unsigned)r->n_src);
+    k_pair<P, KC><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, G, coef, r->mu, r->lam, T);
+    if constexpr (KC != KD_E)
+      k_imageq<P, KC><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, coef, r->mu, r->lam, T);
+    if (r->fold) {
+      k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
+      dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
+      const size_t fsm = sizeof(FoldShared<P, KC>);
+      CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+      k_fold<P, KC><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
+                                                      r->mu, r->lam, T, status);
+    }
+    FinalArgs a;
+    a.kind = r->kind;
+    a.subtract = r->subtract_eigenstress;
+    a.out_f32 = r->out_f32;
+    a.n_a = r->n_a;
+    a.n_b = r->n_b;
+    a.lo = lo;
+    a.n_chunk = nc;
+    a.n_src = r->n_src;
+    a.n_obs = r->n_obs;
+    a.n_dof = n_dof;
+    a.normals = r->normals;
+    a.rec_basis = r->rec_basis;
+    a.src_basis = r->src_basis;
+    a.col_ptr = r->col_ptr;
+    a.col_ent = r->col_ent;
+    a.mu = r->mu;
+    a.lam = r->lam;
+    a.out = r->out;
+    dim3 gfin((unsigned)((n_dof + TB - 1) / TB), (unsigned)nc);
+    if (r->out_f32) {
+      if (cont) k_final<P, KC, float, true><<<gfin, TB, 0, st>>>(a, prep, T);
+      else k_final<P, KC, float, false><<<gfin, TB, 0, st>>>(a, prep, T);
+    } else {
+      if (cont) k_final<P, KC, double, true><<<gfin, TB, 0, st>>>(a, prep, T);
+      else k_final<P, KC, double, false><<<gfin, TB, 0, st>>>(a, prep, T);
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  return MHS_OK;
+}
+
+template <int P>
+int run_kind(const mhs_request* r, cudaStream_t st, const Layout& L) {
+  switch (kind_class(r->kind)) {
+    case KD_DISP: return run<P, KD_DISP>(r, st, L);
+    case KD_HE: return run<P, KD_HE>(r, st, L);
+    default: return run<P, KD_E>(r, st, L);
+  }
+}
+
+constexpr size_t GOOD_T_BYTES = size_t(2) << 30;
+
+}  // namespace
+
+extern "C" {
+
+int mhs_workspace_bytes(const mhs_request* req, size_t* min_bytes, size_t* good_bytes) {
+  int rc = check_request(req);
+  if (rc) return rc;
+  const Layout one = plan(req, 1);
+  const size_t row = plan(req, 2).total - one.total;
+  int64_t chunk = std::min<int64_t>(req->n_obs, 65535);
+  const Layout all = plan(req, chunk);
+  if (all.total - one.total > GOOD_T_BYTES && row > 0) {
+    chunk = std::max<int64_t>(1, (int64_t)(GOOD_T_BYTES / row));
+  }
+  if (min_bytes) *min_bytes = one.total;
+  if (good_bytes) *good_bytes = plan(req, chunk).total;
+  return MHS_OK;
+}
+
+int mhs_assemble(const mhs_request* req, void* stream) {
+  int rc = check_request(req);
+  if (rc) return rc;
+  rc = ensure_device_tables();
+  if (rc) return rc;
+  // largest chunk the workspace holds
+  const Layout one = plan(req, 1);
+  if (!req->workspace || req->workspace_bytes < one.total)
+    return fail(MHS_ERR_WORKSPACE, "workspace %zu bytes, need at least %zu", req->workspace_bytes,
+                one.total);
+  int64_t lo = 1, hi = std::min<int64_t>(req->n_obs, 65535);
+  while (lo < hi) {  // plan() is monotone in chunk
+    const int64_t mid = lo + (hi - lo + 1) / 2;
+    if (plan(req, mid).total <= req->workspace_bytes) lo = mid;
+    else hi = mid - 1;
+  }
+  const Layout L = plan(req, lo);
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (req->order) {
+    case 0: return run_kind<0>(req, st, L);
+    case 1: return run_kind<1>(req, st, L);
+    default: return run_kind<2>(req, st, L);
+  }
+}
+
+int mhs_read_status(void* workspace, void* stream, int* bits) {
+  cudaStream_t st = (cudaStream_t)stream;
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, workspace, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) CUDA_TRY(cudaMemsetAsync(workspace, 0, sizeof(int), st));
+  if (bits) *bits = h;
+  return MHS_OK;
+}
+
+int mhs_column_plan(const int64_t* ids, int64_t n_src, int64_t n_cols, int32_t* col_ptr,
+                    int32_t* col_ent) {
+  if (!ids || !col_ptr || !col_ent || n_src <= 0 || n_cols <= 0) return fail(MHS_ERR_ARG, "column plan args");
+  std::vector<int32_t> count(n_cols + 1, 0);
+  for (int64_t i = 0; i < n_src * 6; ++i) {
+    if (ids[i] < 0 || ids[i] >= n_cols) return fail(MHS_ERR_ARG, "ids[%lld] out of range", (long long)i);
+    count[ids[i] + 1]++;
+  }
+  for (int64_t c = 0; c < n_cols; ++c) count[c + 1] += count[c];
+  for (int64_t c = 0; c <= n_cols; ++c) col_ptr[c] = count[c];
+  for (int64_t i = 0; i < n_src * 6; ++i) col_ent[count[ids[i]]++] = (int32_t)i;  // ascending i
+  return MHS_OK;
+}
+
+const char* mhs_last_error(void) { return g_err; }
+
+const char* mhs_version(void) { return "mhs_b200 0.1.0"; }
+
+}  // extern "C"

@@ -1,0 +1,164 @@
+"""Generate the golden fixtures: inputs and mhs's own outputs, as .npz.
+
+Run where the reference package is importable (its source tree on
+``MHS_REFERENCE_SRC``, default the read-only checkout used to build this
+repository)::
+
+    python tests/golden/make_golden.py [case ...]
+
+Each case stores its inputs (``obs``, ``tris``, ``eps``, material, options)
+and the arrays mhs returns for them.  Sizes are small so the whole set runs
+in a few minutes on one core and the fixtures stay small; the GPU tests
+compare the CUDA path against these arrays and the CPU tests pin the numpy
+oracle against them.
+"""
+from __future__ import annotations
+
+import os
+import pathlib
+import sys
+import time
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+sys.path.insert(0, os.environ.get("MHS_REFERENCE_SRC", "/root/reference/src"))
+
+import mhs  # noqa: E402  (the reference)
+
+from mhs_b200 import synthetic  # noqa: E402
+
+
+def _save(name: str, **arrays) -> None:
+    np.savez_compressed(HERE / f"{name}.npz", **arrays)
+
+
+def case_c1_subset():
+    """Config-1 geometry, 60 of its 600 observers, disp + stress P0."""
+    c = synthetic.config1(seed=0)
+    obs = c["obs"][::10].copy()
+    mat = mhs.Material(c["mu"], c["lam"])
+    U = mhs.disp_matrix(obs, c["tris"], mat, c["eps"])
+    S = mhs.stress_matrix(obs, c["tris"], mat, c["eps"])
+    T = mhs.total_stress_matrix(obs, c["tris"], mat, c["eps"])
+    _save("c1_subset", obs=obs, tris=c["tris"], mu=c["mu"], lam=c["lam"], eps=c["eps"],
+          disp=U, stress=S, total_stress=T)
+
+
+def _patch(seed=1, top=-0.6, dip=55.0, strike=20.0, nu=3, nv=2):
+    tris = synthetic.planar_fault(strike, dip, 3.0, 2.0, top, nu, nv)
+    rng = np.random.default_rng(seed)
+    obs = np.concatenate([
+        rng.uniform([-3, -3, -3], [3, 3, 0], (16, 3)),        # near the patch
+        rng.uniform([-25, -25, -15], [25, 25, 0], (8, 3)),     # far field
+    ])
+    return tris, obs
+
+
+def case_orders():
+    """A 12-triangle patch, 24 observers, orders 0/1/2: disp, stress,
+    total stress and traction (random unit normals), scalar eps."""
+    tris, obs = _patch()
+    rng = np.random.default_rng(7)
+    nrm = rng.standard_normal((obs.shape[0], 3))
+    mat = mhs.Material(30.0, 20.0)
+    out = dict(obs=obs, tris=tris, mu=30.0, lam=20.0, eps=0.15, normals=nrm)
+    for p in (0, 1, 2):
+        out[f"disp_p{p}"] = mhs.disp_matrix(obs, tris, mat, 0.15, order=p)
+        out[f"stress_p{p}"] = mhs.stress_matrix(obs, tris, mat, 0.15, order=p)
+        out[f"total_p{p}"] = mhs.total_stress_matrix(obs, tris, mat, 0.15, order=p)
+        out[f"traction_p{p}"] = mhs.traction_matrix(obs, nrm, tris, mat, 0.15, order=p)
+    _save("orders", **out)
+
+
+def case_eps_per_tri():
+    """Per-triangle eps and a lam < mu material, P0 and P1."""
+    tris, obs = _patch(seed=3, top=-1.2, dip=75.0, strike=-35.0)
+    eps = np.linspace(0.08, 0.3, tris.shape[0])
+    mat = mhs.Material(25.0, 12.0)
+    out = dict(obs=obs, tris=tris, mu=25.0, lam=12.0, eps=eps)
+    for p in (0, 1):
+        out[f"disp_p{p}"] = mhs.disp_matrix(obs, tris, mat, eps, order=p)
+        out[f"stress_p{p}"] = mhs.stress_matrix(obs, tris, mat, eps, order=p)
+    _save("eps_per_tri", **out)
+
+
+def case_interaction():
+    """Self-interaction on a 24-triangle buried fault, P0 full 3x3, P1
+    (strike, dip) x all, P2 strike x strike; plus a rectangular block with
+    rows=."""
+    tris = synthetic.planar_fault(10.0, 50.0, 6.0, 3.0, -1.0, 4, 3)
+    mat = mhs.Material(30.0, 30.0)
+    out = dict(tris=tris, mu=30.0, lam=30.0, eps=0.1)
+    out["int_p0"] = mhs.interaction_matrix(tris, mat, 0.1)
+    out["int_p1"] = mhs.interaction_matrix(tris, mat, 0.1, order=1, receiver=("strike", "dip"))
+    out["int_p2"] = mhs.interaction_matrix(tris, mat, 0.1, order=2, receiver="strike",
+                                           source="strike")
+    out["int_p0_rows"] = mhs.interaction_matrix(tris, mat, 0.1, rows=(5, 17))
+    out["int_p0_noeig"] = mhs.interaction_matrix(tris, mat, 0.1, subtract_eigenstress=False)
+    _save("interaction", **out)
+
+
+def case_fold():
+    """Surface-reaching fault (top at z = 0): the top row folds.  Interaction
+    P0 (3x3), stress and disp at near-surface observers, with and without
+    the fold, and the P1 interaction."""
+    tris = synthetic.planar_fault(0.0, 60.0, 3.0, 1.6, 0.0, 3, 2)
+    rng = np.random.default_rng(11)
+    obs = np.column_stack([rng.uniform(-2.0, 2.0, 6), rng.uniform(-1.0, 2.0, 6),
+                           -rng.uniform(0.0, 0.9, 6)])
+    mat = mhs.Material(30.0, 25.0)
+    eps = 0.12
+    out = dict(tris=tris, obs=obs, mu=30.0, lam=25.0, eps=eps)
+    out["int_p0"] = mhs.interaction_matrix(tris, mat, eps)
+    out["stress_p0"] = mhs.stress_matrix(obs, tris, mat, eps)
+    out["stress_p0_nofold"] = mhs.stress_matrix(obs, tris, mat, eps, fold=False)
+    out["disp_p0"] = mhs.disp_matrix(obs, tris, mat, eps)
+    out["int_p1"] = mhs.interaction_matrix(tris, mat, eps, order=1, receiver=("strike",),
+                                           source=("strike", "dip"))
+    _save("fold", **out)
+
+
+def case_continuous():
+    """Continuous P2 interaction on a two-group network (buried) and its
+    traction matrix at a few observers."""
+    a = synthetic.planar_fault(0.0, 90.0, 2.0, 1.0, -1.0, 2, 1)
+    b = synthetic.planar_fault(30.0, 60.0, 1.5, 1.0, -1.2, 2, 1, centre=(2.5, 0.5))
+    tris = np.concatenate([a, b])
+    groups = np.array([0] * a.shape[0] + [1] * b.shape[0])
+    mat = mhs.Material(30.0, 30.0)
+    sn = mhs.shared_nodes(tris, groups=groups)
+    out = dict(tris=tris, groups=groups, mu=30.0, lam=30.0, eps=0.1, ids=sn.ids,
+               coords=sn.coords, normals=sn.normals)
+    out["int_cont"] = mhs.interaction_matrix(tris, mat, 0.1, order=2, layout="continuous",
+                                             shared=sn, source=("strike", "dip"))
+    rng = np.random.default_rng(5)
+    obs = rng.uniform([-2, -2, -3], [4, 2, 0], (10, 3))
+    nrm = rng.standard_normal((10, 3))
+    out["obs"] = obs
+    out["obs_normals"] = nrm
+    out["trac_cont"] = mhs.traction_matrix(obs, nrm, tris, mat, 0.1, order=2,
+                                           layout="continuous", shared=sn)
+    _save("continuous", **out)
+
+
+def case_rough_surface():
+    """Scaled-down config 2: rough surface-reaching fault, per-triangle eps,
+    full 3x3 interaction with the fold."""
+    c = synthetic.config2(seed=3, nu=4, nv=3)
+    mat = mhs.Material(c["mu"], c["lam"])
+    K = mhs.interaction_matrix(c["tris"], mat, c["eps"])
+    _save("rough_surface", tris=c["tris"], eps=c["eps"], mu=c["mu"], lam=c["lam"], int_p0=K)
+
+
+CASES = {f.__name__[5:]: f for f in (case_c1_subset, case_orders, case_eps_per_tri,
+                                     case_interaction, case_fold, case_continuous,
+                                     case_rough_surface)}
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CASES)
+    for n in names:
+        t = time.time()
+        CASES[n]()
+        print(f"{n}: {time.time() - t:.1f} s", flush=True)
