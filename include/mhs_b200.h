@@ -101,6 +101,16 @@ int mhs_read_status(void* workspace, void* stream, int* bits);
 int mhs_column_plan(const int64_t* ids_host, int64_t n_src, int64_t n_cols, int32_t* col_ptr,
                     int32_t* col_ent);
 
+/* Diagnostics: one influence term of ONE source at n observers, one thread
+ * per observer, as the pipeline evaluates it (term 0 direct, 1 image
+ * R-family, 2 image Q-family, 3 folded image).  out (device) receives per
+ * observer K x C values (C = 9 for want_u, else 27) then K blob weights.
+ * coef_scratch: device buffer of at least 4096 doubles.  No counterpart in
+ * mhs; the per-term split follows mhs/kernels/assemble.py:96-120. */
+int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, const double* tri,
+                    double mu, double lam, double eps, double* coef_scratch, double* out,
+                    void* stream);
+
 /* Last error message of this thread. */
 const char* mhs_last_error(void);
 

@@ -354,7 +354,7 @@ template <int P>
 MHS_HD void fold_surface_load(const Frame& f, const QuadRule& r12, const QuadRule& r8, double px,
                               double py, double eps, const Material& m, double* s /*K x 3*/) {
   constexpr int K = n_nodes(P);
-  double H[K * 27], E[K];
+  double H[K * 27] = {}, E[K] = {};
   const double x[3] = {px, py, 0.0};
   direct_eval<P, W_H | W_E>(f, r12, r8, x, eps, m, nullptr, H, E);
   double ezz[3];

@@ -65,7 +65,7 @@ template <class S>
 MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, const Material& m,
                      double* U) {
   double zp[4] = {1.0, z, z * z, z * z * z};
-  const int s3 = nslot(3), s5 = nslot(5);
+  const int s5 = nslot(5);
   constexpr Spec sp = S::spec;
   constexpr int o3 = sp.w_off[nslot(3)], o5 = sp.w_off[nslot(5)];
   const double V3[3] = {-W[o3 + tri_idx(1, 0)], -W[o3 + tri_idx(0, 1)], z * W[o3]};
@@ -99,7 +99,7 @@ template <class S>
 MHS_HD void kernel_H(const Frame& f, const double* W, double z, double eps, const Material& m,
                      double* H) {
   double zp[5] = {1.0, z, z * z, z * z * z, z * z * z * z};
-  const int s3 = nslot(3), s5 = nslot(5), s7 = nslot(7);
+  const int s5 = nslot(5), s7 = nslot(7);
   constexpr Spec sp = S::spec;
   const double I3 = W[sp.w_off[nslot(3)]];
   const double I5 = W[sp.w_off[nslot(5)]];
@@ -175,7 +175,7 @@ MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
     shape_coeffs<P>(f, X0, X1, c);
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
-      double W[NW];
+      double W[NW] = {};
       weight_closed<S, P>(T, c, k, W);
       if (WANT & W_U) kernel_U<S>(f, W, z, eps, m, U + 9 * k);
       if (WANT & W_H) kernel_H<S>(f, W, z, eps, m, H + 27 * k);
@@ -183,7 +183,7 @@ MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
     }
   } else {
     const QuadRule& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
-    double W[K * NW];
+    double W[K * NW] = {};
     weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
@@ -326,7 +326,7 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
   double zpow[G_RMAX + 1];
   zpow[0] = 1.0;
   for (int i = 1; i <= G_RMAX; ++i) zpow[i] = zpow[i - 1] * zp;
-  double Wall[K * NW];
+  double Wall[K * NW] = {};
   if (D <= cst::D_STAR * fi.L) {
     MomentTable<S> T;
     closed_moments<S>(fi, X0, X1, h2, T);

@@ -184,7 +184,7 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   const double eps = sp.eps;
   double* row = T + ((oc * n_src + s) * K) * NR;
   if constexpr (KC == KD_E) {
-    double E[K];
+    double E[K] = {};
     direct_eval<P, W_E>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
     for (int k = 0; k < K; ++k) {
       row[k * NR + 0] = E[k];
@@ -193,14 +193,14 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     return;
   } else {
     constexpr int C = comps_of(KC);
-    double A[K * C], E[K];
+    double A[K * C] = {}, E[K] = {};
     if constexpr (KC == KD_DISP)
       direct_eval<P, W_U>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
     else
       direct_eval<P, W_H | W_E>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
     const bool band = sp.straddle && fold_band(x, sp.centre, eps);
     if (!band) {
-      double B[K * C];
+      double B[K * C] = {};
       const ImageCoef ic = image_coef_view(coef);
       if constexpr (KC == KD_DISP)
         image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
@@ -346,7 +346,7 @@ k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ 
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) ti[3 * i + j] = sp.fi.v[i][j];
   const int n = q_gauss_order(x, ti, eps, sp.f.L, P);
-  double B[K * C];
+  double B[K * C] = {};
   constexpr int WANT = KC == KD_DISP ? W_U : W_H;
   if (n == QFLOOR) {
     QRuleSmem<P> r{qy, qw, QFLOOR * QFLOOR};
@@ -471,7 +471,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   const QuadRule r12 = rd.r12(), r8 = rd.r8();
   if constexpr (KC == KD_E) {
     if (lane == 0) {
-      double E[K];
+      double E[K] = {};
       direct_eval<P, W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, nullptr, E);
       for (int k = 0; k < K; ++k) row[k * NR + 1] = E[k];
     }
@@ -483,7 +483,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
       double R1;
       sbrk_n[wid] = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, brk[wid], &R1);
       sR1[wid] = R1;
-      double sl[NJ];
+      double sl[NJ] = {};
       fold_surface_load<P>(sp.f, r12, r8, x[0], x[1], eps, m, sl);
       for (int j = 0; j < NJ; ++j) sh_load[wid][j] = sl[j];
     }
@@ -513,7 +513,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
       const int npts = cst::FOLD_N_RADIAL * A.n;
       for (int b0 = 0; b0 < npts; b0 += 32) {
         const int t = b0 + lane;
-        double Bv[NC], sv[NJ];
+        double Bv[NC] = {}, sv[NJ] = {};
         if (t < npts) {
           const int ir = t / A.n, j = t % A.n;
           const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
@@ -554,7 +554,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     }
     __syncwarp();
     if (lane == 0) {
-      double Mv[K * C], E[K];
+      double Mv[K * C] = {}, E[K] = {};
       if constexpr (WH) {
         direct_eval<P, W_H | W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, Mv, E);
         double srr, szz;
@@ -829,6 +829,7 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
   int* list = (int*)(ws + L.list);
   double* T = (double*)(ws + L.T);
   constexpr int K = n_nodes(P);
+  CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
   k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(r->mu, r->lam, coef);
   k_prep<<<(unsigned)((r->n_src + 127) / 128), 128, 0, st>>>(r->n_src, r->tris, r->eps, r->fold,
                                                               KC != KD_E, prep, G);
@@ -890,6 +891,72 @@ int run_kind(const mhs_request* r, cudaStream_t st, const Layout& L) {
 }
 
 constexpr size_t GOOD_T_BYTES = size_t(2) << 30;
+
+// ---------------------------------------------------- per-term diagnostics
+// One source, n observers, one thread per observer: a single influence term
+// exactly as the pipeline evaluates it.  term 0 direct (H + E or U), 1 image
+// R-family, 2 image Q-family, 3 folded image (mirror + Boussinesq).
+// out per observer: K x C tensor values, then K blob weights (direct only).
+template <int P, int WANT>
+__global__ void k_terms(int term, int n, const double* __restrict__ obs,
+                        const double* __restrict__ tri, double mu, double lam, double eps,
+                        const double* __restrict__ coef, double* __restrict__ out) {
+  constexpr int K = n_nodes(P);
+  constexpr int C = (WANT & W_U) ? 9 : 27;
+  __shared__ Frame f, fi;
+  __shared__ SmemRules<P> rd, ri;
+  __shared__ double sG[G_SIZE];
+  if (threadIdx.x == 0) {
+    double ti[9];
+    for (int i = 0; i < 9; ++i) ti[i] = (i % 3 == 2) ? -tri[i] : tri[i];
+    make_frame(tri, f);
+    make_frame(ti, fi);
+    build_basis_products(fi, sG);
+  }
+  __syncthreads();
+  rd.build(f, threadIdx.x, blockDim.x);
+  ri.build(fi, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  const Material m = make_material(mu, lam);
+  const ImageCoef ic = image_coef_view(coef);
+  double A[K * C] = {}, E[K] = {};
+  for (int k = 0; k < K; ++k) E[k] = 0.0;
+  if (term == 0) {
+    if (WANT & W_U) direct_eval<P, W_U>(f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
+    else direct_eval<P, W_H | W_E>(f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
+  } else if (term == 1) {
+    image_r_eval<P, WANT>(fi, sG, f.n, ri.r12(), ri.r8(), x, eps, m, ic, A, A);
+  } else if (term == 2) {
+    double ti[9];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) ti[3 * i + j] = fi.v[i][j];
+    const int nq = q_gauss_order(x, ti, eps, f.L, P);
+    QRuleFly<P> r{&f, nq};
+    image_q_rule<P, WANT>(r, f.n, x, eps, m, ic, A, A);
+  } else {
+    double Mv[K * C] = {}, Bq[K * C] = {};
+    if (WANT & W_U) direct_eval<P, W_U>(fi, ri.r12(), ri.r8(), x, eps, m, Mv, nullptr, nullptr);
+    else direct_eval<P, W_H>(fi, ri.r12(), ri.r8(), x, eps, m, nullptr, Mv, nullptr);
+    fold_boussinesq_scalar<P, !(WANT & W_U)>(f, rd.r12(), rd.r8(), tri, x, eps, m, d_glx, d_glw, Bq);
+    for (int i = 0; i < K * C; ++i) A[i] = Mv[i] * mirror_slip_sign(i % 3) + Bq[i];
+  }
+  for (int i = 0; i < K * C; ++i) out[o * (K * C + K) + i] = A[i];
+  for (int k = 0; k < K; ++k) out[o * (K * C + K) + K * C + k] = E[k];
+}
+
+template <int P>
+int debug_terms(int term, int want_u, int n, const double* obs, const double* tri, double mu,
+                double lam, double eps, double* coef, double* out, cudaStream_t st) {
+  k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(mu, lam, coef);
+  const int nb = (n + 63) / 64;
+  if (want_u) k_terms<P, W_U><<<nb, 64, 0, st>>>(term, n, obs, tri, mu, lam, eps, coef, out);
+  else k_terms<P, W_H><<<nb, 64, 0, st>>>(term, n, obs, tri, mu, lam, eps, coef, out);
+  CUDA_TRY(cudaGetLastError());
+  return MHS_OK;
+}
 
 }  // namespace
 
@@ -957,6 +1024,22 @@ int mhs_column_plan(const int64_t* ids, int64_t n_src, int64_t n_cols, int32_t* 
   for (int64_t c = 0; c <= n_cols; ++c) col_ptr[c] = count[c];
   for (int64_t i = 0; i < n_src * 6; ++i) col_ent[count[ids[i]]++] = (int32_t)i;  // ascending i
   return MHS_OK;
+}
+
+int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, const double* tri,
+                    double mu, double lam, double eps, double* coef_scratch, double* out,
+                    void* stream) {
+  int rc = ensure_device_tables();
+  if (rc) return rc;
+  if (n <= 0 || term < 0 || term > 3 || !obs || !tri || !coef_scratch || !out)
+    return fail(MHS_ERR_ARG, "debug_terms args");
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (order) {
+    case 0: return debug_terms<0>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
+    case 1: return debug_terms<1>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
+    case 2: return debug_terms<2>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
+  }
+  return fail(MHS_ERR_ARG, "order");
 }
 
 const char* mhs_last_error(void) { return g_err; }
