@@ -1,0 +1,86 @@
+"""The device engine's arithmetic, compiled for the CPU (tests/engine_host),
+term by term against the numpy oracle: direct Kelvin-Cortez, image R-family,
+image Q-family and the folded image, every order.  Tolerance 1e-12 relmax."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import build_hostcheck, relmax
+from oracle import mhs_oracle as O
+
+D = ctypes.POINTER(ctypes.c_double)
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def hc():
+    return ctypes.CDLL(str(build_hostcheck()))
+
+
+def _p(a):
+    return a.ctypes.data_as(D)
+
+
+TRI = np.array([[0.37, -0.81, -1.44], [1.92, 0.11, -2.63], [-0.25, 1.57, -1.22]])
+MU, LAM, EPS = 30.0, 20.0, 0.1
+
+
+def _obs():
+    rng = np.random.default_rng(0)
+    o = np.concatenate([rng.uniform(-3, 3, (12, 3)), rng.uniform(-40, 40, (6, 3)),
+                        rng.uniform(-200, 200, (4, 3))])
+    o[:, 2] = -np.abs(o[:, 2])
+    return np.ascontiguousarray(o)
+
+
+def test_gauss_legendre_matches_numpy(hc):
+    for n in (1, 4, 6, 8, 12, 37, 192):
+        x, w = np.zeros(n), np.zeros(n)
+        assert hc.hc_gauss(n, _p(x), _p(w)) == 0
+        xr, wr = np.polynomial.legendre.leggauss(n)
+        assert np.max(np.abs(x - xr)) < 1e-15 and np.max(np.abs(w - wr)) < 2e-14
+
+
+@pytest.mark.parametrize("P", [0, 1, 2])
+def test_direct(hc, P):
+    obs = _obs()
+    N, K = obs.shape[0], (P + 1) * (P + 2) // 2
+    ref = O.direct(obs, TRI, P, MU, LAM, EPS, ("U", "H", "E"))
+    U, H, E = np.zeros((N, K, 3, 3)), np.zeros((N, K, 3, 3, 3)), np.zeros((N, K))
+    c = ctypes.c_double
+    hc.hc_direct(P, 1, _p(obs), N, _p(TRI.copy()), c(MU), c(LAM), c(EPS), _p(U), None, None)
+    hc.hc_direct(P, 6, _p(obs), N, _p(TRI.copy()), c(MU), c(LAM), c(EPS), None, _p(H), _p(E))
+    assert relmax(U, ref["U"]) < TOL
+    assert relmax(H, ref["H"]) < TOL
+    assert relmax(E, ref["E"]) < TOL
+
+
+@pytest.mark.parametrize("P", [0, 1, 2])
+def test_image_r_and_q(hc, P):
+    obs = _obs()
+    N, K = obs.shape[0], (P + 1) * (P + 2) // 2
+    c = ctypes.c_double
+    for code, key in ((1, "U"), (2, "H")):
+        shape = (N, K, 3, 3) if key == "U" else (N, K, 3, 3, 3)
+        A = np.zeros(shape)
+        hc.hc_image_r(P, code, _p(obs), N, _p(TRI.copy()), c(MU), c(LAM), c(EPS), _p(A), _p(A))
+        assert relmax(A, O.image_r(obs, TRI, P, MU, LAM, EPS, (key,))[key]) < TOL
+        B = np.zeros(shape)
+        hc.hc_image_q(P, code, _p(obs), N, _p(TRI.copy()), c(MU), c(LAM), c(EPS), 0, _p(B), _p(B), None)
+        assert relmax(B, O.image_q(obs, TRI, P, MU, LAM, EPS, (key,))[key]) < TOL
+
+
+@pytest.mark.parametrize("P,key", [(0, "H"), (0, "U"), (1, "H")])
+def test_fold_image(hc, P, key):
+    tri = np.array([[0.0, 0.0, 0.0], [1.5, 0.2, -0.05], [0.3, 0.9, -1.1]])
+    obs = np.array([[0.5, 0.5, -0.3], [2.0, -1.0, -0.05]])
+    N, K = obs.shape[0], (P + 1) * (P + 2) // 2
+    shape = (N, K, 3, 3) if key == "U" else (N, K, 3, 3, 3)
+    A = np.zeros(shape)
+    c = ctypes.c_double
+    hc.hc_fold_image(P, 1 if key == "U" else 2, _p(obs), N, _p(tri.copy()), c(MU), c(LAM), c(0.12),
+                     _p(A), _p(A))
+    assert relmax(A, O.fold_image(obs, tri, P, MU, LAM, 0.12, (key,))[key]) < TOL
