@@ -111,6 +111,27 @@ int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, c
                     double mu, double lam, double eps, double* coef_scratch, double* out,
                     void* stream);
 
+/* Stage timing (tracing).  While enabled, every stage launch of every
+ * request is bracketed by CUDA events on its stream; mhs_profile_read waits
+ * for them and returns per-stage milliseconds and launch counts since the
+ * last read (arrays of MHS_N_STAGES).  No counterpart in mhs, which has no
+ * tracing. */
+enum mhs_stage {
+  MHS_STAGE_PREP = 0,    /* per-material coefficients, per-source frames */
+  MHS_STAGE_PAIR = 1,    /* direct term + image R-family */
+  MHS_STAGE_IMAGEQ = 2,  /* image Q-family */
+  MHS_STAGE_FOLD = 3,    /* band lists + folded image */
+  MHS_STAGE_FINAL = 4,   /* eigenstress, contraction, layout stores */
+  MHS_N_STAGES = 5
+};
+int mhs_profile_enable(int on);
+int mhs_profile_read(double* ms, int* launches);
+
+/* Issue ceiling of the device: independent FMA chains on every SM, FP64
+ * (fp64 = 1) or FP32, in TFLOP/s (2 flops per FMA).  The roofline
+ * denominator of the FP64 and mixed forms. */
+int mhs_fp_peak(int fp64, int iters, double* tflops, void* stream);
+
 /* Last error message of this thread. */
 const char* mhs_last_error(void);
 

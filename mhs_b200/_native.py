@@ -51,7 +51,8 @@ class Request(ctypes.Structure):
 
 #: Symbols the header declares; a test checks the library exports each.
 EXPORTS = ("mhs_workspace_bytes", "mhs_assemble", "mhs_read_status", "mhs_column_plan",
-           "mhs_last_error", "mhs_version")
+           "mhs_last_error", "mhs_version", "mhs_profile_enable", "mhs_profile_read",
+           "mhs_fp_peak", "mhs_debug_terms")
 
 _lib = None
 
@@ -81,8 +82,42 @@ def load() -> ctypes.CDLL:
     lib.mhs_last_error.restype = ctypes.c_char_p
     lib.mhs_version.argtypes = []
     lib.mhs_version.restype = ctypes.c_char_p
+    lib.mhs_profile_enable.argtypes = [ctypes.c_int]
+    lib.mhs_profile_enable.restype = ctypes.c_int
+    lib.mhs_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    lib.mhs_profile_read.restype = ctypes.c_int
+    lib.mhs_fp_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                ctypes.c_void_p]
+    lib.mhs_fp_peak.restype = ctypes.c_int
+    lib.mhs_debug_terms.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p]
+    lib.mhs_debug_terms.restype = ctypes.c_int
     _lib = lib
     return lib
+
+
+STAGES = ("prep", "pair", "imageq", "fold", "final")
+
+
+def profile(on: bool) -> None:
+    check(load().mhs_profile_enable(1 if on else 0))
+
+
+def profile_read() -> dict:
+    """Per-stage milliseconds and launch counts since the last read."""
+    ms = (ctypes.c_double * len(STAGES))()
+    n = (ctypes.c_int * len(STAGES))()
+    check(load().mhs_profile_read(ms, n))
+    return {s: (ms[i], n[i]) for i, s in enumerate(STAGES)}
+
+
+def fp_peak(fp64: bool = True, iters: int = 1 << 16, stream=None) -> float:
+    """Measured FMA issue ceiling of the current device, TFLOP/s."""
+    t = ctypes.c_double()
+    check(load().mhs_fp_peak(1 if fp64 else 0, iters, ctypes.byref(t), stream))
+    return t.value
 
 
 def check(rc: int) -> None:

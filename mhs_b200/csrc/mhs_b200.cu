@@ -775,6 +775,50 @@ int ensure_device_tables() {
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+// ------------------------------------------------------ stage timing
+// When enabled, each stage launch is bracketed by CUDA events on the
+// request's stream; mhs_profile_read sums them per stage.
+struct ProfRec {
+  int stage;
+  cudaEvent_t a, b;
+};
+std::mutex g_prof_mu;
+std::vector<ProfRec> g_prof;
+int g_prof_on = 0;
+
+struct StageTimer {
+  int stage;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  StageTimer(int s, cudaStream_t stream) : stage(s), st(stream) {
+    if (__atomic_load_n(&g_prof_on, __ATOMIC_RELAXED)) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~StageTimer() {
+    if (a) {
+      cudaEventRecord(b, st);
+      std::lock_guard<std::mutex> lk(g_prof_mu);
+      g_prof.push_back({stage, a, b});
+    }
+  }
+};
+
+// Independent FMA chains: the FP64 (or FP32) issue ceiling of the device.
+template <class R>
+__global__ void k_fma_peak(R* out, int iters, R b, R c) {
+  R a0 = R(threadIdx.x) * R(1e-9), a1 = a0 + R(1e-9), a2 = a0 + R(2e-9), a3 = a0 + R(3e-9);
+  R a4 = a0 + R(4e-9), a5 = a0 + R(5e-9), a6 = a0 + R(6e-9), a7 = a0 + R(7e-9);
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+    a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+  }
+  const R s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+  if (s == R(-1)) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 struct Layout {
   size_t status, coef, prep, G, cnt, list, T, total;
   int64_t chunk;
@@ -830,18 +874,27 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
   double* T = (double*)(ws + L.T);
   constexpr int K = n_nodes(P);
   CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
-  k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(r->mu, r->lam, coef);
-  k_prep<<<(unsigned)((r->n_src + 127) / 128), 128, 0, st>>>(r->n_src, r->tris, r->eps, r->fold,
-                                                              KC != KD_E, prep, G);
+  {
+    StageTimer t(MHS_STAGE_PREP, st);
+    k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(r->mu, r->lam, coef);
+    k_prep<<<(unsigned)((r->n_src + 127) / 128), 128, 0, st>>>(r->n_src, r->tris, r->eps, r->fold,
+                                                                KC != KD_E, prep, G);
+  }
   const bool cont = r->ids != nullptr;
   const int64_t n_dof = cont ? r->n_cols : r->n_src * K;
   for (int64_t lo = 0; lo < r->n_obs; lo += L.chunk) {
     const int64_t nc = std::min<int64_t>(L.chunk, r->n_obs - lo);
     dim3 g((unsigned)((nc + TB - 1) / TB), (unsigned)r->n_src);
-    k_pair<P, KC><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, G, coef, r->mu, r->lam, T);
-    if constexpr (KC != KD_E)
+    {
+      StageTimer t(MHS_STAGE_PAIR, st);
+      k_pair<P, KC><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, G, coef, r->mu, r->lam, T);
+    }
+    if constexpr (KC != KD_E) {
+      StageTimer t(MHS_STAGE_IMAGEQ, st);
       k_imageq<P, KC><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, coef, r->mu, r->lam, T);
+    }
     if (r->fold) {
+      StageTimer t(MHS_STAGE_FOLD, st);
       k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
       dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
       const size_t fsm = sizeof(FoldShared<P, KC>);
@@ -849,6 +902,7 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
       k_fold<P, KC><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
                                                       r->mu, r->lam, T, status);
     }
+    StageTimer tfin(MHS_STAGE_FINAL, st);
     FinalArgs a;
     a.kind = r->kind;
     a.subtract = r->subtract_eigenstress;
@@ -1040,6 +1094,61 @@ int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, c
     case 2: return debug_terms<2>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
   }
   return fail(MHS_ERR_ARG, "order");
+}
+
+int mhs_profile_enable(int on) {
+  __atomic_store_n(&g_prof_on, on ? 1 : 0, __ATOMIC_RELAXED);
+  return MHS_OK;
+}
+
+int mhs_profile_read(double* ms, int* launches) {
+  std::vector<ProfRec> recs;
+  {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    recs.swap(g_prof);
+  }
+  for (int i = 0; i < MHS_N_STAGES; ++i) {
+    if (ms) ms[i] = 0.0;
+    if (launches) launches[i] = 0;
+  }
+  int rc = MHS_OK;
+  for (auto& r : recs) {
+    float t = 0.0f;
+    if (cudaEventSynchronize(r.b) != cudaSuccess || cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess)
+      rc = fail(MHS_ERR_CUDA, "profile event");
+    if (ms) ms[r.stage] += t;
+    if (launches) launches[r.stage] += 1;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  return rc;
+}
+
+int mhs_fp_peak(int fp64, int iters, double* tflops, void* stream) {
+  int rc = ensure_device_tables();
+  if (rc) return rc;
+  int dev = 0, sms = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int blocks = sms * 8, threads = 256;
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  float ms = 0.0f;
+  for (int rep = 0; rep < 2; ++rep) {  // first pass warms up
+    CUDA_TRY(cudaEventRecord(a, st));
+    if (fp64) k_fma_peak<double><<<blocks, threads, 0, st>>>(nullptr, iters, 0.999999, 1e-7);
+    else k_fma_peak<float><<<blocks, threads, 0, st>>>(nullptr, iters, 0.999999f, 1e-7f);
+    CUDA_TRY(cudaEventRecord(b, st));
+    CUDA_TRY(cudaEventSynchronize(b));
+    CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+  if (tflops) *tflops = flops / (ms * 1e-3) / 1e12;
+  return MHS_OK;
 }
 
 const char* mhs_last_error(void) { return g_err; }

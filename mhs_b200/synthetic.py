@@ -33,7 +33,8 @@ def _strike_dip_vectors(strike_deg: float, dip_deg: float):
 
 def _grid_tris(P: np.ndarray) -> np.ndarray:
     """Triangles of a vertex grid ``P (nu+1, nv+1, 3)``: each cell split along
-    its diagonal into (a, b, c) and (a, c, d)."""
+    its diagonal, wound so the vertex-order normal points up (n_z >= 0; a
+    vertical plane keeps the grid's own consistent winding)."""
     nu, nv = P.shape[0] - 1, P.shape[1] - 1
     a = P[:-1, :-1]
     b = P[1:, :-1]
@@ -41,7 +42,11 @@ def _grid_tris(P: np.ndarray) -> np.ndarray:
     d = P[:-1, 1:]
     t1 = np.stack([a, b, c], axis=2)
     t2 = np.stack([a, c, d], axis=2)
-    return np.stack([t1, t2], axis=2).reshape(nu * nv * 2, 3, 3)
+    t = np.stack([t1, t2], axis=2).reshape(nu * nv * 2, 3, 3)
+    n = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0])
+    if np.median(n[:, 2]) < 0.0:
+        t = t[:, [0, 2, 1], :]
+    return np.ascontiguousarray(t)
 
 
 def planar_vertices(strike_deg, dip_deg, length, width, top_z, nu, nv, centre=(0.0, 0.0)):
@@ -118,8 +123,6 @@ def fault_network(length=80.0, depth=15.0, splay_len=40.0, splay_width=15.0, nu=
         P[:, 0, 1] = 0.0
         P[:, 0, 2] = -depth
         t = _grid_tris(P)
-        if side < 0:
-            t = t[:, ::-1, :].copy()   # keep the winding upward on both splays
         tris.append(t)
         ids.append(np.full(t.shape[0], len(ids), dtype=np.int64))
     return np.concatenate(tris), np.concatenate(ids)

@@ -1,0 +1,69 @@
+"""CUDA path against the numpy oracle on seeded inputs, FP64, relmax <= 1e-12.
+
+Sizes are small enough for the oracle to finish in seconds; every kind,
+order, layout and the fold are covered."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import relmax
+from mhs_b200 import synthetic
+from oracle import mhs_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+MU, LAM = 30.0, 22.0
+
+
+def _case(seed, top=-0.8, n=(3, 2)):
+    rng = np.random.default_rng(seed)
+    tris = synthetic.planar_fault(rng.uniform(0, 90), rng.uniform(30, 90), 3.0, 2.0, top, *n)
+    obs = np.concatenate([rng.uniform([-3, -3, -3], [3, 3, 0], (10, 3)),
+                          rng.uniform([-30, -30, -20], [30, 30, 0], (6, 3))])
+    return tris, obs
+
+
+@pytest.mark.parametrize("p", [0, 1, 2])
+@pytest.mark.parametrize("seed", [1, 2])
+def test_kinds_against_oracle(cuda, p, seed):
+    import mhs_b200 as m
+    tris, obs = _case(seed)
+    mat = m.Material(MU, LAM)
+    eps = 0.12
+    assert relmax(m.disp_matrix(obs, tris, mat, eps, order=p), O.disp_matrix(obs, tris, MU, LAM, eps, p)) < TOL
+    S = O.stress_matrix(obs, tris, MU, LAM, eps, p)
+    assert relmax(m.stress_matrix(obs, tris, mat, eps, order=p), S) < TOL
+    E = O.eigenstress_matrix(obs, tris, MU, LAM, eps, p)
+    assert relmax(m.eigenstress_matrix(obs, tris, mat, eps, order=p), E) < TOL
+    assert relmax(m.elastic_strain_matrix(obs, tris, mat, eps, order=p),
+                  O.elastic_strain_matrix(obs, tris, MU, LAM, eps, p)) < TOL
+    nrm = np.random.default_rng(seed).standard_normal(obs.shape)
+    assert relmax(m.traction_matrix(obs, nrm, tris, mat, eps, order=p),
+                  O.traction_matrix(obs, nrm, tris, MU, LAM, eps, p)) < TOL
+
+
+def test_fold_and_per_triangle_eps(cuda):
+    import mhs_b200 as m
+    c = synthetic.config2(seed=5, nu=3, nv=2)
+    mat = m.Material(c["mu"], c["lam"])
+    K = m.interaction_matrix(c["tris"], mat, c["eps"])
+    R = O.self_interaction(c["tris"], c["mu"], c["lam"], c["eps"])
+    assert relmax(K, R) < TOL
+    rng = np.random.default_rng(3)
+    obs = np.column_stack([rng.uniform(-15, 15, 5), rng.uniform(-2, 5, 5), -rng.uniform(0, 2, 5)])
+    assert relmax(m.disp_matrix(obs, c["tris"], mat, c["eps"]),
+                  O.disp_matrix(obs, c["tris"], c["mu"], c["lam"], c["eps"])) < TOL
+
+
+def test_continuous_p2_against_oracle(cuda):
+    import mhs_b200 as m
+    tris = synthetic.planar_fault(20.0, 70.0, 3.0, 2.0, -0.5, 3, 2)
+    sn = m.shared_nodes(tris)
+    mat = m.Material(MU, LAM)
+    K = m.interaction_matrix(tris, mat, 0.1, order=2, layout="continuous", shared=sn,
+                             receiver=("strike", "normal"), source=("dip",))
+    fr = sn.frames
+    R = O.interaction_matrix(sn.coords, fr[:, 2, :], fr[:, [0, 2], :], tris, fr[:, [1], :], MU, LAM,
+                             0.1, 2, ids=sn.ids, n_dof=sn.n)
+    assert relmax(K, R) < TOL
