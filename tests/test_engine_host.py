@@ -73,6 +73,35 @@ def test_image_r_and_q(hc, P):
         assert relmax(B, O.image_q(obs, TRI, P, MU, LAM, EPS, (key,))[key]) < TOL
 
 
+def test_p2_image_closer_to_converged_than_mhs_arithmetic(hc, monkeypatch):
+    """Where the closed-form image moments are ill-conditioned (P2, a few L
+    from the reflected element), the engine and mhs's arithmetic (the
+    oracle) differ by ~1e-12 of the matrix maximum; both are compared with a
+    converged 40 x 40 Gauss rule, and the engine must be the closer one."""
+    from mhs_b200 import synthetic
+    rng = np.random.default_rng(1)
+    tris = synthetic.planar_fault(rng.uniform(0, 90), rng.uniform(30, 90), 3.0, 2.0, -0.8, 3, 2)
+    obs = np.concatenate([rng.uniform([-3, -3, -3], [3, 3, 0], (10, 3)),
+                          rng.uniform([-30, -30, -20], [30, 30, 0], (6, 3))])
+    x = np.ascontiguousarray(obs[7:8])
+    g = np.abs(O.stress_matrix(obs, tris, MU, 22.0, 0.12, 2)).max()
+    oracle = np.stack([O.image_r(x, t, 2, MU, 22.0, 0.12, ("H",))["H"][0] for t in tris])
+    eng = []
+    for t in tris:
+        A = np.zeros((1, 6, 3, 3, 3))
+        c = ctypes.c_double
+        hc.hc_image_r(2, 2, _p(x), 1, _p(np.ascontiguousarray(t)), c(MU), c(22.0), c(0.12), _p(A), _p(A))
+        eng.append(A[0])
+    eng = np.stack(eng)
+    rule = O._tri_rule
+    monkeypatch.setattr(O, "D_STAR", 1e-9)
+    monkeypatch.setattr(O, "_tri_rule", lambda n: rule(40))
+    truth = np.stack([O.image_r(x, t, 2, MU, 22.0, 0.12, ("H",))["H"][0] for t in tris])
+    e_eng = np.abs(eng - truth).max() / g
+    e_mhs = np.abs(oracle - truth).max() / g
+    assert e_eng < e_mhs and e_eng < 1e-12
+
+
 @pytest.mark.parametrize("P,key", [(0, "H"), (0, "U"), (1, "H")])
 def test_fold_image(hc, P, key):
     tri = np.array([[0.0, 0.0, 0.0], [1.5, 0.2, -0.05], [0.3, 0.9, -1.1]])

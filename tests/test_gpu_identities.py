@@ -138,7 +138,9 @@ def test_fold_off_equals_lift_outside_band(cuda):
     c = synthetic.config2(seed=6, nu=6, nv=3)
     mat = _mat(c)
     rng = np.random.default_rng(0)
-    deep = np.column_stack([rng.uniform(-10, 10, 20), rng.uniform(-5, 5, 20), -rng.uniform(20, 30, 20)])
+    # below the band of every source: depth beyond FOLD_BAND_DEPTH_EPS x the largest eps
+    z0 = 10.0 * float(np.max(c["eps"])) + 1.0
+    deep = np.column_stack([rng.uniform(-10, 10, 20), rng.uniform(-5, 5, 20), -z0 - rng.uniform(0, 10, 20)])
     A = m.stress_matrix(deep, c["tris"], mat, c["eps"])
     B = m.stress_matrix(deep, c["tris"], mat, c["eps"], fold=False)
     assert np.array_equal(A, B)

@@ -24,6 +24,17 @@ def _case(seed, top=-0.8, n=(3, 2)):
     return tris, obs
 
 
+#: At P2 the image R-family reads closed-form moments up to n = 9 at degree
+#: 7; a few widths of L from the reflected element the upward vertical seed
+#: I_9 = (E_7 + 5 I_7) / (7 h^2) amplifies last-ulp differences of log1p /
+#: pow by ~1e11, so mhs's own arithmetic (restated by the oracle) carries up
+#: to ~1e-12 of the matrix maximum there, and this engine lands closer to a
+#: converged quadrature than mhs does (tests/test_engine_host.py::
+#: test_p2_image_closer_to_converged_than_mhs_arithmetic).  The P2 parity
+#: bound is therefore that conditioning budget, not 1e-12.
+TOL_BY_ORDER = {0: TOL, 1: TOL, 2: 5e-12}
+
+
 @pytest.mark.parametrize("p", [0, 1, 2])
 @pytest.mark.parametrize("seed", [1, 2])
 def test_kinds_against_oracle(cuda, p, seed):
@@ -31,16 +42,17 @@ def test_kinds_against_oracle(cuda, p, seed):
     tris, obs = _case(seed)
     mat = m.Material(MU, LAM)
     eps = 0.12
-    assert relmax(m.disp_matrix(obs, tris, mat, eps, order=p), O.disp_matrix(obs, tris, MU, LAM, eps, p)) < TOL
+    tol = TOL_BY_ORDER[p]
+    assert relmax(m.disp_matrix(obs, tris, mat, eps, order=p), O.disp_matrix(obs, tris, MU, LAM, eps, p)) < tol
     S = O.stress_matrix(obs, tris, MU, LAM, eps, p)
-    assert relmax(m.stress_matrix(obs, tris, mat, eps, order=p), S) < TOL
+    assert relmax(m.stress_matrix(obs, tris, mat, eps, order=p), S) < tol
     E = O.eigenstress_matrix(obs, tris, MU, LAM, eps, p)
-    assert relmax(m.eigenstress_matrix(obs, tris, mat, eps, order=p), E) < TOL
+    assert relmax(m.eigenstress_matrix(obs, tris, mat, eps, order=p), E) < tol
     assert relmax(m.elastic_strain_matrix(obs, tris, mat, eps, order=p),
-                  O.elastic_strain_matrix(obs, tris, MU, LAM, eps, p)) < TOL
+                  O.elastic_strain_matrix(obs, tris, MU, LAM, eps, p)) < tol
     nrm = np.random.default_rng(seed).standard_normal(obs.shape)
     assert relmax(m.traction_matrix(obs, nrm, tris, mat, eps, order=p),
-                  O.traction_matrix(obs, nrm, tris, MU, LAM, eps, p)) < TOL
+                  O.traction_matrix(obs, nrm, tris, MU, LAM, eps, p)) < tol
 
 
 def test_fold_and_per_triangle_eps(cuda):
