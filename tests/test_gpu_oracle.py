@@ -33,6 +33,11 @@ def _case(seed, top=-0.8, n=(3, 2)):
 #: test_p2_image_closer_to_converged_than_mhs_arithmetic).  The P2 parity
 #: bound is therefore that conditioning budget, not 1e-12.
 TOL_BY_ORDER = {0: TOL, 1: TOL, 2: 5e-12}
+#: The eigenstress matrix peaks on the element and decays like R^-7, so its
+#: far tail -- the blob weight, from the same upward seed I_7 -- is ~1e-5 of
+#: its maximum and carries mhs's rounding at ~1e-15 absolute: 1e-11 of the
+#: maximum at P2 (the engine is ~30x closer to a converged quadrature there).
+TOL_EIGEN_BY_ORDER = {0: TOL, 1: TOL, 2: 3e-11}
 
 
 @pytest.mark.parametrize("p", [0, 1, 2])
@@ -47,7 +52,7 @@ def test_kinds_against_oracle(cuda, p, seed):
     S = O.stress_matrix(obs, tris, MU, LAM, eps, p)
     assert relmax(m.stress_matrix(obs, tris, mat, eps, order=p), S) < tol
     E = O.eigenstress_matrix(obs, tris, MU, LAM, eps, p)
-    assert relmax(m.eigenstress_matrix(obs, tris, mat, eps, order=p), E) < tol
+    assert relmax(m.eigenstress_matrix(obs, tris, mat, eps, order=p), E) < TOL_EIGEN_BY_ORDER[p]
     assert relmax(m.elastic_strain_matrix(obs, tris, mat, eps, order=p),
                   O.elastic_strain_matrix(obs, tris, MU, LAM, eps, p)) < tol
     nrm = np.random.default_rng(seed).standard_normal(obs.shape)
