@@ -90,6 +90,37 @@ int mhs_workspace_bytes(const mhs_request* req, size_t* min_bytes, size_t* good_
  * subtraction and strain readout of matrices.py:287-294 and :572-579. */
 int mhs_assemble(const mhs_request* req, void* stream);
 
+/* Allocation-free variant of mhs_assemble, for callers that must not
+ * allocate device memory while they run: a solver whose memory pool owns
+ * the device after start-up, a host framework that pre-reserves nearly all
+ * of HBM (so even a small cudaMalloc can fail or stall), or real-time code
+ * where an allocation's implicit synchronisation is not allowed.  It takes
+ * the same request -- the caller still owns inputs and output -- but
+ * ignores workspace / workspace_bytes and uses one fixed scratch array
+ * inside this library instead (MHS_NOALLOC_SCRATCH_BYTES per device, held
+ * by every device that loads the library until the process exits).  It
+ * calls no cudaMalloc or cudaFree.
+ *
+ * Limit: the request's per-source tables plus one observer row of
+ * per-pair tensors must fit the array (about 8.6 KB per source at P2,
+ * so a few thousand sources per call); larger requests are refused with
+ * MHS_ERR_WORKSPACE and a message that says so, and observers beyond what
+ * fits in one pass are processed in chunks.
+ *
+ * The first call on each device does one-time set-up with that device
+ * current (the Gauss-Legendre tables and the scratch array's device
+ * address, via cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Every call shares the one array and it keeps the last
+ * call's contents (the pipeline clears what must start at zero), so calls
+ * whose work overlaps on the GPU -- on different streams, or from
+ * different threads -- race: serialise them.
+ *
+ * status_bits: NULL to return once queued; otherwise the call synchronises
+ * `stream` and stores the device status bits there.
+ * No counterpart in mhs (which never runs on a device). */
+#define MHS_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits);
+
 /* Synchronise `stream` and return the device status bits of the last
  * request that used `workspace` (0 = clean), clearing them. */
 int mhs_read_status(void* workspace, void* stream, int* bits);

@@ -946,6 +946,31 @@ int run_kind(const mhs_request* r, cudaStream_t st, const Layout& L) {
 
 constexpr size_t GOOD_T_BYTES = size_t(2) << 30;
 
+// ------------------------------------------- allocation-free scratch
+// Scratch of mhs_assemble_noalloc: one file-scope device array that every
+// device loading this library holds until the process exits.  Host code
+// never dereferences the symbol; it passes the device address that
+// cudaGetSymbolAddress returns, looked up once per device.
+__device__ __align__(256) unsigned char g_noalloc_scratch[MHS_NOALLOC_SCRATCH_BYTES];
+std::mutex g_noalloc_mu;
+std::vector<void*> g_noalloc_ptr;
+
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if ((int)g_noalloc_ptr.size() <= dev) g_noalloc_ptr.resize(dev + 1, nullptr);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(MHS_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return MHS_OK;
+}
+
 // ---------------------------------------------------- per-term diagnostics
 // One source, n observers, one thread per observer: a single influence term
 // exactly as the pipeline evaluates it.  term 0 direct (H + E or U), 1 image
@@ -1054,6 +1079,45 @@ int mhs_assemble(const mhs_request* req, void* stream) {
     case 1: return run_kind<1>(req, st, L);
     default: return run_kind<2>(req, st, L);
   }
+}
+
+int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits) {
+  int rc = check_request(req);
+  if (rc) return rc;
+  rc = ensure_device_tables();
+  if (rc) return rc;
+  void* scratch = nullptr;
+  rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  const size_t cap = MHS_NOALLOC_SCRATCH_BYTES;
+  const Layout one = plan(req, 1);
+  if (one.total > cap)
+    return fail(MHS_ERR_WORKSPACE,
+                "request needs %zu bytes of scratch for one observer row, above the %zu-byte "
+                "array of the allocation-free entry point (MHS_NOALLOC_SCRATCH_BYTES); pass "
+                "fewer sources per call or use mhs_assemble with a caller workspace",
+                one.total, cap);
+  int64_t lo = 1, hi = std::min<int64_t>(req->n_obs, 65535);
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo + 1) / 2;
+    if (plan(req, mid).total <= cap) lo = mid;
+    else hi = mid - 1;
+  }
+  mhs_request r = *req;
+  r.workspace = scratch;
+  r.workspace_bytes = cap;
+  const Layout L = plan(&r, lo);
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (r.order) {
+    case 0: rc = run_kind<0>(&r, st, L); break;
+    case 1: rc = run_kind<1>(&r, st, L); break;
+    default: rc = run_kind<2>(&r, st, L); break;
+  }
+  if (rc || !status_bits) return rc;
+  CUDA_TRY(cudaMemcpyAsync(status_bits, (char*)scratch + L.status, sizeof(int),
+                           cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return MHS_OK;
 }
 
 int mhs_read_status(void* workspace, void* stream, int* bits) {
