@@ -134,7 +134,9 @@ int mhs_column_plan(const int64_t* ids_host, int64_t n_src, int64_t n_cols, int3
 
 /* Diagnostics: one influence term of ONE source at n observers, one thread
  * per observer, as the pipeline evaluates it (term 0 direct, 1 image
- * R-family, 2 image Q-family, 3 folded image).  out (device) receives per
+ * R-family, 2 image Q-family, 3 folded image; with want_u = 0, 4 and 5 the
+ * fold's surface load at (x, y, 0) as K x 3 values, from the contracted
+ * sigma_zz row and from the full stress kernel).  out (device) receives per
  * observer K x C values (C = 9 for want_u, else 27) then K blob weights.
  * coef_scratch: device buffer of at least 4096 doubles.  No counterpart in
  * mhs; the per-term split follows mhs/kernels/assemble.py:96-120. */

@@ -363,6 +363,104 @@ MHS_HD void fold_surface_load(const Frame& f, const QuadRule& r12, const QuadRul
     for (int j = 0; j < 3; ++j) s[3 * k + j] = 2.0 * (H[27 * k + 9 * 2 + 3 * 2 + j] - E[k] * ezz[j]);
 }
 
+// Per-source constants of the surface load: the global sigma_zz row of H
+// as a linear form in the lifted quantities (per slip component), the
+// eigenstress zz factor per slip component, and the blob-weight factor.
+struct SurfaceLoadConsts {
+  double coef[3][NLIFT];
+  double ezz[3];
+  double e4;
+};
+
+MHS_HD void surface_load_ezz(const Frame& f, double eps, const Material& m, SurfaceLoadConsts& c) {
+  for (int j = 0; j < 3; ++j) c.ezz[j] = m.lam * f.n[j] + (j == 2 ? 2.0 * m.mu * f.n[2] : 0.0);
+  c.e4 = 15.0 * (eps * eps) * (eps * eps) / (8.0 * cst::PI);
+}
+
+MHS_HD void surface_load_consts(const Frame& f, double eps, const Material& m, SurfaceLoadConsts& c) {
+  for (int l = 0; l < NLIFT; ++l) {
+    double col[3] = {};
+    szz_coefficient(f, eps, m, l, col);
+    for (int j = 0; j < 3; ++j) c.coef[j][l] = col[j];
+  }
+  surface_load_ezz(f, eps, m, c);
+}
+
+// Surface load of one node from its weighted moments W (one node's block):
+// each lifted quantity goes straight into the three sigma_zz accumulators.
+MHS_FI void szz_acc(const SurfaceLoadConsts& c, int l, double v, double& a0, double& a1,
+                    double& a2) {
+  a0 += c.coef[0][l] * v;
+  a1 += c.coef[1][l] * v;
+  a2 += c.coef[2][l] * v;
+}
+
+template <class S>
+MHS_HD void surface_load_node(const SurfaceLoadConsts& c, const double* W, double z, double* s3) {
+  constexpr Spec sp = S::spec;
+  constexpr int o3 = sp.w_off[nslot(3)], o5 = sp.w_off[nslot(5)], o7 = sp.w_off[nslot(7)];
+  const double zp[5] = {1.0, z, z * z, z * z * z, z * z * z * z};
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  szz_acc(c, L_I3, W[o3], a0, a1, a2);
+  szz_acc(c, L_I5, W[o5], a0, a1, a2);
+#pragma unroll
+  for (int ca = 0; ca <= 2; ++ca)
+#pragma unroll
+    for (int cb = 0; ca + cb <= 2; ++cb) {
+      const double sg = ((ca + cb) & 1) ? -zp[2 - ca - cb] : zp[2 - ca - cb];
+      szz_acc(c, L_T25 + tri_idx(ca, cb), sg * W[o5 + tri_idx(ca, cb)], a0, a1, a2);
+      szz_acc(c, L_T27 + tri_idx(ca, cb), sg * W[o7 + tri_idx(ca, cb)], a0, a1, a2);
+    }
+#pragma unroll
+  for (int ca = 0; ca <= 4; ++ca)
+#pragma unroll
+    for (int cb = 0; ca + cb <= 4; ++cb) {
+      const double sg = ((ca + cb) & 1) ? -zp[4 - ca - cb] : zp[4 - ca - cb];
+      szz_acc(c, L_T47 + tri_idx(ca, cb), sg * W[o7 + tri_idx(ca, cb)], a0, a1, a2);
+    }
+  const double E = c.e4 * W[o7];
+  s3[0] = 2.0 * (a0 - E * c.ezz[0]);
+  s3[1] = 2.0 * (a1 - E * c.ezz[1]);
+  s3[2] = 2.0 * (a2 - E * c.ezz[2]);
+}
+
+// The same surface load as fold_surface_load, reading only sigma_zz: the
+// weighted moments of each node (as direct_eval forms them), contracted with
+// the precomputed sigma_zz row instead of the full H assembly and rotation.
+template <int P, class R_FAR = double>
+MHS_HD void fold_surface_load_fast(const Frame& f, const QuadRule& r12, const QuadRule& r8,
+                                   const SurfaceLoadConsts& c, double px, double py, double eps,
+                                   double* s /*K x 3*/) {
+  using S = DirectSpec<P, W_H | W_E>;
+  constexpr Spec sp = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = sp.w_off[NS];
+  const double x[3] = {px, py, 0.0};
+  const double d0 = x[0] - f.c[0], d1 = x[1] - f.c[1], d2 = x[2] - f.c[2];
+  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
+  double z, X0, X1;
+  to_plane(f, x, z, X0, X1);
+  const double h2 = z * z + eps * eps;
+  if (D <= cst::D_STAR * f.L) {
+    MomentTable<S> T;
+    closed_moments<S>(f, X0, X1, h2, T);
+    double cc[K][ntri(P)] = {};
+    shape_coeffs<P>(f, X0, X1, cc);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double W[NW] = {};
+      weight_closed<S, P>(T, cc, k, W);
+      surface_load_node<S>(c, W, z, s + 3 * k);
+    }
+  } else {
+    const QuadRule& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
+    double W[K * NW] = {};
+    weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
+#pragma unroll
+    for (int k = 0; k < K; ++k) surface_load_node<S>(c, W + k * NW, z, s + 3 * k);
+  }
+}
+
 // Scalar reference walk of one band pair's Boussinesq correction, for the
 // host test build and for small launches: H[k][a][b][m] (WANT_H) or
 // U[k][i][m].  Returns 0, or -1 if the grid overflowed its capacity.
@@ -380,8 +478,10 @@ MHS_HD int fold_boussinesq_scalar(const Frame& f, const QuadRule& r12, const Qua
   double br[FOLD_MAX_BREAKS];
   const int nb = fold_breaks(fp.rho_s, fp.zeta, r_f, eps, diam, br, &fp.R1);
   if (nb < 0) return -1;
-  double sh[3 * K];
-  fold_surface_load<P>(f, r12, r8, x[0], x[1], eps, m, sh);
+  SurfaceLoadConsts slc;
+  surface_load_consts(f, eps, m, slc);
+  double sh[3 * K] = {};
+  fold_surface_load_fast<P>(f, r12, r8, slc, x[0], x[1], eps, sh);
   const double* gx6 = glx + gl_offset(cst::FOLD_N_RADIAL);
   const double* gw6 = glw + gl_offset(cst::FOLD_N_RADIAL);
   const double* gx4 = glx + gl_offset(cst::FOLD_N_ANGULAR);
@@ -404,8 +504,8 @@ MHS_HD int fold_boussinesq_scalar(const Frame& f, const QuadRule& r12, const Qua
         fold_ang_node(A, gx4, gw4, j, &th, &wt);
         const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
         const double w = wr * wt * R;
-        double s[3 * K];
-        fold_surface_load<P>(f, r12, r8, px, py, eps, m, s);
+        double s[3 * K] = {};
+        fold_surface_load_fast<P>(f, r12, r8, slc, px, py, eps, s);
         double B[NC];
         if (WANT_H) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, B);
         else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, B);

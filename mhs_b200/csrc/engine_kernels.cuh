@@ -94,23 +94,47 @@ MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, cons
   rotate2(f, Ul, U);
 }
 
-// Slip -> total stress (mhs/fullspace/kernels.py:182-210), in the element frame.
+// Lifted local-frame quantities of the stress kernel, one vector per node:
+// I3, I5, then T25(a, b) and T27(a, b) over the six components of a
+// symmetric rank-2 tensor and T47 over the fifteen of a symmetric rank-4
+// tensor, each at tri_idx(count of e1, count of e2).  H is linear in them.
+constexpr int NLIFT = 29;
+constexpr int L_I3 = 0, L_I5 = 1, L_T25 = 2, L_T27 = 8, L_T47 = 14;
+
 template <class S>
-MHS_HD void kernel_H(const Frame& f, const double* W, double z, double eps, const Material& m,
-                     double* H) {
-  double zp[5] = {1.0, z, z * z, z * z * z, z * z * z * z};
+MHS_HD void lift_H(const double* W, double z, double* L) {
+  const double zp[5] = {1.0, z, z * z, z * z * z, z * z * z * z};
   const int s5 = nslot(5), s7 = nslot(7);
   constexpr Spec sp = S::spec;
-  const double I3 = W[sp.w_off[nslot(3)]];
-  const double I5 = W[sp.w_off[nslot(5)]];
+  L[L_I3] = W[sp.w_off[nslot(3)]];
+  L[L_I5] = W[sp.w_off[nslot(5)]];
+#pragma unroll
+  for (int ca = 0; ca <= 2; ++ca)
+#pragma unroll
+    for (int cb = 0; ca + cb <= 2; ++cb) {
+      L[L_T25 + tri_idx(ca, cb)] = lift_local<S>(W, s5, ca, cb, 2 - ca - cb, zp);
+      L[L_T27 + tri_idx(ca, cb)] = lift_local<S>(W, s7, ca, cb, 2 - ca - cb, zp);
+    }
+#pragma unroll
+  for (int ca = 0; ca <= 4; ++ca)
+#pragma unroll
+    for (int cb = 0; ca + cb <= 4; ++cb)
+      L[L_T47 + tri_idx(ca, cb)] = lift_local<S>(W, s7, ca, cb, 4 - ca - cb, zp);
+}
+
+// Slip -> total stress (mhs/fullspace/kernels.py:182-210) from the lifted
+// quantities, assembled in the element frame and rotated.
+MHS_HD void H_from_lift(const Frame& f, const double* L, double eps, const Material& m, double* H) {
+  const double I3 = L[L_I3];
+  const double I5 = L[L_I5];
   const double e2 = eps * eps;
   const double f2 = 2.0 * m.one_m_nu * e2;
   double T25[3][3], T27[3][3];
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
       const int ca = (i == 0) + (j == 0), cb = (i == 1) + (j == 1);
-      T25[i][j] = lift_local<S>(W, s5, ca, cb, 2 - ca - cb, zp);
-      T27[i][j] = lift_local<S>(W, s7, ca, cb, 2 - ca - cb, zp);
+      T25[i][j] = L[L_T25 + tri_idx(ca, cb)];
+      T27[i][j] = L[L_T27 + tri_idx(ca, cb)];
     }
   // D2[r][p][s][q] / C1
   double D2[3][3][3][3];
@@ -122,7 +146,7 @@ MHS_HD void kernel_H(const Frame& f, const double* W, double z, double eps, cons
                        drq = r == q;
           const int ca = (r == 0) + (p == 0) + (s == 0) + (q == 0);
           const int cb = (r == 1) + (p == 1) + (s == 1) + (q == 1);
-          const double T47 = lift_local<S>(W, s7, ca, cb, 4 - ca - cb, zp);
+          const double T47 = L[L_T47 + tri_idx(ca, cb)];
           double d = -m.c34 * (drp * dsq * I3 - 3.0 * (drp * T25[s][q]));
           d += drs * dpq * I3 - 3.0 * (drs * T25[p][q]);
           d += dps * drq * I3 - 3.0 * (dps * T25[r][q]);
@@ -148,12 +172,33 @@ MHS_HD void kernel_H(const Frame& f, const double* W, double z, double eps, cons
   rotate3(f, Hl, H);
 }
 
+template <class S>
+MHS_HD void kernel_H(const Frame& f, const double* W, double z, double eps, const Material& m,
+                     double* H) {
+  double L[NLIFT] = {};
+  lift_H<S>(W, z, L);
+  H_from_lift(f, L, eps, m, H);
+}
+
+// Coefficients of the global sigma_zz row: H[2][2][j] = sum_l col[l][j] L_l,
+// read off by evaluating H_from_lift on the unit vector of lifted slot l.
+MHS_HD void szz_coefficient(const Frame& f, double eps, const Material& m, int l, double* col3) {
+  double e[NLIFT] = {};
+  e[l] = 1.0;
+  double H[27] = {};
+  H_from_lift(f, e, eps, m, H);
+  for (int j = 0; j < 3; ++j) col3[j] = H[9 * 2 + 3 * 2 + j];
+}
+
 // ----------------------------------------------------------- direct term
 // One source triangle at one observer, all K nodes: near field by the
 // closed-form recursion (sqrt(|x - c|^2 + eps^2) <= D_STAR L), far field by
 // the 12x12 (8x8 beyond D_STAR_DISTANT L) product rule
 // (mhs/fullspace/moments.py:551-601, mhs/fullspace/kernels.py:126-215).
 // R_FAR is the arithmetic type of the far-field quadrature.
+// The node loops are fully unrolled so that every output offset is a
+// compile-time constant: a -O3 device build with them kept rolled returned
+// wrong P >= 1 tensors where this function is inlined into the fold kernels.
 template <int P, int WANT, class R_FAR = double>
 MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
                         const double* x, double eps, const Material& m,
@@ -173,7 +218,7 @@ MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
     closed_moments<S>(f, X0, X1, h2, T);
     double c[K][ntri(P)];
     shape_coeffs<P>(f, X0, X1, c);
-#pragma unroll 1
+#pragma unroll
     for (int k = 0; k < K; ++k) {
       double W[NW] = {};
       weight_closed<S, P>(T, c, k, W);
@@ -185,7 +230,7 @@ MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
     const QuadRule& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
     double W[K * NW] = {};
     weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
-#pragma unroll 1
+#pragma unroll
     for (int k = 0; k < K; ++k) {
       if (WANT & W_U) kernel_U<S>(f, W + k * NW, z, eps, m, U + 9 * k);
       if (WANT & W_H) kernel_H<S>(f, W + k * NW, z, eps, m, H + 27 * k);

@@ -411,6 +411,7 @@ struct FoldShared {
   SrcPrep sp;
   SmemRules<P> rd;       // element (surface load)
   SmemRules<P> rm;       // mirror element (its full-space field)
+  SurfaceLoadConsts slc; // sigma_zz row of the element's H, per slip component
   double brk[FOLD_WARPS][FOLD_MAX_BREAKS];
   double sh_load[FOLD_WARPS][NJ];
   double sB[FOLD_WARPS][32][NC];
@@ -455,17 +456,26 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   auto& sbrk_n = sh.sbrk_n;
   auto& sR1 = sh.sR1;
   auto& outv = sh.outv;
+  const Material m = make_material(mu, lam);
   if (threadIdx.x == 0) sp = prep[s];
   __syncthreads();
   rd.build(sp.f, threadIdx.x, 32 * FOLD_WARPS);
   rm.build(sp.fi, threadIdx.x, 32 * FOLD_WARPS);
+  if (KC != KD_E) {
+    static_assert(NLIFT <= 32 * FOLD_WARPS, "one thread per lifted slot");
+    if (threadIdx.x < NLIFT) {
+      double col[3] = {};
+      szz_coefficient(sp.f, sp.eps, m, threadIdx.x, col);
+      for (int j = 0; j < 3; ++j) sh.slc.coef[j][threadIdx.x] = col[j];
+    }
+    if (threadIdx.x == 32) surface_load_ezz(sp.f, sp.eps, m, sh.slc);
+  }
   __syncthreads();
   const int bi = blockIdx.x * FOLD_WARPS + wid;
   if (bi >= n_band) return;
   const int64_t oc = list[s * n_chunk + bi];
   const int64_t o = lo + oc;
   const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const Material m = make_material(mu, lam);
   const double eps = sp.eps;
   double* row = T + ((oc * n_src + s) * K) * NR;
   const QuadRule r12 = rd.r12(), r8 = rd.r8();
@@ -484,7 +494,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
       sbrk_n[wid] = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, brk[wid], &R1);
       sR1[wid] = R1;
       double sl[NJ] = {};
-      fold_surface_load<P>(sp.f, r12, r8, x[0], x[1], eps, m, sl);
+      fold_surface_load_fast<P>(sp.f, r12, r8, sh.slc, x[0], x[1], eps, sl);
       for (int j = 0; j < NJ; ++j) sh_load[wid][j] = sl[j];
     }
     __syncwarp();
@@ -522,7 +532,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
           fold_ang_node(A, gx4, gw4, j, &th, &wt);
           const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
           const double w = wr * wt * R;
-          fold_surface_load<P>(sp.f, r12, r8, px, py, eps, m, sv);
+          fold_surface_load_fast<P>(sp.f, r12, r8, sh.slc, px, py, eps, sv);
           if (WH) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, Bv);
           else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, Bv);
           for (int c = 0; c < NC; ++c) sB[wid][lane][c] = w * Bv[c];
@@ -974,7 +984,9 @@ int noalloc_scratch(void** out) {
 // ---------------------------------------------------- per-term diagnostics
 // One source, n observers, one thread per observer: a single influence term
 // exactly as the pipeline evaluates it.  term 0 direct (H + E or U), 1 image
-// R-family, 2 image Q-family, 3 folded image (mirror + Boussinesq).
+// R-family, 2 image Q-family, 3 folded image (mirror + Boussinesq); with
+// H, 4 and 5 the fold's surface load at (x, y, 0) (K x 3 values), from the
+// sigma_zz row and from the full H.
 // out per observer: K x C tensor values, then K blob weights (direct only).
 template <int P, int WANT>
 __global__ void k_terms(int term, int n, const double* __restrict__ obs,
@@ -1015,6 +1027,16 @@ __global__ void k_terms(int term, int n, const double* __restrict__ obs,
     const int nq = q_gauss_order(x, ti, eps, f.L, P);
     QRuleFly<P> r{&f, nq};
     image_q_rule<P, WANT>(r, f.n, x, eps, m, ic, A, A);
+  } else if (term >= 4) {
+    if (!(WANT & W_U)) {
+      if (term == 4) {
+        SurfaceLoadConsts c;
+        surface_load_consts(f, eps, m, c);
+        fold_surface_load_fast<P>(f, rd.r12(), rd.r8(), c, x[0], x[1], eps, A);
+      } else {
+        fold_surface_load<P>(f, rd.r12(), rd.r8(), x[0], x[1], eps, m, A);
+      }
+    }
   } else {
     double Mv[K * C] = {}, Bq[K * C] = {};
     if (WANT & W_U) direct_eval<P, W_U>(fi, ri.r12(), ri.r8(), x, eps, m, Mv, nullptr, nullptr);
@@ -1149,7 +1171,8 @@ int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, c
                     void* stream) {
   int rc = ensure_device_tables();
   if (rc) return rc;
-  if (n <= 0 || term < 0 || term > 3 || !obs || !tri || !coef_scratch || !out)
+  if (n <= 0 || term < 0 || term > 5 || (term >= 4 && want_u) || !obs || !tri || !coef_scratch ||
+      !out)
     return fail(MHS_ERR_ARG, "debug_terms args");
   cudaStream_t st = (cudaStream_t)stream;
   switch (order) {

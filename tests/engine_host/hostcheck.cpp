@@ -135,6 +135,27 @@ void fold_all(const double* obs, int nobs, const double* tri, double mu, double 
   }
 }
 
+// Surface load sigma_zz at surface points (x, y, 0) for every node and slip
+// component: fast = 1 reads the contracted sigma_zz row, 0 the full H.
+template <int P, int FAST>
+void surface_load_all(const double* pts, int npts, const double* tri, double mu, double lam,
+                      double eps, double* s) {
+  ensure_gl();
+  constexpr int K = n_nodes(P);
+  Frame f;
+  make_frame(tri, f);
+  Rule<P> r12, r8;
+  r12.build(f, cst::FAR_GAUSS_N);
+  r8.build(f, cst::FAR_GAUSS_N_DISTANT);
+  const Material m = make_material(mu, lam);
+  SurfaceLoadConsts c;
+  surface_load_consts(f, eps, m, c);
+  for (int i = 0; i < npts; ++i) {
+    if (FAST) fold_surface_load_fast<P>(f, r12.q, r8.q, c, pts[2 * i], pts[2 * i + 1], eps, s + 3 * K * i);
+    else fold_surface_load<P>(f, r12.q, r8.q, pts[2 * i], pts[2 * i + 1], eps, m, s + 3 * K * i);
+  }
+}
+
 }  // namespace
 
 #define DISPATCH_P(FN, WANT, ...)                 \
@@ -182,6 +203,12 @@ int hc_fold_image(int P, int want, const double* obs, int nobs, const double* tr
   if (want == W_U) { DISPATCH_P(fold_all, W_U, obs, nobs, tri, mu, lam, eps, U, H) }
   if (want == W_H) { DISPATCH_P(fold_all, W_H, obs, nobs, tri, mu, lam, eps, U, H) }
   return -2;
+}
+
+int hc_surface_load(int P, int fast, const double* pts, int npts, const double* tri, double mu,
+                    double lam, double eps, double* s) {
+  if (fast) { DISPATCH_P(surface_load_all, 1, pts, npts, tri, mu, lam, eps, s) }
+  DISPATCH_P(surface_load_all, 0, pts, npts, tri, mu, lam, eps, s)
 }
 
 }  // extern "C"

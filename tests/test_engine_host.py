@@ -113,3 +113,24 @@ def test_fold_image(hc, P, key):
     hc.hc_fold_image(P, 1 if key == "U" else 2, _p(obs), N, _p(tri.copy()), c(MU), c(LAM), c(0.12),
                      _p(A), _p(A))
     assert relmax(A, O.fold_image(obs, tri, P, MU, LAM, 0.12, (key,))[key]) < TOL
+
+
+@pytest.mark.parametrize("P", [0, 1, 2])
+def test_surface_load_fast_matches_full_stress(hc, P):
+    """The fold's surface load contracts the lifted moments with a per-source
+    sigma_zz row instead of assembling and rotating all of H; both forms
+    agree at surface points in the closed-form and both quadrature zones."""
+    tri = np.array([[0.0, 0.0, 0.0], [1.5, 0.2, -0.05], [0.3, 0.9, -1.1]])
+    rng = np.random.default_rng(3)
+    pts = np.ascontiguousarray(np.concatenate([rng.uniform(-2, 3, (40, 2)), rng.uniform(-30, 30, (10, 2)),
+                                               rng.uniform(-300, 300, (6, 2))]))
+    K = (P + 1) * (P + 2) // 2
+    c = ctypes.c_double
+    out = {}
+    for fast in (0, 1):
+        s = np.zeros((pts.shape[0], K, 3))
+        assert hc.hc_surface_load(P, fast, _p(pts), pts.shape[0], _p(tri.copy()), c(MU), c(LAM),
+                                  c(0.12), _p(s)) == 0
+        out[fast] = s
+    assert np.abs(out[1]).max() > 0
+    assert relmax(out[1], out[0]) < 1e-13
