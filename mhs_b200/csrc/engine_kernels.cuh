@@ -8,6 +8,7 @@
 #pragma once
 
 #include "engine_moments.cuh"
+#include "tables_q.inc"
 
 namespace mhs {
 
@@ -479,12 +480,21 @@ MHS_HD int q_gauss_order(const double* x, const double* tri_img, double eps, dou
   return (int)nq;
 }
 
-// A Q-family rule on the REAL element: Cartesian nodes y, weights wN[k] =
-// area weight x N_k (image.py:325-339).
+// A Q-family rule on the REAL element held in arrays: Cartesian nodes y,
+// weights wN[k] = area weight x N_k (image.py:325-339).
+template <int P>
 struct QRule {
+  static constexpr int K = n_nodes(P);
   int nq;
   const double* y;    // nq x 3
   const double* wN;   // nq x K
+  MHS_HD int count() const { return nq; }
+  MHS_HD void node(int t, double* yy, double* w) const {
+    yy[0] = y[3 * t];
+    yy[1] = y[3 * t + 1];
+    yy[2] = y[3 * t + 2];
+    for (int k = 0; k < K; ++k) w[k] = wN[t * K + k];
+  }
 };
 
 template <int P>
@@ -513,59 +523,68 @@ MHS_HD void build_qrule(const Frame& f, const double* glx, const double* glw, in
 }
 
 // Q-family moments by quadrature, contracted (image.py:315-432).
-template <int P, int WANT>
-MHS_HD void image_q_eval(const QRule& q, const double* nrm, const double* x, double eps,
+//
+// One pass per node k.  The basis sums B_m = sum_t wN_t[k] D1^a D2^b D3^c /
+// (R2^n Q^q) of exactly the monomials the contraction reads are kept in
+// registers: the generated lists spell every monomial's exponents as
+// literals, so the products and the record-by-record contraction are
+// straight-line code.  Each monomial is formed as the ordered product
+// p1[a] p2[b] p3[c] pr[n] pq[q] with p[0] = 1 (a factor of one is exact), the
+// points are summed in rule order and the records in table order, as mhs
+// does.  Rule: count() and node(t, y, wN[K]).
+template <int P, int WANT, class Rule>
+MHS_HD void image_q_eval(const Rule& q, const double* nrm, const double* x, double eps,
                          const Material& m, const ImageCoef& ic, double* U, double* H) {
+  static_assert(WANT == W_U || WANT == W_H, "one contraction per call");
   constexpr int K = n_nodes(P);
-  double basis[MHS_Q_NMONO][K];
-  for (int i = 0; i < MHS_Q_NMONO; ++i)
-    for (int k = 0; k < K; ++k) basis[i][k] = 0.0;
   const double e2 = eps * eps;
-#pragma unroll 1
-  for (int t = 0; t < q.nq; ++t) {
-    const double d1 = x[0] - q.y[3 * t + 0];
-    const double d2 = x[1] - q.y[3 * t + 1];
-    const double d3 = x[2] + q.y[3 * t + 2];
-    const double r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
-    const double ir = 1.0 / r2, iq = 1.0 / (r2 - d3);
-    double p1[5], p2[5], p3[5], pr[8], pq[5];
-    p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
-    for (int i = 2; i < 5; ++i) {
-      p1[i] = p1[i - 1] * d1;
-      p2[i] = p2[i - 1] * d2;
-      p3[i] = p3[i - 1] * d3;
-      pq[i] = pq[i - 1] * iq;
-    }
-    for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
-    const double* wN = q.wN + t * K;
-#pragma unroll 1
-    for (int mi = 0; mi < MHS_Q_NMONO; ++mi) {
-      const int* e = MHS_TAB(mhs_q_mono)[mi];
-      double v = 1.0;
-      bool first = true;
-      if (e[0]) { v = p1[e[0]]; first = false; }
-      if (e[1]) { v = first ? p2[e[1]] : v * p2[e[1]]; first = false; }
-      if (e[2]) { v = first ? p3[e[2]] : v * p3[e[2]]; first = false; }
-      if (e[3]) { v = first ? pr[e[3]] : v * pr[e[3]]; first = false; }
-      if (e[4]) { v = first ? pq[e[4]] : v * pq[e[4]]; first = false; }
-      for (int k = 0; k < K; ++k) basis[mi][k] += v * wN[k];
-    }
-  }
-#pragma unroll 1
+  const int nq = q.count();
+#pragma unroll
   for (int k = 0; k < K; ++k) {
-    if (WANT & W_U) {
-      double DG[27];
-      for (int i = 0; i < 27; ++i) DG[i] = 0.0;
-      for (int r = 0; r < MHS_Q_NDG; ++r)
-        DG[MHS_TAB(mhs_q_dg_idx)[r][1]] += ic.q_dg[r] * basis[MHS_TAB(mhs_q_dg_idx)[r][0]][k];
+    double bs[MHS_Q_NMONO];
+#define MHS_QZ(i, a, b, c, n, qq) bs[i] = 0.0;
+    if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QZ) }
+    else { MHS_Q_MONO_DDG(MHS_QZ) }
+#undef MHS_QZ
+#pragma unroll 1
+    for (int t = 0; t < nq; ++t) {
+      double y[3], wN[K];
+      q.node(t, y, wN);
+      const double d1 = x[0] - y[0];
+      const double d2 = x[1] - y[1];
+      const double d3 = x[2] + y[2];
+      const double r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
+      const double ir = 1.0 / r2, iq = 1.0 / (r2 - d3);
+      double p1[5], p2[5], p3[5], pr[8], pq[5];
+      p1[0] = 1.0; p2[0] = 1.0; p3[0] = 1.0; pr[0] = 1.0; pq[0] = 1.0;
+      p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
+#pragma unroll
+      for (int i = 2; i < 5; ++i) {
+        p1[i] = p1[i - 1] * d1;
+        p2[i] = p2[i - 1] * d2;
+        p3[i] = p3[i - 1] * d3;
+        pq[i] = pq[i - 1] * iq;
+      }
+#pragma unroll
+      for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
+      const double w = wN[k];
+#define MHS_QA(i, a, b, c, n, qq) bs[i] += ((((p1[a] * p2[b]) * p3[c]) * pr[n]) * pq[qq]) * w;
+      if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QA) }
+      else { MHS_Q_MONO_DDG(MHS_QA) }
+#undef MHS_QA
+    }
+    if constexpr (WANT == W_U) {
+      double DG[27] = {};
+#define MHS_QT(r, mi, slot) DG[slot] += ic.q_dg[r] * bs[mi];
+      MHS_Q_TERMS_DG(MHS_QT)
+#undef MHS_QT
       for (int i = 0; i < 27; ++i) DG[i] *= m.scale_c;
       contract_dg(DG, nrm, m, U + 9 * k);
-    }
-    if (WANT & W_H) {
-      double DDG[81];
-      for (int i = 0; i < 81; ++i) DDG[i] = 0.0;
-      for (int r = 0; r < MHS_Q_NDDG; ++r)
-        DDG[MHS_TAB(mhs_q_ddg_idx)[r][1]] += ic.q_ddg[r] * basis[MHS_TAB(mhs_q_ddg_idx)[r][0]][k];
+    } else {
+      double DDG[81] = {};
+#define MHS_QT(r, mi, slot) DDG[slot] += ic.q_ddg[r] * bs[mi];
+      MHS_Q_TERMS_DDG(MHS_QT)
+#undef MHS_QT
       for (int i = 0; i < 81; ++i) DDG[i] *= m.scale_c;
       contract_ddg(DDG, nrm, m, H + 27 * k);
     }

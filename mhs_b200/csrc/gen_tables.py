@@ -124,6 +124,7 @@ def main(src: str) -> None:
     lines.append("MHS_TBL int mhs_q_mono[MHS_Q_NMONO][5] = {")
     lines += [f"  {{{a}, {b}, {c}, {n}, {q}}}," for a, b, c, n, q in qmono]
     lines.append("};")
+    qlists = {}
     for name, records, nix in (("DG", t["Q_DG_RECORDS"], 3),
                                ("DDG", t["Q_DDG_RECORDS"], 4)):
         rows = []
@@ -143,6 +144,7 @@ def main(src: str) -> None:
         lines.append(f"MHS_TBLC double mhs_q_{name.lower()}_c[MHS_Q_N{name}][3] = {{")
         lines += ["  {" + ", ".join(_num(v) for v in c) + "}," for _, _, c in rows]
         lines.append("};")
+        qlists[name] = rows
 
     # ---------------- binomial series ----------------
     lines.append("// C(-m/2, j) for m = -1, 1, 3, 5, 7, 9 (row (m+1)/2), j = 0..31")
@@ -156,6 +158,21 @@ def main(src: str) -> None:
         lines.append("  {" + ", ".join(_num(v) for v in vals) + "},")
     lines.append("};")
     (HERE / "tables.inc").write_text("\n".join(lines) + "\n")
+    # X-macro lists of the Q family for straight-line device code: the
+    # monomials each contraction reads (global index, exponents) and its
+    # records in table order (record, monomial, slot).
+    ql = ["// GENERATED by gen_tables.py -- do not edit by hand.",
+          "// Q-family lists as X-macros over the records of tables.inc.", ""]
+    for name in ("DG", "DDG"):
+        used = sorted({m for m, _, _ in qlists[name]})
+        ql.append(f"#define MHS_Q_MONO_{name}(X) \\")
+        ql += [f"  X({i}, {qmono[i][0]}, {qmono[i][1]}, {qmono[i][2]}, {qmono[i][3]}, {qmono[i][4]}) \\"
+               for i in used]
+        ql.append("")
+        ql.append(f"#define MHS_Q_TERMS_{name}(X) \\")
+        ql += [f"  X({r}, {m}, {sl}) \\" for r, (m, sl, _) in enumerate(qlists[name])]
+        ql.append("")
+    (HERE / "tables_q.inc").write_text("\n".join(ql) + "\n")
     print(f"wrote {HERE / 'tables.inc'}: R {len(rmono)} monomials, "
           f"Q {len(qmono)} monomials")
 

@@ -254,67 +254,6 @@ struct QRuleFly {
   }
 };
 
-template <int P, int WANT, class Rule>
-__device__ void image_q_rule(const Rule& q, const double* nrm, const double* x, double eps,
-                             const Material& m, const ImageCoef& ic, double* U, double* H) {
-  constexpr int K = n_nodes(P);
-  double basis[MHS_Q_NMONO][K];
-  for (int i = 0; i < MHS_Q_NMONO; ++i)
-    for (int k = 0; k < K; ++k) basis[i][k] = 0.0;
-  const double e2 = eps * eps;
-  const int nq = q.count();
-  for (int t = 0; t < nq; ++t) {
-    double y[3], wN[K];
-    q.node(t, y, wN);
-    const double d1 = x[0] - y[0];
-    const double d2 = x[1] - y[1];
-    const double d3 = x[2] + y[2];
-    const double r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
-    const double ir = 1.0 / r2, iq = 1.0 / (r2 - d3);
-    double p1[5], p2[5], p3[5], pr[8], pq[5];
-    p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
-#pragma unroll
-    for (int i = 2; i < 5; ++i) {
-      p1[i] = p1[i - 1] * d1;
-      p2[i] = p2[i - 1] * d2;
-      p3[i] = p3[i - 1] * d3;
-      pq[i] = pq[i - 1] * iq;
-    }
-#pragma unroll
-    for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
-#pragma unroll 4
-    for (int mi = 0; mi < MHS_Q_NMONO; ++mi) {
-      const int* e = tab_d::mhs_q_mono[mi];
-      double v = 1.0;
-      bool first = true;
-      if (e[0]) { v = p1[e[0]]; first = false; }
-      if (e[1]) { v = first ? p2[e[1]] : v * p2[e[1]]; first = false; }
-      if (e[2]) { v = first ? p3[e[2]] : v * p3[e[2]]; first = false; }
-      if (e[3]) { v = first ? pr[e[3]] : v * pr[e[3]]; first = false; }
-      if (e[4]) { v = first ? pq[e[4]] : v * pq[e[4]]; first = false; }
-      for (int k = 0; k < K; ++k) basis[mi][k] += v * wN[k];
-    }
-  }
-  for (int k = 0; k < K; ++k) {
-    if (WANT & W_U) {
-      double DG[27];
-      for (int i = 0; i < 27; ++i) DG[i] = 0.0;
-      for (int r = 0; r < MHS_Q_NDG; ++r)
-        DG[tab_d::mhs_q_dg_idx[r][1]] += ic.q_dg[r] * basis[tab_d::mhs_q_dg_idx[r][0]][k];
-      for (int i = 0; i < 27; ++i) DG[i] *= m.scale_c;
-      contract_dg(DG, nrm, m, U + 9 * k);
-    }
-    if (WANT & W_H) {
-      double DDG[81];
-      for (int i = 0; i < 81; ++i) DDG[i] = 0.0;
-      for (int r = 0; r < MHS_Q_NDDG; ++r)
-        DDG[tab_d::mhs_q_ddg_idx[r][1]] += ic.q_ddg[r] * basis[tab_d::mhs_q_ddg_idx[r][0]][k];
-      for (int i = 0; i < 81; ++i) DDG[i] *= m.scale_c;
-      contract_ddg(DDG, nrm, m, H + 27 * k);
-    }
-  }
-}
-
 template <int P, int KC>
 __global__ void __launch_bounds__(TB)
 k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
@@ -350,10 +289,10 @@ k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ 
   constexpr int WANT = KC == KD_DISP ? W_U : W_H;
   if (n == QFLOOR) {
     QRuleSmem<P> r{qy, qw, QFLOOR * QFLOOR};
-    image_q_rule<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
+    image_q_eval<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
   } else {
     QRuleFly<P> r{&sp.f, n};
-    image_q_rule<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
+    image_q_eval<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
   }
   double* row = T + ((oc * n_src + s) * K) * NR;
   for (int k = 0; k < K; ++k)
@@ -1026,7 +965,7 @@ __global__ void k_terms(int term, int n, const double* __restrict__ obs,
       for (int j = 0; j < 3; ++j) ti[3 * i + j] = fi.v[i][j];
     const int nq = q_gauss_order(x, ti, eps, f.L, P);
     QRuleFly<P> r{&f, nq};
-    image_q_rule<P, WANT>(r, f.n, x, eps, m, ic, A, A);
+    image_q_eval<P, WANT>(r, f.n, x, eps, m, ic, A, A);
   } else if (term >= 4) {
     if (!(WANT & W_U)) {
       if (term == 4) {

@@ -95,7 +95,7 @@ void image_q_all(const double* obs, int nobs, const double* tri, double mu, doub
     y.resize(3 * n * n);
     wN.resize(K * n * n);
     build_qrule<P>(f, g_glx.data(), g_glw.data(), n, y.data(), wN.data());
-    const QRule q{n * n, y.data(), wN.data()};
+    const QRule<P> q{n * n, y.data(), wN.data()};
     image_q_eval<P, WANT>(q, f.n, obs + 3 * o, eps, m, ic, U ? U + o * K * 9 : nullptr,
                           H ? H + o * K * 27 : nullptr);
   }
