@@ -424,6 +424,53 @@ MHS_HD void surface_load_node(const SurfaceLoadConsts& c, const double* W, doubl
   s3[2] = 2.0 * (a2 - E * c.ezz[2]);
 }
 
+// Moment spec of the surface load (stress and blob weight).
+template <int P> using SurfaceSpec = DirectSpec<P, W_H | W_E>;
+
+// Surface load from the closed-form moment table at foot (X0, X1), height z.
+template <int P>
+MHS_HD void surface_load_near(const Frame& f, const MomentTable<SurfaceSpec<P>>& T,
+                              const SurfaceLoadConsts& c, double z, double X0, double X1,
+                              double* s /*K x 3*/) {
+  using S = SurfaceSpec<P>;
+  constexpr Spec sp = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = sp.w_off[NS];
+  double cc[K][ntri(P)] = {};
+  shape_coeffs<P>(f, X0, X1, cc);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double W[NW] = {};
+    weight_closed<S, P>(T, cc, k, W);
+    surface_load_node<S>(c, W, z, s + 3 * k);
+  }
+}
+
+// Surface load by the far-field product rule q.
+template <int P, class R_FAR = double>
+MHS_HD void surface_load_far(const QuadRule& q, const SurfaceLoadConsts& c, double z, double X0,
+                             double X1, double h2, double* s /*K x 3*/) {
+  using S = SurfaceSpec<P>;
+  constexpr Spec sp = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = sp.w_off[NS];
+  double W[K * NW] = {};
+  weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
+#pragma unroll
+  for (int k = 0; k < K; ++k) surface_load_node<S>(c, W + k * NW, z, s + 3 * k);
+}
+
+// Near / far class of a surface point: 0 closed form, 1 the 12 x 12 rule,
+// 2 the 8 x 8 rule (the direct term's split, mhs/fullspace/moments.py:551-601).
+enum : int { SL_NEAR = 0, SL_FAR12 = 1, SL_FAR8 = 2 };
+
+MHS_FI int surface_class(const Frame& f, double px, double py, double eps) {
+  const double d0 = px - f.c[0], d1 = py - f.c[1], d2 = 0.0 - f.c[2];
+  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
+  if (D <= cst::D_STAR * f.L) return SL_NEAR;
+  return (D > cst::D_STAR_DISTANT * f.L) ? SL_FAR8 : SL_FAR12;
+}
+
 // The same surface load as fold_surface_load, reading only sigma_zz: the
 // weighted moments of each node (as direct_eval forms them), contracted with
 // the precomputed sigma_zz row instead of the full H assembly and rotation.
@@ -431,33 +478,18 @@ template <int P, class R_FAR = double>
 MHS_HD void fold_surface_load_fast(const Frame& f, const QuadRule& r12, const QuadRule& r8,
                                    const SurfaceLoadConsts& c, double px, double py, double eps,
                                    double* s /*K x 3*/) {
-  using S = DirectSpec<P, W_H | W_E>;
-  constexpr Spec sp = S::spec;
-  constexpr int K = n_nodes(P);
-  constexpr int NW = sp.w_off[NS];
+  using S = SurfaceSpec<P>;
   const double x[3] = {px, py, 0.0};
-  const double d0 = x[0] - f.c[0], d1 = x[1] - f.c[1], d2 = x[2] - f.c[2];
-  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
   double z, X0, X1;
   to_plane(f, x, z, X0, X1);
   const double h2 = z * z + eps * eps;
-  if (D <= cst::D_STAR * f.L) {
+  const int cls = surface_class(f, px, py, eps);
+  if (cls == SL_NEAR) {
     MomentTable<S> T;
     closed_moments<S>(f, X0, X1, h2, T);
-    double cc[K][ntri(P)] = {};
-    shape_coeffs<P>(f, X0, X1, cc);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      double W[NW] = {};
-      weight_closed<S, P>(T, cc, k, W);
-      surface_load_node<S>(c, W, z, s + 3 * k);
-    }
+    surface_load_near<P>(f, T, c, z, X0, X1, s);
   } else {
-    const QuadRule& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
-    double W[K * NW] = {};
-    weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
-#pragma unroll
-    for (int k = 0; k < K; ++k) surface_load_node<S>(c, W + k * NW, z, s + 3 * k);
+    surface_load_far<P, R_FAR>(cls == SL_FAR8 ? r8 : r12, c, z, X0, X1, h2, s);
   }
 }
 

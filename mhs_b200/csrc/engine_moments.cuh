@@ -85,36 +85,54 @@ MHS_HD void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
     }
 }
 
+// Small-|u| series, P[m][k] = rho^(k+1-m) sum_t C(-m/2, t) E[k + 2t + 1] with
+// E[pw] = (yb^pw - ya^pw) / pw, y = u / rho.  E is produced in order of pw
+// and every term goes to its sum as it appears: for each (m, k) the terms
+// arrive in increasing t, the order of the plain double loop.
 template <class S>
 MHS_HD void edge_small(double ua, double ub, double rho, double P[MS][8]) {
   constexpr Spec sp = S::spec;
-  constexpr int PWMAX = sp.kmax + 2 * (cst::SERIES_TERMS - 1) + 1;
+  constexpr int T = cst::SERIES_TERMS;
+  constexpr int PWMAX = sp.kmax + 2 * (T - 1) + 1;
   const double ya = ua / rho, yb = ub / rho;
   const bool same = ua * ub > 0.0;
   // E[pw] = (yb^pw - ya^pw) / pw; the same-sign recurrence
   // D_{pw+1} = yb D_pw + ya^pw (yb - ya) has no cancellation.
-  double E[PWMAX + 1];
   const double dy = yb - ya;
   double yap = ya, ybp = yb, D = dy;
+  double acc[MS][8];
 #pragma unroll
-  for (int pw = 1; pw <= PWMAX; ++pw) {
-    E[pw] = D * inv_int(pw);
-    if (same) D = yb * D + yap * dy;
-    yap *= ya;
-    ybp *= yb;
-    if (!same) D = ybp - yap;
+  for (int j = 0; j < MS; ++j)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[j][k] = 0.0;
+#pragma unroll 1
+  for (int u = 0; 2 * u + 1 <= PWMAX; ++u) {
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int pw = 2 * u + 1 + half;   // k parity = half
+      if (pw > PWMAX) break;
+      const double E = D * MHS_TAB(mhs_inv_int)[pw];
+      if (same) D = yb * D + yap * dy;
+      yap *= ya;
+      ybp *= yb;
+      if (!same) D = ybp - yap;
+#pragma unroll
+      for (int j = 0; j < MS; ++j)
+#pragma unroll
+        for (int k = half; k < 8; k += 2) {
+          if (k > sp.edge[j]) continue;
+          const int t = u - k / 2;            // pw = k + 2t + 1
+          if (t >= 0 && t < T) acc[j][k] += MHS_TAB(mhs_binom_half)[j][t] * E;
+        }
+    }
   }
 #pragma unroll
   for (int j = 0; j < MS; ++j) {
-    if (sp.edge[j] < 0) continue;
     const int m = 2 * j - 1;
-    const double* bh = MHS_TAB(mhs_binom_half)[j];
 #pragma unroll
-    for (int k = 0; k <= sp.edge[j]; ++k) {
-      double acc = 0.0;
-#pragma unroll
-      for (int t = 0; t < cst::SERIES_TERMS; ++t) acc += bh[t] * E[k + 2 * t + 1];
-      P[j][k] = ipow(rho, k + 1 - m) * acc;
+    for (int k = 0; k < 8; ++k) {
+      if (k > sp.edge[j]) continue;
+      P[j][k] = ipow(rho, k + 1 - m) * acc[j][k];
     }
   }
 }
@@ -138,67 +156,119 @@ MHS_FI constexpr int spec_max_need0(const Spec& sp) {
   return d;
 }
 
+// Large-|u| series on one side of the foot (a = min|u|, b = max|u|):
+// P[m][k] = +-a^s sum_t C(-m/2, t) x^t dq[s - 2t], s = k - m + 1,
+// x = rho^2 / a^2, dq[q] = [t^q / q]_1^(b/a) (log at q = 0).  Near r = b/a = 1
+// the geometric sums (r - 1) sum r^i and (1 - 1/r) sum r^-i replace expm1
+// without cancellation.  The negative-q values come from one recurrence in
+// increasing -q; the sum over t keeps a window of them in registers, and each
+// (m, k) sum takes its terms in increasing t as the plain double loop does.
 template <class S>
 MHS_HD void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
   constexpr Spec sp = S::spec;
-  // exponent range q = k - m + 1 - 2 t over the spec
-  constexpr int QHI = series_qhi(sp);
-  constexpr int QLO = series_qlo(sp);
-  constexpr int NQ = QHI - QLO + 1;
+  constexpr int T = cst::SERIES_TERMS;
+  constexpr int QHI = series_qhi(sp);             // largest s
+  constexpr int SMIN = series_qlo(sp) + 2 * (T - 1);   // smallest s
+  constexpr int W = QHI - SMIN + 1;               // window width
+  static_assert(QHI <= 2, "large-u series exponent above 2");
+  static_assert(SMIN <= 0, "window shift assumes a negative exponent at t = 0");
   const bool neg = ua < 0.0;
   const double a = neg ? -ub : ua, b = neg ? -ua : ub;
   const double r = b / a;
   const double log_r = log1p((b - a) / a);
   const bool close = r < 2.0;
   const double x = rho2 / (a * a);
-  // dq[q] = [t^q / q]_1^r (log r at q = 0).  Near r = 1 the geometric sums
-  // (r - 1) sum r^i and (1 - 1/r) sum r^-i replace expm1 without cancellation.
-  double dq[NQ];
   const double rm1 = (b - a) / a;     // r - 1
   const double omt = (b - a) / b;     // 1 - 1/r
-  const double t = a / b;             // 1/r
-  if constexpr (QHI >= 0) dq[0 - QLO] = log_r;
-  if constexpr (QHI >= 1) dq[1 - QLO] = close ? rm1 : r - 1.0;
-  if constexpr (QHI >= 2) dq[2 - QLO] = (close ? rm1 * (1.0 + r) : r * r - 1.0) * 0.5;
-  static_assert(QHI <= 2, "large-u series exponent above 2");
-  {
-    double gsum = 0.0, tk = 1.0;
+  const double tt = a / b;            // 1/r
+  double dpos[3] = {0.0, 0.0, 0.0};
+  if constexpr (QHI >= 0) dpos[0] = log_r;
+  if constexpr (QHI >= 1) dpos[1] = close ? rm1 : r - 1.0;
+  if constexpr (QHI >= 2) dpos[2] = (close ? rm1 * (1.0 + r) : r * r - 1.0) * 0.5;
+  // recurrence over k = -q = 1, 2, ...: dq[-k] = (close ? omt G_k : 1 - t^k) / k
+  double gsum = 0.0, tk = 1.0;
+  int kc = 0;
+  // win[w] = dq[QHI - w - 2i] at step i
+  double win[W];
 #pragma unroll
-    for (int k = 1; k <= -QLO; ++k) {
-      gsum += tk;
-      tk *= t;
-      if (-k <= QHI) dq[-k - QLO] = (close ? omt * gsum : 1.0 - tk) * inv_int(k);
+  for (int w = 0; w < W; ++w) {
+    const int q = QHI - w;
+    if (q >= 0) {
+      win[w] = dpos[q >= 0 && q <= 2 ? q : 0];
+    } else {
+      // generate up to k = -q (k ascending as w grows)
+      while (kc < -q) {
+        ++kc;
+        gsum += tk;
+        tk *= tt;
+      }
+      win[w] = (close ? omt * gsum : 1.0 - tk) * MHS_TAB(mhs_inv_int)[kc];
     }
   }
-  double xj[cst::SERIES_TERMS];
-  xj[0] = 1.0;
+  double acc[MS][8];
 #pragma unroll
-  for (int i = 1; i < cst::SERIES_TERMS; ++i) xj[i] = xj[i - 1] * x;
+  for (int j = 0; j < MS; ++j)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[j][k] = 0.0;
+  double xj = 1.0;
+#pragma unroll 1
+  for (int i = 0; i < T; ++i) {
+    if (i > 0) {
+      xj = xj * x;
+      // shift by two and append the next two recurrence values
+      double g[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        ++kc;
+        gsum += tk;
+        tk *= tt;
+        g[h] = (close ? omt * gsum : 1.0 - tk) * MHS_TAB(mhs_inv_int)[kc];
+      }
+#pragma unroll
+      for (int w = 0; w < W; ++w) win[w] = (w + 2 < W) ? win[w + 2] : g[w - (W - 2)];
+    }
+#pragma unroll
+    for (int j = 0; j < MS; ++j) {
+      const double bx = MHS_TAB(mhs_binom_half)[j][i] * xj;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k > sp.edge[j]) continue;
+        const int s = k - (2 * j - 1) + 1;
+        acc[j][k] += bx * win[QHI - s];
+      }
+    }
+  }
 #pragma unroll
   for (int j = 0; j < MS; ++j) {
-    if (sp.edge[j] < 0) continue;
     const int m = 2 * j - 1;
-    const double* bh = MHS_TAB(mhs_binom_half)[j];
 #pragma unroll
-    for (int k = 0; k <= sp.edge[j]; ++k) {
+    for (int k = 0; k < 8; ++k) {
+      if (k > sp.edge[j]) continue;
       const int s = k - m + 1;
-      double acc = 0.0;
-#pragma unroll
-      for (int i = 0; i < cst::SERIES_TERMS; ++i) acc += (bh[i] * xj[i]) * dq[s - 2 * i - QLO];
-      const double v = ipow(a, s) * acc;
+      const double v = ipow(a, s) * acc[j][k];
       P[j][k] = (neg && (k & 1)) ? -v : v;
     }
   }
 }
 
-template <class S>
-MHS_HD void edge_table(double ua, double ub, double rho2, double P[MS][8]) {
-  const double rho = sqrt(rho2);
+enum : int { EDGE_CLOSED = 0, EDGE_SMALL = 1, EDGE_LARGE = 2 };
+
+// Which of the three forms evaluates an edge (rho = sqrt(rho2)).
+MHS_FI int edge_regime(double ua, double ub, double rho) {
   const double aua = fabs(ua), aub = fabs(ub);
   const double umax = aua > aub ? aua : aub;
   const double umin = aua < aub ? aua : aub;
-  if (umax <= cst::SMALL_U_OVER_RHO * rho) edge_small<S>(ua, ub, rho, P);
-  else if (ua * ub > 0.0 && umin >= cst::SERIES_U_OVER_RHO * rho) edge_large<S>(ua, ub, rho2, P);
+  if (umax <= cst::SMALL_U_OVER_RHO * rho) return EDGE_SMALL;
+  if (ua * ub > 0.0 && umin >= cst::SERIES_U_OVER_RHO * rho) return EDGE_LARGE;
+  return EDGE_CLOSED;
+}
+
+template <class S>
+MHS_HD void edge_table(double ua, double ub, double rho2, double P[MS][8]) {
+  const double rho = sqrt(rho2);
+  const int r = edge_regime(ua, ub, rho);
+  if (r == EDGE_SMALL) edge_small<S>(ua, ub, rho, P);
+  else if (r == EDGE_LARGE) edge_large<S>(ua, ub, rho2, P);
   else edge_closed<S>(ua, ub, rho2, P);
 }
 
@@ -238,78 +308,92 @@ MHS_HD double solid_angle_local(const double pr[3][2], double h) {
   return 2.0 * atan2(numer, denom);
 }
 
-template <class S>
-MHS_HD void closed_moments(const Frame& f, double X0, double X1, double h2, MomentTable<S>& T) {
-  constexpr Spec sp = S::spec;
-  constexpr int NB = sp.b_off[MS] > 0 ? sp.b_off[MS] : 1;
-  double BN1[NB], BN2[NB], BD[MS];
-#pragma unroll
-  for (int i = 0; i < NB; ++i) {
-    BN1[i] = 0.0;
-    BN2[i] = 0.0;
-  }
-#pragma unroll
-  for (int j = 0; j < MS; ++j) BD[j] = 0.0;
-  double pr[3][2];
+// One edge of the triangle seen from the foot: tangent (s1, s2), outward
+// normal (c1, c2) = (s2, -s1), signed normal distance dp, the foot's
+// coordinates ua, ub of the edge ends along the tangent, rho2 = dp^2 + h2.
+struct EdgeGeom {
+  double s1, s2, dp, ua, ub, rho2;
+};
+
+MHS_FI EdgeGeom edge_geom(const double pr[3][2], int e, double h2) {
+  const int e2 = e == 2 ? 0 : e + 1;
+  const double pa0 = pr[e][0], pa1 = pr[e][1], pb0 = pr[e2][0], pb1 = pr[e2][1];
+  const double ev0 = pb0 - pa0, ev1 = pb1 - pa1;
+  const double L = sqrt(ev0 * ev0 + ev1 * ev1);
+  EdgeGeom g;
+  g.s1 = ev0 / L;
+  g.s2 = ev1 / L;
+  const double c1 = g.s2, c2 = -g.s1;
+  g.dp = pa0 * c1 + pa1 * c2;
+  g.ua = pa0 * g.s1 + pa1 * g.s2;
+  g.ub = pb0 * g.s1 + pb1 * g.s2;
+  g.rho2 = g.dp * g.dp + h2;
+  return g;
+}
+
+// Vertices relative to the foot X (in-plane, centroid frame).
+MHS_FI void foot_vertices(const Frame& f, double X0, double X1, double pr[3][2]) {
   for (int k = 0; k < 3; ++k) {
     pr[k][0] = f.p[k][0] - X0;
     pr[k][1] = f.p[k][1] - X1;
   }
-#pragma unroll 1
-  for (int e = 0; e < 3; ++e) {
-    const int e2 = e == 2 ? 0 : e + 1;
-    const double pa0 = pr[e][0], pa1 = pr[e][1], pb0 = pr[e2][0], pb1 = pr[e2][1];
-    const double ev0 = pb0 - pa0, ev1 = pb1 - pa1;
-    const double L = sqrt(ev0 * ev0 + ev1 * ev1);
-    const double s1 = ev0 / L, s2 = ev1 / L;   // edge tangent t
-    const double c1 = s2, c2 = -s1;            // outward normal (t_y, -t_x)
-    const double dp = pa0 * c1 + pa1 * c2;
-    const double ua = pa0 * s1 + pa1 * s2;
-    const double ub = pb0 * s1 + pb1 * s2;
-    const double rho2 = dp * dp + h2;
-    double P[MS][8];
-    edge_table<S>(ua, ub, rho2, P);
+}
+
+// Add one edge's boundary terms: BD[j] += dp P[j][0] and the normal
+// components of xi_1^a xi_2^b / R^m along the edge, BN1/BN2, expanded as
+// polynomials in u (xi_1 = dp c1 + u s1, xi_2 = dp c2 + u s2).
+template <class S>
+MHS_HD void edge_accumulate(const EdgeGeom& g, const double P[MS][8], double* BN1, double* BN2,
+                            double* BD) {
+  constexpr Spec sp = S::spec;
+  const double s1 = g.s1, s2 = g.s2, dp = g.dp;
+  const double c1 = s2, c2 = -s1;
 #pragma unroll
-    for (int j = 0; j < MS; ++j)
-      if (sp.edge[j] >= 0) BD[j] += dp * P[j][0];
-    // xi_1^a xi_2^b along the edge as a polynomial in u:
-    // xi_1 = dp c1 + u s1, xi_2 = dp c2 + u s2.
-    constexpr int KM = sp.kmax;
-    double pa_[KM + 1];   // xi_1^a
-    pa_[0] = 1.0;
+  for (int j = 0; j < MS; ++j)
+    if (sp.edge[j] >= 0) BD[j] += dp * P[j][0];
+  constexpr int KM = sp.kmax;
+  double pa_[KM + 1];   // xi_1^a
+  pa_[0] = 1.0;
 #pragma unroll
-    for (int i = 1; i <= KM; ++i) pa_[i] = 0.0;
-    const double l0 = dp * c1, l1 = s1, m0 = dp * c2, m1 = s2;
+  for (int i = 1; i <= KM; ++i) pa_[i] = 0.0;
+  const double l0 = dp * c1, l1 = s1, m0 = dp * c2, m1 = s2;
 #pragma unroll
-    for (int a = 0; a <= KM; ++a) {
-      double pb_[KM + 1];
+  for (int a = 0; a <= KM; ++a) {
+    double pb_[KM + 1];
 #pragma unroll
-      for (int i = 0; i <= KM; ++i) pb_[i] = pa_[i];
+    for (int i = 0; i <= KM; ++i) pb_[i] = pa_[i];
 #pragma unroll
-      for (int b = 0; a + b <= KM; ++b) {
-        // pb_ holds xi_1^a xi_2^b (degree a + b)
+    for (int b = 0; a + b <= KM; ++b) {
+      // pb_ holds xi_1^a xi_2^b (degree a + b)
 #pragma unroll
-        for (int j = 0; j < MS; ++j) {
-          if (sp.edge[j] < a + b) continue;
-          double val = 0.0;
+      for (int j = 0; j < MS; ++j) {
+        if (sp.edge[j] < a + b) continue;
+        double val = 0.0;
 #pragma unroll
-          for (int i = 0; i <= a + b; ++i) val += pb_[i] * P[j][i];
-          BN1[sp.b_off[j] + tri_idx(a, b)] += c1 * val;
-          BN2[sp.b_off[j] + tri_idx(a, b)] += c2 * val;
-        }
-        if (a + b < KM) {  // multiply by xi_2
-#pragma unroll
-          for (int i = KM; i >= 1; --i) pb_[i] = pb_[i] * m0 + pb_[i - 1] * m1;
-          pb_[0] = pb_[0] * m0;
-        }
+        for (int i = 0; i <= a + b; ++i) val += pb_[i] * P[j][i];
+        BN1[sp.b_off[j] + tri_idx(a, b)] += c1 * val;
+        BN2[sp.b_off[j] + tri_idx(a, b)] += c2 * val;
       }
-      if (a < KM) {  // multiply by xi_1
+      if (a + b < KM) {  // multiply by xi_2
 #pragma unroll
-        for (int i = KM; i >= 1; --i) pa_[i] = pa_[i] * l0 + pa_[i - 1] * l1;
-        pa_[0] = pa_[0] * l0;
+        for (int i = KM; i >= 1; --i) pb_[i] = pb_[i] * m0 + pb_[i - 1] * m1;
+        pb_[0] = pb_[0] * m0;
       }
     }
+    if (a < KM) {  // multiply by xi_1
+#pragma unroll
+      for (int i = KM; i >= 1; --i) pa_[i] = pa_[i] * l0 + pa_[i - 1] * l1;
+      pa_[0] = pa_[0] * l0;
+    }
   }
+}
+
+// Seeds (solid angle, vertical identities) and the horizontal recursion
+// from the summed boundary terms.
+template <class S>
+MHS_HD void closed_finish(const double pr[3][2], double h2, const double* BN1, const double* BN2,
+                          const double* BD, MomentTable<S>& T) {
+  constexpr Spec sp = S::spec;
   const double h = sqrt(h2);
   const double I3 = -solid_angle_local(pr, h) / h;
 #pragma unroll
@@ -351,6 +435,30 @@ MHS_HD void closed_moments(const Frame& f, double X0, double X1, double h2, Mome
         T.at(s, a, b) = val * inv;
       }
   }
+}
+
+template <class S>
+MHS_HD void closed_moments(const Frame& f, double X0, double X1, double h2, MomentTable<S>& T) {
+  constexpr Spec sp = S::spec;
+  constexpr int NB = sp.b_off[MS] > 0 ? sp.b_off[MS] : 1;
+  double BN1[NB], BN2[NB], BD[MS];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    BN1[i] = 0.0;
+    BN2[i] = 0.0;
+  }
+#pragma unroll
+  for (int j = 0; j < MS; ++j) BD[j] = 0.0;
+  double pr[3][2];
+  foot_vertices(f, X0, X1, pr);
+#pragma unroll 1
+  for (int e = 0; e < 3; ++e) {
+    const EdgeGeom g = edge_geom(pr, e, h2);
+    double P[MS][8];
+    edge_table<S>(g.ua, g.ub, g.rho2, P);
+    edge_accumulate<S>(g, P, BN1, BN2, BD);
+  }
+  closed_finish<S>(pr, h2, BN1, BN2, BD, T);
 }
 
 // W_k[n](a, b) = sum_{a'+b'<=P} c_k(a', b') M_n(a + a', b + b'), at the

@@ -157,6 +157,11 @@ def main(src: str) -> None:
             cur = cur * (a - j) / (j + 1)
         lines.append("  {" + ", ".join(_num(v) for v in vals) + "},")
     lines.append("};")
+    # 1 / k as the compiler rounds 1.0 / (double)k, for loops whose k is not
+    # a compile-time constant
+    lines.append("MHS_TBL double mhs_inv_int[128] = {")
+    lines.append("  0.0, " + ", ".join(repr(1.0 / k) for k in range(1, 128)))
+    lines.append("};")
     (HERE / "tables.inc").write_text("\n".join(lines) + "\n")
     # X-macro lists of the Q family for straight-line device code: the
     # monomials each contraction reads (global index, exponents) and its

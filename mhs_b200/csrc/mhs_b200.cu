@@ -341,30 +341,149 @@ k_band(int64_t lo, int64_t n_chunk, const double* __restrict__ obs,
 }
 
 // ---------------------------------------------------------------- k_fold
+// Grid nodes are processed in pages of FOLD_PAGE.  Each page is split by
+// surface-load class (closed form, 12 x 12 rule, 8 x 8 rule) and every
+// 32-node batch of one class runs one code path; the edges of a batch of
+// near nodes are sorted again by edge form (closed, small-|u| series,
+// large-|u| series) before their integrals are taken.  The weighted
+// point-load products are then summed in grid order, 32 nodes at a time.
+constexpr int FOLD_PAGE = 128;
+
+// Packed size of one edge's integrals P[j][0..edge[j]].
+MHS_FI constexpr int edge_pack_size(const Spec& sp) {
+  int o = 0;
+  for (int j = 0; j < MS; ++j) o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
+  return o;
+}
+
 template <int P, int KC>
-struct FoldShared {
+struct FoldWarp {
   static constexpr int K = n_nodes(P);
   static constexpr int NC = KC == KD_HE ? 6 : 3;
   static constexpr int NJ = 3 * K;
-  static constexpr int NOUT = NC * NJ;
+  static constexpr int NP = edge_pack_size(SurfaceSpec<P>::spec);
+  double px[FOLD_PAGE], py[FOLD_PAGE], wt[FOLD_PAGE];
+  double sS[FOLD_PAGE][NJ + 1];      // load minus the load at the foot
+  double sB[32][NC + 1];             // weighted point-load tensor
+  EdgeGeom eg[96];                   // edges of one near batch (node * 3 + e)
+  double eP[96][NP];                 // their packed integrals
+  unsigned char list[3][FOLD_PAGE];  // page nodes per class
+  unsigned char elist[3][96];        // batch edges per form
+  double brk[FOLD_MAX_BREAKS];
+  double sh_load[NJ];
+  double outv[NC * NJ];
+  double R1;
+  int nbrk;
+};
+
+template <int P, int KC>
+struct FoldShared {
   SrcPrep sp;
   SmemRules<P> rd;       // element (surface load)
   SmemRules<P> rm;       // mirror element (its full-space field)
   SurfaceLoadConsts slc; // sigma_zz row of the element's H, per slip component
-  double brk[FOLD_WARPS][FOLD_MAX_BREAKS];
-  double sh_load[FOLD_WARPS][NJ];
-  double sB[FOLD_WARPS][32][NC];
-  double sS[FOLD_WARPS][32][NJ + 1];
-  double sR1[FOLD_WARPS];
-  double outv[FOLD_WARPS][NOUT];
-  int sbrk_n[FOLD_WARPS];
+  FoldWarp<P, KC> w[FOLD_WARPS];
 };
 
-// One warp per band pair.  Lanes evaluate 32 grid nodes at a time (each a
-// full-space H + E of the source at a surface point); the weighted
-// point-load tensor and the load difference go through shared memory and
-// each lane accumulates a fixed subset of the (component x node x slip)
-// products, so the sum has a fixed order.
+// Append `val` to `list` for every lane where pred holds, in lane order.
+__device__ __forceinline__ void warp_append(bool pred, int val, unsigned char* list, int& count,
+                                            int lane) {
+  const unsigned mask = __ballot_sync(0xffffffffu, pred);
+  if (pred) list[count + __popc(mask & ((1u << lane) - 1u))] = (unsigned char)val;
+  count += __popc(mask);
+}
+
+// Surface loads of the near nodes list[0..n) of a page into W.sS.
+template <int P, int KC>
+__device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const SurfaceLoadConsts& c,
+                                double eps, int n, int lane) {
+  using S = SurfaceSpec<P>;
+  constexpr Spec sp = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NJ = 3 * K;
+  constexpr int NB = sp.b_off[MS] > 0 ? sp.b_off[MS] : 1;
+  for (int b = 0; b < n; b += 32) {
+    const int i = b + lane;
+    const bool active = i < n;
+    const int u = active ? W.list[SL_NEAR][i] : 0;
+    double z = 0.0, X0 = 0.0, X1 = 0.0, h2 = 1.0;
+    double pr[3][2] = {};
+    int cnt[3] = {0, 0, 0};
+    if (active) {
+      const double x[3] = {W.px[u], W.py[u], 0.0};
+      to_plane(f, x, z, X0, X1);
+      h2 = z * z + eps * eps;
+      foot_vertices(f, X0, X1, pr);
+    }
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      int form = -1;
+      if (active) {
+        const EdgeGeom g = edge_geom(pr, e, h2);
+        W.eg[3 * lane + e] = g;
+        form = edge_regime(g.ua, g.ub, sqrt(g.rho2));
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r) warp_append(form == r, 3 * lane + e, W.elist[r], cnt[r], lane);
+    }
+    __syncwarp();
+    // edge integrals, one form per pass
+#pragma unroll 1
+    for (int r = 0; r < 3; ++r) {
+      for (int q = 0; q < cnt[r]; q += 32) {
+        if (q + lane < cnt[r]) {
+          const int slot = W.elist[r][q + lane];
+          const EdgeGeom g = W.eg[slot];
+          double Pt[MS][8];
+          if (r == EDGE_CLOSED) edge_closed<S>(g.ua, g.ub, g.rho2, Pt);
+          else if (r == EDGE_SMALL) edge_small<S>(g.ua, g.ub, sqrt(g.rho2), Pt);
+          else edge_large<S>(g.ua, g.ub, g.rho2, Pt);
+          int o = 0;
+#pragma unroll
+          for (int j = 0; j < MS; ++j) {
+#pragma unroll
+            for (int k = 0; k <= sp.edge[j]; ++k) W.eP[slot][o + k] = Pt[j][k];
+            o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (active) {
+      double BN1[NB], BN2[NB], BD[MS];
+#pragma unroll
+      for (int t = 0; t < NB; ++t) {
+        BN1[t] = 0.0;
+        BN2[t] = 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < MS; ++j) BD[j] = 0.0;
+#pragma unroll 1
+      for (int e = 0; e < 3; ++e) {
+        const int slot = 3 * lane + e;
+        const EdgeGeom g = W.eg[slot];
+        double Pt[MS][8] = {};
+        int o = 0;
+#pragma unroll
+        for (int j = 0; j < MS; ++j) {
+#pragma unroll
+          for (int k = 0; k <= sp.edge[j]; ++k) Pt[j][k] = W.eP[slot][o + k];
+          o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
+        }
+        edge_accumulate<S>(g, Pt, BN1, BN2, BD);
+      }
+      MomentTable<S> T;
+      closed_finish<S>(pr, h2, BN1, BN2, BD, T);
+      double sl[NJ] = {};
+      surface_load_near<P>(f, T, c, z, X0, X1, sl);
+#pragma unroll
+      for (int jj = 0; jj < NJ; ++jj) W.sS[u][jj] = sl[jj] - W.sh_load[jj];
+    }
+    __syncwarp();
+  }
+}
+
+// One warp per band pair.
 template <int P, int KC>
 __global__ void __launch_bounds__(32 * FOLD_WARPS)
 k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
@@ -388,13 +507,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   SrcPrep& sp = sh.sp;
   SmemRules<P>& rd = sh.rd;
   SmemRules<P>& rm = sh.rm;
-  auto& brk = sh.brk;
-  auto& sh_load = sh.sh_load;
-  auto& sB = sh.sB;
-  auto& sS = sh.sS;
-  auto& sbrk_n = sh.sbrk_n;
-  auto& sR1 = sh.sR1;
-  auto& outv = sh.outv;
+  FoldWarp<P, KC>& W = sh.w[wid];
   const Material m = make_material(mu, lam);
   if (threadIdx.x == 0) sp = prep[s];
   __syncthreads();
@@ -426,23 +539,24 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     }
     return;
   } else {
+    const SurfaceLoadConsts& slc = sh.slc;
     FoldPair fp;
     fold_pair_setup(x, sp.centre, sp.r_f, eps, fp);
     if (lane == 0) {
       double R1;
-      sbrk_n[wid] = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, brk[wid], &R1);
-      sR1[wid] = R1;
+      W.nbrk = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, W.brk, &R1);
+      W.R1 = R1;
       double sl[NJ] = {};
-      fold_surface_load_fast<P>(sp.f, r12, r8, sh.slc, x[0], x[1], eps, sl);
-      for (int j = 0; j < NJ; ++j) sh_load[wid][j] = sl[j];
+      fold_surface_load_fast<P>(sp.f, r12, r8, slc, x[0], x[1], eps, sl);
+      for (int j = 0; j < NJ; ++j) W.sh_load[j] = sl[j];
     }
     __syncwarp();
-    const int nb = sbrk_n[wid];
+    const int nb = W.nbrk;
     if (nb < 0) {
       if (lane == 0) atomic_status(status, MHS_DEV_FOLD_GRID_OVERFLOW);
       return;
     }
-    fp.R1 = sR1[wid];
+    fp.R1 = W.R1;
     const double* gx6 = d_glx + gl_offset(cst::FOLD_N_RADIAL);
     const double* gw6 = d_glw + gl_offset(cst::FOLD_N_RADIAL);
     const double* gx4 = d_glx + gl_offset(cst::FOLD_N_ANGULAR);
@@ -451,7 +565,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
 #pragma unroll
     for (int i = 0; i < PER_LANE; ++i) acc[i] = 0.0;
     for (int pi = 0; pi + 1 < nb; ++pi) {
-      const double ra = brk[wid][pi], rb = brk[wid][pi + 1];
+      const double ra = W.brk[pi], rb = W.brk[pi + 1];
       if (rb - ra < 1e-9 * eps) continue;
       AngRule A;
       fold_panel_rule(fp, ra, rb, A);
@@ -460,46 +574,82 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
         return;
       }
       const int npts = cst::FOLD_N_RADIAL * A.n;
-      for (int b0 = 0; b0 < npts; b0 += 32) {
-        const int t = b0 + lane;
-        double Bv[NC] = {}, sv[NJ] = {};
-        if (t < npts) {
-          const int ir = t / A.n, j = t % A.n;
-          const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
-          const double wr = (rb - ra) * (0.5 * gw6[ir]);
-          double th, wt;
-          fold_ang_node(A, gx4, gw4, j, &th, &wt);
-          const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
-          const double w = wr * wt * R;
-          fold_surface_load_fast<P>(sp.f, r12, r8, sh.slc, px, py, eps, sv);
-          if (WH) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, Bv);
-          else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, Bv);
-          for (int c = 0; c < NC; ++c) sB[wid][lane][c] = w * Bv[c];
-          for (int jj = 0; jj < NJ; ++jj) sS[wid][lane][jj] = sv[jj] - sh_load[wid][jj];
-        } else {
-          for (int c = 0; c < NC; ++c) sB[wid][lane][c] = 0.0;
-          for (int jj = 0; jj < NJ; ++jj) sS[wid][lane][jj] = 0.0;
+      for (int p0 = 0; p0 < npts; p0 += FOLD_PAGE) {
+        const int np = min(FOLD_PAGE, npts - p0);
+        // nodes of the page and their classes
+        int ncls[3] = {0, 0, 0};
+#pragma unroll
+        for (int r = 0; r < FOLD_PAGE / 32; ++r) {
+          const int u = 32 * r + lane;
+          int cls = -1;
+          if (u < np) {
+            const int t = p0 + u;
+            const int ir = t / A.n, j = t % A.n;
+            const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
+            const double wr = (rb - ra) * (0.5 * gw6[ir]);
+            double th, wt;
+            fold_ang_node(A, gx4, gw4, j, &th, &wt);
+            const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
+            W.px[u] = px;
+            W.py[u] = py;
+            W.wt[u] = wr * wt * R;
+            cls = surface_class(sp.f, px, py, eps);
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) warp_append(cls == c, u, W.list[c], ncls[c], lane);
         }
         __syncwarp();
-        const int nvalid = min(32, npts - b0);
+        // far loads
+#pragma unroll 1
+        for (int c = SL_FAR12; c <= SL_FAR8; ++c) {
+          const QuadRule& q = c == SL_FAR8 ? r8 : r12;
+          for (int b = 0; b < ncls[c]; b += 32) {
+            if (b + lane < ncls[c]) {
+              const int u = W.list[c][b + lane];
+              const double xx[3] = {W.px[u], W.py[u], 0.0};
+              double z, X0, X1;
+              to_plane(sp.f, xx, z, X0, X1);
+              double sl[NJ] = {};
+              surface_load_far<P>(q, slc, z, X0, X1, z * z + eps * eps, sl);
 #pragma unroll
-        for (int i = 0; i < PER_LANE; ++i) {
-          const int oi = lane + 32 * i;
-          if (oi < NOUT) {
-            const int c = oi / NJ, jj = oi % NJ;
-            double a = acc[i];
-            for (int u = 0; u < nvalid; ++u) a += sB[wid][u][c] * sS[wid][u][jj];
-            acc[i] = a;
+              for (int jj = 0; jj < NJ; ++jj) W.sS[u][jj] = sl[jj] - W.sh_load[jj];
+            }
           }
         }
+        // near loads
+        fold_near_batch<P, KC>(W, sp.f, slc, eps, ncls[SL_NEAR], lane);
         __syncwarp();
+        // weighted point loads and the ordered sum, 32 nodes at a time
+        for (int c0 = 0; c0 < np; c0 += 32) {
+          const int u = c0 + lane;
+          if (u < np) {
+            const double px = W.px[u], py = W.py[u], w = W.wt[u];
+            double Bv[NC] = {};
+            if (WH) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, Bv);
+            else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, Bv);
+            for (int c = 0; c < NC; ++c) W.sB[lane][c] = w * Bv[c];
+          }
+          __syncwarp();
+          const int nvalid = min(32, np - c0);
+#pragma unroll
+          for (int i = 0; i < PER_LANE; ++i) {
+            const int oi = lane + 32 * i;
+            if (oi < NOUT) {
+              const int c = oi / NJ, jj = oi % NJ;
+              double a = acc[i];
+              for (int v = 0; v < nvalid; ++v) a += W.sB[v][c] * W.sS[c0 + v][jj];
+              acc[i] = a;
+            }
+          }
+          __syncwarp();
+        }
       }
     }
     // gather the lane partials into the scratch row
 #pragma unroll
     for (int i = 0; i < PER_LANE; ++i) {
       const int oi = lane + 32 * i;
-      if (oi < NOUT) outv[wid][oi] = acc[i];
+      if (oi < NOUT) W.outv[oi] = acc[i];
     }
     __syncwarp();
     if (lane == 0) {
@@ -513,11 +663,11 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
           for (int mm = 0; mm < 3; ++mm) {
             double Hb[3][3];
             for (int c = 0; c < 6; ++c) {
-              const double v = outv[wid][c * NJ + 3 * k + mm];
+              const double v = W.outv[c * NJ + 3 * k + mm];
               Hb[ia[c]][ib[c]] = v;
               Hb[ib[c]][ia[c]] = v;
             }
-            const double shv = sh_load[wid][3 * k + mm];
+            const double shv = W.sh_load[3 * k + mm];
             Hb[0][0] += shv * srr;
             Hb[1][1] += shv * srr;
             Hb[2][2] += shv * szz;
@@ -533,8 +683,8 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
         for (int k = 0; k < K; ++k)
           for (int mm = 0; mm < 3; ++mm)
             for (int i = 0; i < 3; ++i) {
-              const double v = outv[wid][i * NJ + 3 * k + mm] +
-                               (i == 2 ? sh_load[wid][3 * k + mm] * uz : 0.0);
+              const double v = W.outv[i * NJ + 3 * k + mm] +
+                               (i == 2 ? W.sh_load[3 * k + mm] * uz : 0.0);
               row[k * NR + 3 * i + mm] += Mv[9 * k + 3 * i + mm] * mirror_slip_sign(mm) + v;
             }
       }
