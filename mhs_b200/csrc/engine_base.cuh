@@ -82,6 +82,23 @@ constexpr int GL_TABLE = gl_offset(GL_MAX + 1);
 // ------------------------------------------------------ triangular packing
 // Index of (a, b), a + b <= D, independent of D: ordered by total degree,
 // then by b.  ntri(D) entries cover every degree <= D.
+// 1 / sqrt(x): the device's reciprocal square root (within an ulp), one
+// division and square root on the host.
+MHS_FI double rsqrt_r(double x) {
+#if defined(__CUDA_ARCH__)
+  return ::rsqrt(x);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
+MHS_FI float rsqrt_r(float x) {
+#if defined(__CUDA_ARCH__)
+  return ::rsqrtf(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+
 MHS_FI constexpr int tri_idx(int a, int b) { return (a + b) * (a + b + 1) / 2 + b; }
 MHS_FI constexpr int ntri(int d) { return d < 0 ? 0 : (d + 1) * (d + 2) / 2; }
 MHS_FI constexpr int imax(int a, int b) { return a > b ? a : b; }

@@ -92,20 +92,23 @@ MHS_HD double tri_diameter(const double* tri) {
 MHS_HD void point_stress6(double dx, double dy, double zeta, double nu, double* S) {
   const double r2 = dx * dx + dy * dy;
   const double rho = sqrt(r2 + zeta * zeta);
-  const double rho3 = rho * rho * rho;
-  const double rho5 = rho3 * rho * rho;
+  const double irho = 1.0 / rho;
+  const double irho3 = irho * irho * irho;
+  const double irho5 = irho3 * irho * irho;
   const double a = 1.0 / (rho * (rho + zeta));
   const double c = 1.0 - 2.0 * nu;
-  const double s_th = c * (-a + zeta / rho3);
-  const double s_r_th = 2.0 * c * a - 3.0 * zeta * r2 / rho5 - c * zeta / rho3;
+  const double zr3 = zeta * irho3;
+  const double s_th = c * (-a + zr3);
+  const double s_r_th = 2.0 * c * a - 3.0 * zeta * r2 * irho5 - c * zr3;
   const double r = sqrt(r2);
-  const double ex = r > 0.0 ? dx / r : 0.0, ey = r > 0.0 ? dy / r : 0.0;
+  const double ir = r > 0.0 ? 1.0 / r : 0.0;
+  const double ex = dx * ir, ey = dy * ir;
   const double pref = 1.0 / (2.0 * cst::PI);
   S[0] = pref * (s_th + s_r_th * ex * ex);
   S[1] = pref * (s_th + s_r_th * ey * ey);
-  S[2] = -pref * 3.0 * (zeta * zeta * zeta) / rho5;
+  S[2] = -pref * 3.0 * (zeta * zeta * zeta) * irho5;
   S[3] = pref * s_r_th * ex * ey;
-  const double t_rz = pref * 3.0 * r * zeta * zeta / rho5;
+  const double t_rz = pref * 3.0 * r * zeta * zeta * irho5;
   S[4] = t_rz * ex;
   S[5] = t_rz * ey;
 }
@@ -149,6 +152,16 @@ MHS_FI double linspace_at(double a, double b, int num, int i) {
 #endif
 }
 
+// The same point with the step (b - a) / (num - 1) already formed.
+MHS_FI double linspace_step_at(double a, double b, double step, int num, int i) {
+  if (i == num - 1) return b;
+#if defined(__CUDA_ARCH__)
+  return __dadd_rn(__dmul_rn((double)i, step), a);
+#else
+  return (double)i * step + a;
+#endif
+}
+
 // One-sided angular half-width of the circles r in [ra, rb] inside the disk
 // of `radius` about the crease centre at distance rho_s (fold.py:251-258).
 MHS_HD double fold_halfwidth(double ra, double rb, double rho_s, double radius) {
@@ -164,6 +177,7 @@ MHS_HD double fold_halfwidth(double ra, double rb, double rho_s, double radius) 
 struct AngRule {
   int npiece;
   double a[4], b[4];
+  double step[4];  // (b - a) / m, the linspace step of the piece
   int m[4];        // intervals per piece
   int n;           // total nodes = FOLD_N_ANGULAR * sum(m); -1 past the cap
 };
@@ -191,6 +205,7 @@ MHS_HD void fold_angular(double theta_c, double w_fine, double w_med, double rb,
     if (m < 8) m = 8;
     A.a[0] = 0.0;
     A.b[0] = two_pi;
+    A.step[0] = (two_pi - 0.0) / (double)m;
     A.m[0] = m;
     A.npiece = 1;
     A.n = n * m;
@@ -239,6 +254,7 @@ MHS_HD void fold_angular(double theta_c, double w_fine, double w_med, double rb,
     if (!(pb[i] > pa[i])) continue;
     A.a[A.npiece] = pa[i];
     A.b[A.npiece] = pb[i];
+    A.step[A.npiece] = (pb[i] - pa[i]) / (double)pm[i];
     A.m[A.npiece] = pm[i];
     A.n += n * pm[i];
     ++A.npiece;
@@ -341,8 +357,8 @@ MHS_HD void fold_ang_node(const AngRule& A, const double* glx4, const double* gl
     ++p;
   }
   const int iv = j / cst::FOLD_N_ANGULAR, nd = j % cst::FOLD_N_ANGULAR;
-  const double a = linspace_at(A.a[p], A.b[p], A.m[p] + 1, iv);
-  const double b = linspace_at(A.a[p], A.b[p], A.m[p] + 1, iv + 1);
+  const double a = linspace_step_at(A.a[p], A.b[p], A.step[p], A.m[p] + 1, iv);
+  const double b = linspace_step_at(A.a[p], A.b[p], A.step[p], A.m[p] + 1, iv + 1);
   const double u = 0.5 * (glx4[nd] + 1.0), wu = 0.5 * glw4[nd];
   *theta = a + (b - a) * u;
   *wt = (b - a) * wu;
@@ -534,7 +550,9 @@ MHS_HD int fold_boussinesq_scalar(const Frame& f, const QuadRule& r12, const Qua
       for (int j = 0; j < A.n; ++j) {
         double th, wt;
         fold_ang_node(A, gx4, gw4, j, &th, &wt);
-        const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        const double px = fp.xh0 + R * cs, py = fp.xh1 + R * sn;
         const double w = wr * wt * R;
         double s[3 * K] = {};
         fold_surface_load_fast<P>(f, r12, r8, slc, px, py, eps, s);

@@ -541,14 +541,16 @@ MHS_HD void weight_far(const QuadRule& q, double X0, double X1, double h2, doubl
   for (int t = 0; t < q.nq; ++t) {
     const R xi0 = R(q.eta0[t]) - x0, xi1 = R(q.eta1[t]) - x1;
     const R R2 = xi0 * xi0 + xi1 * xi1 + hh;
-    const R inv = R(1) / sqrt(R2);
+    const R inv = rsqrt_r(R2);
     const R inv2 = inv * inv;
-    R rp[NS];   // R^-n for odd n
+    // w_s = wq R^-n for the odd n of the spec, then times each monomial
+    const R wq = R(q.wq[t]);
+    R ws[NS];
     {
-      R cur = inv;
+      R cur = wq * inv;
 #pragma unroll
       for (int s = 1; s < NS; ++s) {
-        rp[s] = cur;
+        ws[s] = cur;
         cur = cur * inv2;
       }
     }
@@ -560,7 +562,6 @@ MHS_HD void weight_far(const QuadRule& q, double X0, double X1, double h2, doubl
       p0[i] = p0[i - 1] * xi0;
       p1[i] = p1[i - 1] * xi1;
     }
-    const R wq = R(q.wq[t]);
     R Nk[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) Nk[k] = R(q.Nq[t * K + k]);
@@ -568,13 +569,17 @@ MHS_HD void weight_far(const QuadRule& q, double X0, double X1, double h2, doubl
     for (int a = 0; a <= DM; ++a)
 #pragma unroll
       for (int b = 0; a + b <= DM; ++b) {
-        const R mono = (a && b) ? wq * p0[a] * p1[b] : a ? wq * p0[a] : b ? wq * p1[b] : wq;
+        const R mono = (a && b) ? p0[a] * p1[b] : a ? p0[a] : b ? p1[b] : R(1);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
           if (sp.need0[s] < a + b) continue;
-          const R v = mono * rp[s];
+          const R v = (a || b) ? ws[s] * mono : ws[s];
+          if constexpr (P == 0) {
+            acc[0][sp.w_off[s] + tri_idx(a, b)] += v;   // N = 1
+          } else {
 #pragma unroll
-          for (int k = 0; k < K; ++k) acc[k][sp.w_off[s] + tri_idx(a, b)] += v * Nk[k];
+            for (int k = 0; k < K; ++k) acc[k][sp.w_off[s] + tri_idx(a, b)] += v * Nk[k];
+          }
         }
       }
   }

@@ -589,7 +589,9 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
             const double wr = (rb - ra) * (0.5 * gw6[ir]);
             double th, wt;
             fold_ang_node(A, gx4, gw4, j, &th, &wt);
-            const double px = fp.xh0 + R * cos(th), py = fp.xh1 + R * sin(th);
+            double sn, cs;
+            sincos(th, &sn, &cs);
+            const double px = fp.xh0 + R * cs, py = fp.xh1 + R * sn;
             W.px[u] = px;
             W.py[u] = py;
             W.wt[u] = wr * wt * R;
