@@ -12,7 +12,10 @@ edge, receivers at the centroids with cutde frames, mu = lam = 30: output
   e2e    entries/s through the public API from pinned host inputs, with the
          host->device copies and the full device->host read of the matrix
          inside the timed region
-  roofline   the dominant kernel against the measured FP64 FMA ceiling
+  roofline   the dominant stage (the fold): its algorithmic flops -- per-unit
+         operation counts of the op-counting host build times the device
+         census of its work units in an untimed step -- over its time per
+         launch, against the measured FP64 FMA ceiling
   cpu_baseline   the numpy oracle (a restatement of mhs's CPU path) on a
          stratified sample of the same workload, extrapolated
 
@@ -40,10 +43,9 @@ METRIC = "Green's-fn entries/s"
 UNIT = "entries/s"
 WORKLOAD = "interaction_matrix (3,3), rough surface-reaching fault, 2400 tris, per-tri eps, fold on"
 
-# Executed FP64 operations per launch of the dominant kernels on this
-# workload (seed 0), from an ncu census of the same command
-# (profiles/fold_c2_fp64_census.md): dadd + dmul + 2 dfma.
-FP64_FLOPS_PER_LAUNCH = {}
+# DRAM bytes (read + write) of one k_fold launch on this workload, from
+# profiles/fold_c2_traffic.md; keyed by (nu, nv, precision).
+FOLD_TRAFFIC_PER_LAUNCH = {(60, 20, "fp64"): 120.4e6 + 1.78e9}
 # Kernels each profiled stage launches (csrc/mhs_b200.cu: run()).
 KERNELS_PER_STAGE = {"prep": 2, "pair": 1, "imageq": 1, "fold": 2, "final": 1}
 
@@ -203,6 +205,11 @@ def run_ours(a, rank, world):
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
+    # untimed census of the fold's work units (algorithmic flops, below)
+    _native.census(True)
+    step()
+    census = _native.census_read()
+    _native.census(False)
     if world > 1:
         torch.distributed.barrier()
     _native.profile(True)
@@ -255,15 +262,26 @@ def run_ours(a, rank, world):
     e2e_ms = float(e2e_t.item())
     e2e_val = world * entries * e2e_steps / (e2e_ms * 1e-3)
 
-    # roofline of the dominant stage
+    # roofline of the dominant stage (the fold): algorithmic flops of the
+    # census'd work units over the stage's time per launch
     top = max(stages, key=lambda s: stages[s][0])
     top_ms, top_n = stages[top]
     peak = _native.fp_peak(fp64=True)
-    flops = FP64_FLOPS_PER_LAUNCH.get((top, a.nu, a.nv, a.precision))
-    achieved = (flops / (top_ms / max(top_n, 1) * 1e-3) / 1e12) if flops else None
+    achieved, fl = None, None
+    if top == "fold":
+        from mhs_b200 import flops as _flops
+        fl = _flops.fold_flops(census, order=0, want_h=True, mu=mu, lam=lam,
+                               eps=float(np.mean(eps)))
+        achieved = fl["flop"] / (top_ms / max(top_n, 1) * 1e-3) / 1e12
     roof = {"bound": "fp64", "kernel": top, "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+            "traffic": FOLD_TRAFFIC_PER_LAUNCH.get((a.nu, a.nv, a.precision)) if top == "fold" else None,
             "peak_source": "measured FP64 FMA ceiling (mhs_fp_peak, this run)",
+            "algorithmic": None if fl is None else {
+                "flop_per_launch": fl["flop"], "div": fl["div"], "sqrt": fl["sqrt"],
+                "special": fl["special"], "census": census,
+                "counting": "op-counting host build of the engine (mhs_b200/csrc/opcount.cpp): "
+                            "add/sub/mul 1 flop, fma 2; div, sqrt, library calls apart"},
             "stage_ms_per_step": {k: v[0] / a.steps for k, v in stages.items()},
             "stage_launches_per_step": {k: v[1] / a.steps for k, v in stages.items()}}
 

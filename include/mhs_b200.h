@@ -160,6 +160,29 @@ enum mhs_stage {
 int mhs_profile_enable(int on);
 int mhs_profile_read(double* ms, int* launches);
 
+/* Fold work census (measurement).  While enabled, the fold kernel counts its
+ * work units into device counters: band pairs, radial panels, polar-grid
+ * nodes per surface-load form (closed form, 12 x 12 rule, 8 x 8 rule) and
+ * near-field edge integrals per form (closed, small-|u| series, large-|u|
+ * series).  mhs_census_read synchronises the device, returns the
+ * MHS_CENSUS_N counts accumulated since the last read or enable, and clears
+ * them.  Multiplied by the per-unit operation counts of the op-counting build
+ * (mhs_b200/csrc/opcount.cpp) they give the fold's algorithmic flops.  No
+ * counterpart in mhs. */
+enum mhs_census_item {
+  MHS_CENSUS_PAIRS = 0,
+  MHS_CENSUS_PANELS = 1,
+  MHS_CENSUS_NEAR = 2,
+  MHS_CENSUS_FAR12 = 3,
+  MHS_CENSUS_FAR8 = 4,
+  MHS_CENSUS_EDGE_CLOSED = 5,
+  MHS_CENSUS_EDGE_SMALL = 6,
+  MHS_CENSUS_EDGE_LARGE = 7,
+  MHS_CENSUS_N = 8
+};
+int mhs_census_enable(int on);
+int mhs_census_read(unsigned long long* counts);
+
 /* Issue ceiling of the device: independent FMA chains on every SM, FP64
  * (fp64 = 1) or FP32, in TFLOP/s (2 flops per FMA).  The roofline
  * denominator of the FP64 and mixed forms. */

@@ -52,7 +52,8 @@ class Request(ctypes.Structure):
 #: Symbols the header declares; a test checks the library exports each.
 EXPORTS = ("mhs_workspace_bytes", "mhs_assemble", "mhs_read_status", "mhs_column_plan",
            "mhs_last_error", "mhs_version", "mhs_profile_enable", "mhs_profile_read",
-           "mhs_fp_peak", "mhs_debug_terms")
+           "mhs_fp_peak", "mhs_debug_terms", "mhs_assemble_noalloc", "mhs_census_enable",
+           "mhs_census_read")
 
 _lib = None
 
@@ -94,6 +95,10 @@ def load() -> ctypes.CDLL:
                                     ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p]
     lib.mhs_debug_terms.restype = ctypes.c_int
+    lib.mhs_census_enable.argtypes = [ctypes.c_int]
+    lib.mhs_census_enable.restype = ctypes.c_int
+    lib.mhs_census_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.mhs_census_read.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -111,6 +116,21 @@ def profile_read() -> dict:
     n = (ctypes.c_int * len(STAGES))()
     check(load().mhs_profile_read(ms, n))
     return {s: (ms[i], n[i]) for i, s in enumerate(STAGES)}
+
+
+CENSUS = ("pairs", "panels", "near", "far12", "far8", "edge_closed", "edge_small", "edge_large")
+
+
+def census(on: bool) -> None:
+    """Start (clearing the counters) or stop the fold work census."""
+    check(load().mhs_census_enable(1 if on else 0))
+
+
+def census_read() -> dict:
+    """Fold work units counted since the last read (synchronises the device)."""
+    c = (ctypes.c_ulonglong * len(CENSUS))()
+    check(load().mhs_census_read(c))
+    return {k: int(c[i]) for i, k in enumerate(CENSUS)}
 
 
 def fp_peak(fp64: bool = True, iters: int = 1 << 16, stream=None) -> float:

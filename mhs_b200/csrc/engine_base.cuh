@@ -79,9 +79,6 @@ constexpr int GL_MAX = cst::IMAGE_Q_GAUSS_MAX;
 MHS_FI constexpr int gl_offset(int n) { return (n - 1) * n / 2; }
 constexpr int GL_TABLE = gl_offset(GL_MAX + 1);
 
-// ------------------------------------------------------ triangular packing
-// Index of (a, b), a + b <= D, independent of D: ordered by total degree,
-// then by b.  ntri(D) entries cover every degree <= D.
 // 1 / sqrt(x): the device's reciprocal square root (within an ulp), one
 // division and square root on the host.
 MHS_FI double rsqrt_r(double x) {
@@ -99,6 +96,9 @@ MHS_FI float rsqrt_r(float x) {
 #endif
 }
 
+// ------------------------------------------------------ triangular packing
+// Index of (a, b), a + b <= D, independent of D: ordered by total degree,
+// then by b.  ntri(D) entries cover every degree <= D.
 MHS_FI constexpr int tri_idx(int a, int b) { return (a + b) * (a + b + 1) / 2 + b; }
 MHS_FI constexpr int ntri(int d) { return d < 0 ? 0 : (d + 1) * (d + 2) / 2; }
 MHS_FI constexpr int imax(int a, int b) { return a > b ? a : b; }

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -341,6 +342,11 @@ k_band(int64_t lo, int64_t n_chunk, const double* __restrict__ obs,
 }
 
 // ---------------------------------------------------------------- k_fold
+// Work census (measurement only): pairs, panels, nodes per class, near
+// edges per form; counted when the kernel is given a non-null pointer.
+__device__ unsigned long long g_census[MHS_CENSUS_N];
+std::atomic<int> g_census_on{0};
+
 // Grid nodes are processed in pages of FOLD_PAGE.  Each page is split by
 // surface-load class (closed form, 12 x 12 rule, 8 x 8 rule) and every
 // 32-node batch of one class runs one code path; the edges of a batch of
@@ -396,7 +402,7 @@ __device__ __forceinline__ void warp_append(bool pred, int val, unsigned char* l
 // Surface loads of the near nodes list[0..n) of a page into W.sS.
 template <int P, int KC>
 __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const SurfaceLoadConsts& c,
-                                double eps, int n, int lane) {
+                                double eps, int n, int lane, unsigned long long* census) {
   using S = SurfaceSpec<P>;
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
@@ -426,6 +432,9 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
 #pragma unroll
       for (int r = 0; r < 3; ++r) warp_append(form == r, 3 * lane + e, W.elist[r], cnt[r], lane);
     }
+    if (census && lane == 0)
+      for (int r = 0; r < 3; ++r)
+        atomicAdd(census + MHS_CENSUS_EDGE_CLOSED + r, (unsigned long long)cnt[r]);
     __syncwarp();
     // edge integrals, one form per pass
 #pragma unroll 1
@@ -489,7 +498,7 @@ __global__ void __launch_bounds__(32 * FOLD_WARPS)
 k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
        const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
        const int* __restrict__ list, double mu, double lam, double* __restrict__ T,
-       int* __restrict__ status) {
+       int* __restrict__ status, unsigned long long* __restrict__ census) {
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);
   constexpr int C = comps_of(KC);
@@ -545,6 +554,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     if (lane == 0) {
       double R1;
       W.nbrk = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, W.brk, &R1);
+      if (census) atomicAdd(census + MHS_CENSUS_PAIRS, 1ull);
       W.R1 = R1;
       double sl[NJ] = {};
       fold_surface_load_fast<P>(sp.f, r12, r8, slc, x[0], x[1], eps, sl);
@@ -574,6 +584,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
         return;
       }
       const int npts = cst::FOLD_N_RADIAL * A.n;
+      if (census && lane == 0) atomicAdd(census + MHS_CENSUS_PANELS, 1ull);
       for (int p0 = 0; p0 < npts; p0 += FOLD_PAGE) {
         const int np = min(FOLD_PAGE, npts - p0);
         // nodes of the page and their classes
@@ -600,6 +611,9 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
 #pragma unroll
           for (int c = 0; c < 3; ++c) warp_append(cls == c, u, W.list[c], ncls[c], lane);
         }
+        if (census && lane == 0)
+          for (int c = 0; c < 3; ++c)
+            atomicAdd(census + MHS_CENSUS_NEAR + c, (unsigned long long)ncls[c]);
         __syncwarp();
         // far loads
 #pragma unroll 1
@@ -619,7 +633,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
           }
         }
         // near loads
-        fold_near_batch<P, KC>(W, sp.f, slc, eps, ncls[SL_NEAR], lane);
+        fold_near_batch<P, KC>(W, sp.f, slc, eps, ncls[SL_NEAR], lane, census);
         __syncwarp();
         // weighted point loads and the ordered sum, 32 nodes at a time
         for (int c0 = 0; c0 < np; c0 += 32) {
@@ -1000,8 +1014,11 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
       dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
       const size_t fsm = sizeof(FoldShared<P, KC>);
       CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+      unsigned long long* census = nullptr;
+      if (g_census_on.load(std::memory_order_relaxed))
+        CUDA_TRY(cudaGetSymbolAddress((void**)&census, g_census));
       k_fold<P, KC><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
-                                                      r->mu, r->lam, T, status);
+                                                      r->mu, r->lam, T, status, census);
     }
     StageTimer tfin(MHS_STAGE_FINAL, st);
     FinalArgs a;
@@ -1272,6 +1289,27 @@ int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, c
     case 2: return debug_terms<2>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
   }
   return fail(MHS_ERR_ARG, "order");
+}
+
+int mhs_census_enable(int on) {
+  if (on) {
+    const unsigned long long zero[MHS_CENSUS_N] = {};
+    if (cudaMemcpyToSymbol(g_census, zero, sizeof(zero)) != cudaSuccess)
+      return fail(MHS_ERR_CUDA, "census: clearing the counters failed");
+  }
+  g_census_on.store(on ? 1 : 0, std::memory_order_relaxed);
+  return MHS_OK;
+}
+
+int mhs_census_read(unsigned long long* counts) {
+  if (!counts) return fail(MHS_ERR_ARG, "census: null counts");
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpyFromSymbol(counts, g_census, sizeof(unsigned long long) * MHS_CENSUS_N) != cudaSuccess)
+    return fail(MHS_ERR_CUDA, "census: reading the counters failed");
+  const unsigned long long zero[MHS_CENSUS_N] = {};
+  if (cudaMemcpyToSymbol(g_census, zero, sizeof(zero)) != cudaSuccess)
+    return fail(MHS_ERR_CUDA, "census: clearing the counters failed");
+  return MHS_OK;
 }
 
 int mhs_profile_enable(int on) {
