@@ -47,7 +47,7 @@ WORKLOAD = "interaction_matrix (3,3), rough surface-reaching fault, 2400 tris, p
 # profiles/fold_c2_traffic.md; keyed by (nu, nv, precision).
 FOLD_TRAFFIC_PER_LAUNCH = {(60, 20, "fp64"): 120.4e6 + 1.78e9}
 # Kernels each profiled stage launches (csrc/mhs_b200.cu: run()).
-KERNELS_PER_STAGE = {"prep": 2, "pair": 1, "imageq": 1, "fold": 2, "final": 1}
+KERNELS_PER_STAGE = {"prep": 2, "pair": 1, "imageq": 1, "fold": 3, "final": 1}
 
 
 def parse():

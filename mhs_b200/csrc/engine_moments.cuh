@@ -537,7 +537,7 @@ MHS_HD void weight_far(const QuadRule& q, double X0, double X1, double h2, doubl
 #pragma unroll
     for (int i = 0; i < NW; ++i) acc[k][i] = R(0);
   const R x0 = R(X0), x1 = R(X1), hh = R(h2);
-#pragma unroll 1
+#pragma unroll 2
   for (int t = 0; t < q.nq; ++t) {
     const R xi0 = R(q.eta0[t]) - x0, xi1 = R(q.eta1[t]) - x1;
     const R R2 = xi0 * xi0 + xi1 * xi1 + hh;

@@ -370,9 +370,13 @@ struct FoldWarp {
   static constexpr int NP = edge_pack_size(SurfaceSpec<P>::spec);
   double px[FOLD_PAGE], py[FOLD_PAGE], wt[FOLD_PAGE];
   double sS[FOLD_PAGE][NJ + 1];      // load minus the load at the foot
-  double sB[32][NC + 1];             // weighted point-load tensor
-  EdgeGeom eg[96];                   // edges of one near batch (node * 3 + e)
-  double eP[96][NP];                 // their packed integrals
+  union {
+    struct {
+      double eu[96][3];              // (ua, ub, rho2) of one near batch's edges (node * 3 + e)
+      double eP[96][NP];             // their packed integrals
+    } edge;
+    double sB[32][NC + 1];           // weighted point-load tensor (after the loads)
+  };
   unsigned char list[3][FOLD_PAGE];  // page nodes per class
   unsigned char elist[3][96];        // batch edges per form
   double brk[FOLD_MAX_BREAKS];
@@ -386,7 +390,6 @@ template <int P, int KC>
 struct FoldShared {
   SrcPrep sp;
   SmemRules<P> rd;       // element (surface load)
-  SmemRules<P> rm;       // mirror element (its full-space field)
   SurfaceLoadConsts slc; // sigma_zz row of the element's H, per slip component
   FoldWarp<P, KC> w[FOLD_WARPS];
 };
@@ -426,7 +429,9 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
       int form = -1;
       if (active) {
         const EdgeGeom g = edge_geom(pr, e, h2);
-        W.eg[3 * lane + e] = g;
+        W.edge.eu[3 * lane + e][0] = g.ua;
+        W.edge.eu[3 * lane + e][1] = g.ub;
+        W.edge.eu[3 * lane + e][2] = g.rho2;
         form = edge_regime(g.ua, g.ub, sqrt(g.rho2));
       }
 #pragma unroll
@@ -442,16 +447,16 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
       for (int q = 0; q < cnt[r]; q += 32) {
         if (q + lane < cnt[r]) {
           const int slot = W.elist[r][q + lane];
-          const EdgeGeom g = W.eg[slot];
+          const double ua = W.edge.eu[slot][0], ub = W.edge.eu[slot][1], rho2 = W.edge.eu[slot][2];
           double Pt[MS][8];
-          if (r == EDGE_CLOSED) edge_closed<S>(g.ua, g.ub, g.rho2, Pt);
-          else if (r == EDGE_SMALL) edge_small<S>(g.ua, g.ub, sqrt(g.rho2), Pt);
-          else edge_large<S>(g.ua, g.ub, g.rho2, Pt);
+          if (r == EDGE_CLOSED) edge_closed<S>(ua, ub, rho2, Pt);
+          else if (r == EDGE_SMALL) edge_small<S>(ua, ub, sqrt(rho2), Pt);
+          else edge_large<S>(ua, ub, rho2, Pt);
           int o = 0;
 #pragma unroll
           for (int j = 0; j < MS; ++j) {
 #pragma unroll
-            for (int k = 0; k <= sp.edge[j]; ++k) W.eP[slot][o + k] = Pt[j][k];
+            for (int k = 0; k <= sp.edge[j]; ++k) W.edge.eP[slot][o + k] = Pt[j][k];
             o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
           }
         }
@@ -470,13 +475,13 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
 #pragma unroll 1
       for (int e = 0; e < 3; ++e) {
         const int slot = 3 * lane + e;
-        const EdgeGeom g = W.eg[slot];
+        const EdgeGeom g = edge_geom(pr, e, h2);   // as in the pass above
         double Pt[MS][8] = {};
         int o = 0;
 #pragma unroll
         for (int j = 0; j < MS; ++j) {
 #pragma unroll
-          for (int k = 0; k <= sp.edge[j]; ++k) Pt[j][k] = W.eP[slot][o + k];
+          for (int k = 0; k <= sp.edge[j]; ++k) Pt[j][k] = W.edge.eP[slot][o + k];
           o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
         }
         edge_accumulate<S>(g, Pt, BN1, BN2, BD);
@@ -515,14 +520,12 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   FoldShared<P, KC>& sh = *reinterpret_cast<FoldShared<P, KC>*>(fold_smem);
   SrcPrep& sp = sh.sp;
   SmemRules<P>& rd = sh.rd;
-  SmemRules<P>& rm = sh.rm;
   FoldWarp<P, KC>& W = sh.w[wid];
   const Material m = make_material(mu, lam);
   if (threadIdx.x == 0) sp = prep[s];
   __syncthreads();
   rd.build(sp.f, threadIdx.x, 32 * FOLD_WARPS);
-  rm.build(sp.fi, threadIdx.x, 32 * FOLD_WARPS);
-  if (KC != KD_E) {
+  {
     static_assert(NLIFT <= 32 * FOLD_WARPS, "one thread per lifted slot");
     if (threadIdx.x < NLIFT) {
       double col[3] = {};
@@ -540,14 +543,8 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   const double eps = sp.eps;
   double* row = T + ((oc * n_src + s) * K) * NR;
   const QuadRule r12 = rd.r12(), r8 = rd.r8();
-  if constexpr (KC == KD_E) {
-    if (lane == 0) {
-      double E[K] = {};
-      direct_eval<P, W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, nullptr, E);
-      for (int k = 0; k < K; ++k) row[k * NR + 1] = E[k];
-    }
-    return;
-  } else {
+  static_assert(KC != KD_E, "the eigen-only readout has no Boussinesq term");
+  {
     const SurfaceLoadConsts& slc = sh.slc;
     FoldPair fp;
     fold_pair_setup(x, sp.centre, sp.r_f, eps, fp);
@@ -669,9 +666,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     }
     __syncwarp();
     if (lane == 0) {
-      double Mv[K * C] = {}, E[K] = {};
       if constexpr (WH) {
-        direct_eval<P, W_H | W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, Mv, E);
         double srr, szz;
         disk_stress(fp.R1, fp.zeta, m.nu_f, &srr, &szz);
         const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
@@ -688,23 +683,65 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
             Hb[1][1] += shv * srr;
             Hb[2][2] += shv * szz;
             for (int a = 0; a < 3; ++a)
-              for (int b = 0; b < 3; ++b)
-                row[k * NR + 9 * a + 3 * b + mm] +=
-                    Mv[27 * k + 9 * a + 3 * b + mm] * mirror_slip_sign(mm) + Hb[a][b];
+              for (int b = 0; b < 3; ++b) row[k * NR + 9 * a + 3 * b + mm] += Hb[a][b];
           }
-        for (int k = 0; k < K; ++k) row[k * NR + C + 1] = E[k];
       } else {
-        direct_eval<P, W_U>(sp.fi, rm.r12(), rm.r8(), x, eps, m, Mv, nullptr, nullptr);
         const double uz = disk_disp_z(fp.R1, fp.zeta, m.mu, m.nu_f);
         for (int k = 0; k < K; ++k)
           for (int mm = 0; mm < 3; ++mm)
-            for (int i = 0; i < 3; ++i) {
-              const double v = W.outv[i * NJ + 3 * k + mm] +
-                               (i == 2 ? W.sh_load[3 * k + mm] * uz : 0.0);
-              row[k * NR + 3 * i + mm] += Mv[9 * k + 3 * i + mm] * mirror_slip_sign(mm) + v;
-            }
+            for (int i = 0; i < 3; ++i)
+              row[k * NR + 3 * i + mm] += W.outv[i * NJ + 3 * k + mm] +
+                                          (i == 2 ? W.sh_load[3 * k + mm] * uz : 0.0);
       }
     }
+  }
+}
+
+// --------------------------------------------------------- k_fold_mirror
+// The mirror element of every band pair, one thread per pair: its
+// full-space field with the slip signs of the reflection (fold.py:334-350)
+// added to the pair's row, and its blob weight (the mirror eigenstress).
+template <int P, int KC>
+__global__ void __launch_bounds__(TB)
+k_fold_mirror(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
+              const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
+              const int* __restrict__ list, double mu, double lam, double* __restrict__ T) {
+  constexpr int K = n_nodes(P);
+  constexpr int NR = row_of(KC);
+  constexpr int C = comps_of(KC);
+  const int64_t s = blockIdx.y;
+  const int n_band = cnt[s];
+  if ((int64_t)blockIdx.x * TB >= n_band) return;
+  __shared__ SrcPrep sp;
+  __shared__ SmemRules<P> rm;
+  if (threadIdx.x == 0) sp = prep[s];
+  __syncthreads();
+  rm.build(sp.fi, threadIdx.x, TB);
+  __syncthreads();
+  const int bi = blockIdx.x * TB + threadIdx.x;
+  if (bi >= n_band) return;
+  const int64_t oc = list[s * n_chunk + bi];
+  const int64_t o = lo + oc;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  const Material m = make_material(mu, lam);
+  const double eps = sp.eps;
+  double* row = T + ((oc * n_src + s) * K) * NR;
+  double E[K] = {};
+  if constexpr (KC == KD_E) {
+    direct_eval<P, W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, nullptr, E);
+    for (int k = 0; k < K; ++k) row[k * NR + 1] = E[k];
+  } else if constexpr (KC == KD_HE) {
+    double Mv[K * 27] = {};
+    direct_eval<P, W_H | W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, Mv, E);
+    for (int k = 0; k < K; ++k) {
+      for (int i = 0; i < 27; ++i) row[k * NR + i] += Mv[27 * k + i] * mirror_slip_sign(i % 3);
+      row[k * NR + C + 1] = E[k];
+    }
+  } else {
+    double Mv[K * 9] = {};
+    direct_eval<P, W_U>(sp.fi, rm.r12(), rm.r8(), x, eps, m, Mv, nullptr, nullptr);
+    for (int k = 0; k < K; ++k)
+      for (int i = 0; i < 9; ++i) row[k * NR + i] += Mv[9 * k + i] * mirror_slip_sign(i % 3);
   }
 }
 
@@ -1011,14 +1048,20 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
     if (r->fold) {
       StageTimer t(MHS_STAGE_FOLD, st);
       k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
-      dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
-      const size_t fsm = sizeof(FoldShared<P, KC>);
-      CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
-      unsigned long long* census = nullptr;
-      if (g_census_on.load(std::memory_order_relaxed))
-        CUDA_TRY(cudaGetSymbolAddress((void**)&census, g_census));
-      k_fold<P, KC><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
-                                                      r->mu, r->lam, T, status, census);
+      if constexpr (KC != KD_E) {
+        dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
+        const size_t fsm = sizeof(FoldShared<P, KC>);
+        CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fsm));
+        unsigned long long* census = nullptr;
+        if (g_census_on.load(std::memory_order_relaxed))
+          CUDA_TRY(cudaGetSymbolAddress((void**)&census, g_census));
+        k_fold<P, KC><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
+                                                        r->mu, r->lam, T, status, census);
+      }
+      dim3 gm((unsigned)((nc + TB - 1) / TB), (unsigned)r->n_src);
+      k_fold_mirror<P, KC><<<gm, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list, r->mu,
+                                              r->lam, T);
     }
     StageTimer tfin(MHS_STAGE_FINAL, st);
     FinalArgs a;
