@@ -156,7 +156,9 @@ __global__ void k_prep(int64_t n_src, const double* __restrict__ tris,
 
 // ---------------------------------------------------------------- k_pair
 // Direct term and image R-family of one (observer, source) pair.
-template <int P, int KC>
+// RF: arithmetic type of the far-field quadrature (double; float in the
+// mixed form).
+template <int P, int KC, class RF>
 __global__ void __launch_bounds__(TB)
 k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
        const SrcPrep* __restrict__ prep, const double* __restrict__ Gall,
@@ -186,7 +188,7 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   double* row = T + ((oc * n_src + s) * K) * NR;
   if constexpr (KC == KD_E) {
     double E[K] = {};
-    direct_eval<P, W_E>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
+    direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
     for (int k = 0; k < K; ++k) {
       row[k * NR + 0] = E[k];
       row[k * NR + 1] = 0.0;
@@ -196,9 +198,9 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     constexpr int C = comps_of(KC);
     double A[K * C] = {}, E[K] = {};
     if constexpr (KC == KD_DISP)
-      direct_eval<P, W_U>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
+      direct_eval<P, W_U, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
     else
-      direct_eval<P, W_H | W_E>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
+      direct_eval<P, W_H | W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
     const bool band = sp.straddle && fold_band(x, sp.centre, eps);
     if (!band) {
       double B[K * C] = {};
@@ -498,7 +500,7 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
 }
 
 // One warp per band pair.
-template <int P, int KC>
+template <int P, int KC, class RF>
 __global__ void __launch_bounds__(32 * FOLD_WARPS)
 k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
        const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
@@ -554,7 +556,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
       if (census) atomicAdd(census + MHS_CENSUS_PAIRS, 1ull);
       W.R1 = R1;
       double sl[NJ] = {};
-      fold_surface_load_fast<P>(sp.f, r12, r8, slc, x[0], x[1], eps, sl);
+      fold_surface_load_fast<P, RF>(sp.f, r12, r8, slc, x[0], x[1], eps, sl);
       for (int j = 0; j < NJ; ++j) W.sh_load[j] = sl[j];
     }
     __syncwarp();
@@ -623,7 +625,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
               double z, X0, X1;
               to_plane(sp.f, xx, z, X0, X1);
               double sl[NJ] = {};
-              surface_load_far<P>(q, slc, z, X0, X1, z * z + eps * eps, sl);
+              surface_load_far<P, RF>(q, slc, z, X0, X1, z * z + eps * eps, sl);
 #pragma unroll
               for (int jj = 0; jj < NJ; ++jj) W.sS[u][jj] = sl[jj] - W.sh_load[jj];
             }
@@ -701,7 +703,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
 // The mirror element of every band pair, one thread per pair: its
 // full-space field with the slip signs of the reflection (fold.py:334-350)
 // added to the pair's row, and its blob weight (the mirror eigenstress).
-template <int P, int KC>
+template <int P, int KC, class RF>
 __global__ void __launch_bounds__(TB)
 k_fold_mirror(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
               const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
@@ -728,18 +730,18 @@ k_fold_mirror(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restri
   double* row = T + ((oc * n_src + s) * K) * NR;
   double E[K] = {};
   if constexpr (KC == KD_E) {
-    direct_eval<P, W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, nullptr, E);
+    direct_eval<P, W_E, RF>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, nullptr, E);
     for (int k = 0; k < K; ++k) row[k * NR + 1] = E[k];
   } else if constexpr (KC == KD_HE) {
     double Mv[K * 27] = {};
-    direct_eval<P, W_H | W_E>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, Mv, E);
+    direct_eval<P, W_H | W_E, RF>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, Mv, E);
     for (int k = 0; k < K; ++k) {
       for (int i = 0; i < 27; ++i) row[k * NR + i] += Mv[27 * k + i] * mirror_slip_sign(i % 3);
       row[k * NR + C + 1] = E[k];
     }
   } else {
     double Mv[K * 9] = {};
-    direct_eval<P, W_U>(sp.fi, rm.r12(), rm.r8(), x, eps, m, Mv, nullptr, nullptr);
+    direct_eval<P, W_U, RF>(sp.fi, rm.r12(), rm.r8(), x, eps, m, Mv, nullptr, nullptr);
     for (int k = 0; k < K; ++k)
       for (int i = 0; i < 9; ++i) row[k * NR + i] += Mv[9 * k + i] * mirror_slip_sign(i % 3);
   }
@@ -1014,7 +1016,7 @@ int check_request(const mhs_request* r) {
   return MHS_OK;
 }
 
-template <int P, int KC>
+template <int P, int KC, class RF>
 int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
   char* ws = (char*)r->workspace;
   int* status = (int*)(ws + L.status);
@@ -1039,7 +1041,7 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
     dim3 g((unsigned)((nc + TB - 1) / TB), (unsigned)r->n_src);
     {
       StageTimer t(MHS_STAGE_PAIR, st);
-      k_pair<P, KC><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, G, coef, r->mu, r->lam, T);
+      k_pair<P, KC, RF><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, G, coef, r->mu, r->lam, T);
     }
     if constexpr (KC != KD_E) {
       StageTimer t(MHS_STAGE_IMAGEQ, st);
@@ -1051,16 +1053,16 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
       if constexpr (KC != KD_E) {
         dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
         const size_t fsm = sizeof(FoldShared<P, KC>);
-        CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)fsm));
         unsigned long long* census = nullptr;
         if (g_census_on.load(std::memory_order_relaxed))
           CUDA_TRY(cudaGetSymbolAddress((void**)&census, g_census));
-        k_fold<P, KC><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
+        k_fold<P, KC, RF><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
                                                         r->mu, r->lam, T, status, census);
       }
       dim3 gm((unsigned)((nc + TB - 1) / TB), (unsigned)r->n_src);
-      k_fold_mirror<P, KC><<<gm, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list, r->mu,
+      k_fold_mirror<P, KC, RF><<<gm, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list, r->mu,
                                               r->lam, T);
     }
     StageTimer tfin(MHS_STAGE_FINAL, st);
@@ -1098,10 +1100,17 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
 
 template <int P>
 int run_kind(const mhs_request* r, cudaStream_t st, const Layout& L) {
+  // mixed: far-field quadrature of the direct term, the fold's surface
+  // loads and its mirror in float with float accumulation; near-field
+  // recursions, image terms and the eigenstress subtraction stay double
+  const bool mixed = r->precision == MHS_MIXED;
   switch (kind_class(r->kind)) {
-    case KD_DISP: return run<P, KD_DISP>(r, st, L);
-    case KD_HE: return run<P, KD_HE>(r, st, L);
-    default: return run<P, KD_E>(r, st, L);
+    case KD_DISP:
+      return mixed ? run<P, KD_DISP, float>(r, st, L) : run<P, KD_DISP, double>(r, st, L);
+    case KD_HE:
+      return mixed ? run<P, KD_HE, float>(r, st, L) : run<P, KD_HE, double>(r, st, L);
+    default:
+      return mixed ? run<P, KD_E, float>(r, st, L) : run<P, KD_E, double>(r, st, L);
   }
 }
 
