@@ -184,6 +184,73 @@ def cpu_baseline(tris, eps, mu, lam, seconds: float, seed: int = 1):
 
 
 # ----------------------------------------------------------- our arm
+# Serving stream: seeded Poisson arrivals of uneven requests (the BASELINE
+# serving config's distributions with the sizes scaled down so the stream
+# takes seconds): kind uniform in {disp, stress, traction, interaction},
+# triangles log-uniform in [100, 2000], observers log-uniform in [100, 5000],
+# order uniform in {0, 1, 2}, eps per triangle 0.3 x its mean edge.
+SERVE = {"requests": 48, "rate_per_s": 20.0, "tris": (100, 2000), "obs": (100, 5000)}
+
+
+def _serve_requests(torch, dev, seed):
+    import mhs_b200 as mhs
+    from mhs_b200 import synthetic
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(SERVE["requests"]):
+        nt = int(np.exp(rng.uniform(*np.log(SERVE["tris"]))))
+        no = int(np.exp(rng.uniform(*np.log(SERVE["obs"]))))
+        nv = max(1, int(round(np.sqrt(nt / 6.0))))
+        nu = max(1, int(round(nt / (2 * nv))))
+        L, W = 2.0 * nu, 2.0 * nv
+        tris = synthetic.planar_fault(rng.uniform(0, 180), rng.uniform(15, 90), L, W,
+                                      -rng.uniform(0, 5), nu, nv)
+        edges = np.linalg.norm(tris - np.roll(tris, 1, axis=1), axis=2).mean(axis=1)
+        eps = torch.as_tensor(0.3 * edges, device=dev)
+        ext = 1.5 * max(L, W)
+        obs = np.column_stack([rng.uniform(-ext, ext, no), rng.uniform(-ext, ext, no),
+                               -rng.uniform(0, ext, no)])
+        t = torch.as_tensor(tris, device=dev)
+        o = torch.as_tensor(obs, device=dev)
+        mat = mhs.Material(30.0, float(rng.uniform(20, 40)))
+        order = int(rng.integers(0, 3))
+        kind = int(rng.integers(0, 4))
+        if kind == 0:
+            r = (mhs.disp_matrix, (o, t, mat, eps), {"order": order})
+        elif kind == 1:
+            r = (mhs.stress_matrix, (o, t, mat, eps), {"order": order})
+        elif kind == 2:
+            nrm = torch.as_tensor(rng.standard_normal((no, 3)), device=dev)
+            r = (mhs.traction_matrix, (o, nrm, t, mat, eps), {"order": order})
+        else:
+            r = (mhs.interaction_matrix, (t, mat, eps), {"order": order})
+        out.append((r, float(rng.exponential(1.0 / SERVE["rate_per_s"]))))
+    return out
+
+
+def serve_stream(dev, precision, seed):
+    """Latency percentiles and throughput of the seeded stream through the
+    serving loop (requests overlap on the device)."""
+    import torch
+    from mhs_b200 import serve
+    reqs = _serve_requests(torch, dev, seed)
+    torch.cuda.synchronize()
+    with serve.Server(dev, slots=8) as srv:
+        futs = []
+        t_next = time.perf_counter()
+        for (fn, args, kw), gap in reqs:
+            t_next += gap
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futs.append(srv.submit(fn, *args, precision=precision, **kw))
+        for f in futs:
+            f.result()
+        st = srv.stats()
+        st["peak_in_flight"] = srv.peak_in_flight
+    return st
+
+
 def run_ours(a, rank, world):
     import torch
     import mhs_b200 as mhs
@@ -303,6 +370,13 @@ def run_ours(a, rank, world):
     e2e_ms = float(e2e_t.item())
     e2e_val = world * entries * e2e_steps / (e2e_ms * 1e-3)
 
+    # serving: the seeded Poisson stream through the request loop, FP64 and mixed
+    serving = {"stream": dict(SERVE, note="sizes scaled down from the serving config; "
+                                        "arrivals Poisson, seeded; latency = submit to "
+                                        "result ready on the device, host clock"),
+               "fp64": serve_stream(dev, "fp64", 100 + rank),
+               "mixed": serve_stream(dev, "mixed", 100 + rank)}
+
     # roofline of the dominant stage (the fold): algorithmic flops of the
     # census'd work units over the stage's time per launch
     top = max(stages, key=lambda s: stages[s][0])
@@ -337,7 +411,7 @@ def run_ours(a, rank, world):
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": int(tris.nbytes + eps.nbytes),
                     "d2h_bytes_per_step": int(entries * 8)},
-            "roofline": roof, "mixed": mixed, "clocks": clk.summary(),
+            "roofline": roof, "mixed": mixed, "serving": serving, "clocks": clk.summary(),
             "gpu_launches": int(sum(v[1] * KERNELS_PER_STAGE[k] for k, v in stages.items()))}
     return line, tris, eps, mu, lam
 

@@ -463,8 +463,8 @@ MHS_HD void surface_load_near(const Frame& f, const MomentTable<SurfaceSpec<P>>&
 }
 
 // Surface load by the far-field product rule q.
-template <int P, class R_FAR = double>
-MHS_HD void surface_load_far(const QuadRule& q, const SurfaceLoadConsts& c, double z, double X0,
+template <int P, class R_FAR = double, class Q = QuadRule>
+MHS_HD void surface_load_far(const Q& q, const SurfaceLoadConsts& c, double z, double X0,
                              double X1, double h2, double* s /*K x 3*/) {
   using S = SurfaceSpec<P>;
   constexpr Spec sp = S::spec;

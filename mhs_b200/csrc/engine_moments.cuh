@@ -489,13 +489,15 @@ MHS_HD void weight_closed(const MomentTable<S>& T, const double c[][ntri(P)], in
 // Collapsed Gauss product rule on the reference triangle, mapped onto the
 // element: nodes eta (centroid frame), weights wq (area measure) and N_k at
 // the nodes (mhs/fullspace/moments.py:401-446).  Built once per source.
-struct QuadRule {
+template <class T>
+struct QuadRuleT {
   int nq;
-  const double* eta0;
-  const double* eta1;
-  const double* wq;
-  const double* Nq;   // nq x K, node-major
+  const T* eta0;
+  const T* eta1;
+  const T* wq;
+  const T* Nq;   // nq x K, node-major
 };
+using QuadRule = QuadRuleT<double>;
 
 // Fill a rule for order n from the 1-D Gauss-Legendre table (x in [-1, 1]).
 template <int P>
@@ -525,8 +527,8 @@ MHS_HD void build_rule(const Frame& f, const double* glx, const double* glw, int
 // W_k[n](a, b) by quadrature of N_k xi_1^a xi_2^b R^-n at the constant-slip
 // degrees (mhs/fullspace/moments.py:427-498).  R is float or double: the
 // mixed-precision form runs this in float with float accumulation.
-template <class S, int P, class R>
-MHS_HD void weight_far(const QuadRule& q, double X0, double X1, double h2, double* Wout) {
+template <class S, int P, class R, class Q = QuadRule>
+MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, double* Wout) {
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
   constexpr int NW = sp.w_off[NS];

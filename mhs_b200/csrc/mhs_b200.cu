@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <type_traits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -388,11 +389,21 @@ struct FoldWarp {
   int nbrk;
 };
 
-template <int P, int KC>
+// Float copies of the element's far rules for the mixed form.
+template <int P>
+struct FloatRules {
+  static constexpr int N = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N +
+                           cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
+  float e0[N], e1[N], wq[N], Nq[N * n_nodes(P)];
+};
+struct NoRules {};
+
+template <int P, int KC, class RF>
 struct FoldShared {
   SrcPrep sp;
   SmemRules<P> rd;       // element (surface load)
   SurfaceLoadConsts slc; // sigma_zz row of the element's H, per slip component
+  std::conditional_t<std::is_same<RF, float>::value, FloatRules<P>, NoRules> fr;
   FoldWarp<P, KC> w[FOLD_WARPS];
 };
 
@@ -519,7 +530,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if ((int64_t)blockIdx.x * FOLD_WARPS >= n_band) return;
   extern __shared__ __align__(16) unsigned char fold_smem[];
-  FoldShared<P, KC>& sh = *reinterpret_cast<FoldShared<P, KC>*>(fold_smem);
+  FoldShared<P, KC, RF>& sh = *reinterpret_cast<FoldShared<P, KC, RF>*>(fold_smem);
   SrcPrep& sp = sh.sp;
   SmemRules<P>& rd = sh.rd;
   FoldWarp<P, KC>& W = sh.w[wid];
@@ -537,6 +548,16 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     if (threadIdx.x == 32) surface_load_ezz(sp.f, sp.eps, m, sh.slc);
   }
   __syncthreads();
+  if constexpr (std::is_same<RF, float>::value) {
+    constexpr int NQ = FloatRules<P>::N;
+    for (int t = threadIdx.x; t < NQ; t += 32 * FOLD_WARPS) {
+      sh.fr.e0[t] = (float)rd.e0[t];
+      sh.fr.e1[t] = (float)rd.e1[t];
+      sh.fr.wq[t] = (float)rd.wq[t];
+    }
+    for (int t = threadIdx.x; t < NQ * K; t += 32 * FOLD_WARPS) sh.fr.Nq[t] = (float)rd.Nq[t];
+    __syncthreads();
+  }
   const int bi = blockIdx.x * FOLD_WARPS + wid;
   if (bi >= n_band) return;
   const int64_t oc = list[s * n_chunk + bi];
@@ -617,7 +638,16 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
         // far loads
 #pragma unroll 1
         for (int c = SL_FAR12; c <= SL_FAR8; ++c) {
-          const QuadRule& q = c == SL_FAR8 ? r8 : r12;
+          constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
+          const QuadRule& qd = c == SL_FAR8 ? r8 : r12;
+          QuadRuleT<RF> q;
+          if constexpr (std::is_same<RF, float>::value) {
+            const int off = c == SL_FAR8 ? N12 : 0;
+            q = QuadRuleT<float>{qd.nq, sh.fr.e0 + off, sh.fr.e1 + off, sh.fr.wq + off,
+                                 sh.fr.Nq + off * K};
+          } else {
+            q = qd;
+          }
           for (int b = 0; b < ncls[c]; b += 32) {
             if (b + lane < ncls[c]) {
               const int u = W.list[c][b + lane];
@@ -1052,7 +1082,7 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
       k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
       if constexpr (KC != KD_E) {
         dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
-        const size_t fsm = sizeof(FoldShared<P, KC>);
+        const size_t fsm = sizeof(FoldShared<P, KC, RF>);
         CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)fsm));
         unsigned long long* census = nullptr;

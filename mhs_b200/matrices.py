@@ -22,6 +22,7 @@ One extra keyword, ``precision="fp64"`` (default, every term in float64) or
 from __future__ import annotations
 
 import ctypes
+import threading
 
 import numpy as np
 
@@ -211,6 +212,77 @@ def _dev_tensor(a, device):
     return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device)
 
 
+# Deferred mode (used by mhs_b200.serve): inside ``deferred()`` the public
+# functions validate and stage their inputs on the device but return a
+# Pending request instead of running it.
+_defer = threading.local()
+
+
+class deferred:
+    """Context manager: public matrix functions return :class:`Pending`."""
+
+    def __enter__(self):
+        _defer.on = True
+        return self
+
+    def __exit__(self, *exc):
+        _defer.on = False
+
+
+class Pending:
+    """A validated request, staged on its device and not yet run.  The
+    caller supplies the stream and workspace; the result stays on the
+    device."""
+
+    def __init__(self, req, keep, out_shape, out_dtype, device, ws_bytes, entries):
+        self.req, self.keep = req, keep
+        self.out_shape, self.out_dtype, self.device = out_shape, out_dtype, device
+        self.ws_bytes = int(ws_bytes)
+        self.entries = int(entries)
+        self.out = None
+        self.ws = None
+        self.ready = None   # event after which the staged inputs are on the device
+
+    @property
+    def out_bytes(self) -> int:
+        n = 1
+        for d in self.out_shape:
+            n *= int(d)
+        return n * (4 if self.out_dtype == _torch().float32 else 8)
+
+    @property
+    def device_bytes(self) -> int:
+        """Bytes the run holds on the device: output, workspace, inputs."""
+        return self.out_bytes + self.ws_bytes + sum(t.numel() * t.element_size() for t in self.keep)
+
+    def launch(self, stream) -> None:
+        """Allocate the output and workspace and queue the assembly on `stream`."""
+        torch = _torch()
+        if self.ready is not None:
+            stream.wait_event(self.ready)
+        with torch.cuda.device(self.device), torch.cuda.stream(stream):
+            self.out = torch.empty(self.out_shape, dtype=self.out_dtype, device=self.device)
+            self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
+        self.req.out = ctypes.c_void_p(self.out.data_ptr())
+        self.req.workspace = ctypes.c_void_p(self.ws.data_ptr())
+        self.req.workspace_bytes = self.ws_bytes
+        _native.check(_native.load().mhs_assemble(ctypes.byref(self.req),
+                                                  ctypes.c_void_p(stream.cuda_stream)))
+
+    def finish(self, stream):
+        """After the stream's work completed: check the device status and
+        return the device tensor (workspace and inputs are released)."""
+        bits = ctypes.c_int(0)
+        _native.check(_native.load().mhs_read_status(ctypes.c_void_p(self.ws.data_ptr()),
+                                                     ctypes.c_void_p(stream.cuda_stream),
+                                                     ctypes.byref(bits)))
+        self.ws, self.keep = None, []
+        if bits.value & _native.DEV_FOLD_GRID_OVERFLOW:
+            raise RuntimeError("a fold polar grid exceeded its capacity (FOLD_MAX_BREAKS); "
+                               "the source is far larger than its eps")
+        return self.out
+
+
 def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fold,
             subtract=True, normals=None, rec_basis=None, src_basis=None, precision="fp64",
             like=None):
@@ -219,6 +291,9 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
     lib = _native.load()
     device = _device(*(like or ()), out)
     return_torch = any(_is_torch(x) for x in (like or ()))
+    defer = getattr(_defer, "on", False)
+    if defer and out is not None:
+        raise ValueError("a served request returns its own device tensor: out= does not apply")
     # output buffer
     dev_out = None
     if out is not None and _is_torch(out) and out.is_cuda:
@@ -226,7 +301,7 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
     want_f32 = out is not None and (
         (_is_torch(out) and out.dtype == torch.float32) or
         (not _is_torch(out) and np.asarray(out).dtype == np.float32))
-    if dev_out is None:
+    if dev_out is None and not defer:
         dev_out = torch.empty(out_shape, dtype=torch.float32 if want_f32 else torch.float64,
                               device=device)
     keep = []
@@ -268,9 +343,16 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
             keep.append(t)
             setattr(req, name, ctypes.c_void_p(t.data_ptr()))
         req.n_cols = n_dof
-    req.out = ctypes.c_void_p(dev_out.data_ptr())
+    # (deferred: the output is allocated at launch; the size query only needs
+    # a non-null pointer, so it is given the observers' buffer meanwhile)
+    req.out = req.obs if dev_out is None else ctypes.c_void_p(dev_out.data_ptr())
     mn, good = ctypes.c_size_t(), ctypes.c_size_t()
     _native.check(lib.mhs_workspace_bytes(ctypes.byref(req), ctypes.byref(mn), ctypes.byref(good)))
+    if defer:
+        entries = 1
+        for d in out_shape:
+            entries *= int(d)
+        return Pending(req, keep, tuple(out_shape), torch.float64, device, good.value, entries)
     ws = _WS.get(device, good.value)
     req.workspace = ctypes.c_void_p(ws.data_ptr())
     req.workspace_bytes = ws.numel()
@@ -347,6 +429,9 @@ def stress_matrix(obs_pts, tris, material, eps, *, subtract_eigenstress=True, pa
     if parts and out is not None:
         raise ValueError("parts=True returns two arrays, so out= cannot name the destination "
                          "of both; call twice with out=, or drop out=.")
+    if parts and getattr(_defer, "on", False):
+        raise ValueError("a served request returns one matrix: submit stress and "
+                         "eigenstress separately")
     sig = _launch(_native.STRESS, obs, tri, mu, lam, eps_arr, p, ids, n_dof, shape, out, fold,
                   subtract=subtract_eigenstress, precision=precision, like=(obs_pts, tris))
     if not parts:

@@ -1,0 +1,79 @@
+"""The serving loop (mhs_b200.serve): requests of different kinds, sizes,
+orders and precisions submitted together run overlapped on the device, and
+each result equals the same request run alone through the public API."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from mhs_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(torch, dev):
+    import mhs_b200 as m
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(10):
+        n_u, n_v = int(rng.integers(2, 7)), int(rng.integers(2, 5))
+        tris = synthetic.planar_fault(rng.uniform(0, 90), rng.uniform(20, 90), 6.0, 4.0,
+                                      -rng.uniform(0, 2), n_u, n_v)
+        obs = np.column_stack([rng.uniform(-15, 15, 60), rng.uniform(-15, 15, 60),
+                               -rng.uniform(0, 8, 60)])
+        t = torch.as_tensor(tris, device=dev)
+        o = torch.as_tensor(obs, device=dev)
+        mat = m.Material(30.0, float(rng.uniform(20, 40)))
+        order = int(rng.integers(0, 3))
+        prec = "mixed" if i % 3 == 2 else "fp64"
+        kind = i % 4
+        if kind == 0:
+            reqs.append((m.disp_matrix, (o, t, mat, 0.1), dict(order=order, precision=prec)))
+        elif kind == 1:
+            reqs.append((m.stress_matrix, (o, t, mat, 0.1), dict(order=order, precision=prec)))
+        elif kind == 2:
+            nrm = torch.as_tensor(rng.standard_normal((60, 3)), device=dev)
+            reqs.append((m.traction_matrix, (o, nrm, t, mat, 0.1), dict(order=order, precision=prec)))
+        else:
+            reqs.append((m.interaction_matrix, (t, mat, 0.1), dict(order=order, precision=prec)))
+    return reqs
+
+
+@pytest.mark.parametrize("slots", [4, 1])
+def test_each_result_is_the_same_alone_and_in_the_mix(cuda, slots):
+    import torch
+    from mhs_b200 import serve
+    reqs = _requests(torch, cuda)
+    alone = [fn(*a, **k) for fn, a, k in reqs]
+    torch.cuda.synchronize()
+    with serve.Server(cuda, slots=slots) as srv:
+        futs = [srv.submit(fn, *a, **k) for fn, a, k in reqs]
+        mixed = [f.result(timeout=300) for f in futs]
+        st = srv.stats()
+        peak = srv.peak_in_flight
+    for r_alone, r_mix in zip(alone, mixed):
+        assert r_mix.is_cuda and r_mix.shape == r_alone.shape
+        assert torch.equal(r_alone, r_mix)
+    assert st["requests"] == len(reqs) and st["p50_ms"] > 0 and st["p99_ms"] >= st["p50_ms"]
+    assert 1 <= peak <= slots
+    if slots > 1:
+        assert peak > 1, "requests were never in flight together"
+
+
+def test_byte_budget_admission_and_refusal(cuda):
+    import torch
+    from mhs_b200 import matrices, serve
+    reqs = _requests(torch, cuda)[:6]
+    alone = [fn(*a, **k) for fn, a, k in reqs]
+    with matrices.deferred():
+        sizes = [fn(*a, **k).device_bytes for fn, a, k in reqs]
+    budget = max(sizes) + min(sizes)          # never all six at once
+    with serve.Server(cuda, budget_bytes=budget, slots=8) as srv:
+        res = [f.result(timeout=300) for f in [srv.submit(fn, *a, **k) for fn, a, k in reqs]]
+        assert srv.peak_bytes <= budget
+    for a, b in zip(alone, res):
+        assert torch.equal(a, b)
+    big = int(np.argmax(sizes))
+    with serve.Server(cuda, budget_bytes=sizes[big] - 1, slots=2) as srv:
+        with pytest.raises(MemoryError, match="serving budget"):
+            srv.submit(reqs[big][0], *reqs[big][1], **reqs[big][2])

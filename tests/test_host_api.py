@@ -140,3 +140,11 @@ def test_constants_agree_across_package_engine_and_oracle():
     for k, v in pairs.items():
         assert eng[k] == v, k
         assert getattr(defaults, k) == v, k
+
+
+def test_serving_admission_rule():
+    from mhs_b200.serve import admissible
+    assert admissible(10, 80, 3, 100, 4)
+    assert not admissible(30, 80, 3, 100, 4)     # bytes
+    assert not admissible(1, 0, 4, 100, 4)       # slots
+    assert admissible(100, 0, 0, 100, 1)         # exactly the budget
