@@ -200,8 +200,8 @@ MHS_HD void szz_coefficient(const Frame& f, double eps, const Material& m, int l
 // The node loops are fully unrolled so that every output offset is a
 // compile-time constant: a -O3 device build with them kept rolled returned
 // wrong P >= 1 tensors where this function is inlined into the fold kernels.
-template <int P, int WANT, class R_FAR = double>
-MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
+template <int P, int WANT, class R_FAR = double, class Q = QuadRule>
+MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
                         const double* x, double eps, const Material& m,
                         double* U, double* H, double* E) {
   using S = DirectSpec<P, WANT>;
@@ -228,7 +228,7 @@ MHS_HD void direct_eval(const Frame& f, const QuadRule& r12, const QuadRule& r8,
       if (WANT & W_E) E[k] = e4 * W[sp.w_off[nslot(7)]];
     }
   } else {
-    const QuadRule& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
+    const Q& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
     double W[K * NW] = {};
     weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
 #pragma unroll
@@ -531,32 +531,34 @@ MHS_HD void build_qrule(const Frame& f, const double* glx, const double* glw, in
 // straight-line code.  Each monomial is formed as the ordered product
 // p1[a] p2[b] p3[c] pr[n] pq[q] with p[0] = 1 (a factor of one is exact), the
 // points are summed in rule order and the records in table order, as mhs
-// does.  Rule: count() and node(t, y, wN[K]).
-template <int P, int WANT, class Rule>
+// does.  Rule: count() and node(t, y, wN[K]) in the arithmetic type R of
+// the point sums (double; float for the mixed form's far pairs).
+template <int P, int WANT, class Rule, class R = double>
 MHS_HD void image_q_eval(const Rule& q, const double* nrm, const double* x, double eps,
                          const Material& m, const ImageCoef& ic, double* U, double* H) {
   static_assert(WANT == W_U || WANT == W_H, "one contraction per call");
   constexpr int K = n_nodes(P);
-  const double e2 = eps * eps;
+  const R e2 = R(eps * eps);
+  const R x0 = R(x[0]), x1 = R(x[1]), x2 = R(x[2]);
   const int nq = q.count();
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    double bs[MHS_Q_NMONO];
-#define MHS_QZ(i, a, b, c, n, qq) bs[i] = 0.0;
+    R bs[MHS_Q_NMONO];
+#define MHS_QZ(i, a, b, c, n, qq) bs[i] = R(0);
     if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QZ) }
     else { MHS_Q_MONO_DDG(MHS_QZ) }
 #undef MHS_QZ
 #pragma unroll 1
     for (int t = 0; t < nq; ++t) {
-      double y[3], wN[K];
+      R y[3], wN[K];
       q.node(t, y, wN);
-      const double d1 = x[0] - y[0];
-      const double d2 = x[1] - y[1];
-      const double d3 = x[2] + y[2];
-      const double r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
-      const double ir = 1.0 / r2, iq = 1.0 / (r2 - d3);
-      double p1[5], p2[5], p3[5], pr[8], pq[5];
-      p1[0] = 1.0; p2[0] = 1.0; p3[0] = 1.0; pr[0] = 1.0; pq[0] = 1.0;
+      const R d1 = x0 - y[0];
+      const R d2 = x1 - y[1];
+      const R d3 = x2 + y[2];
+      const R r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
+      const R ir = R(1) / r2, iq = R(1) / (r2 - d3);
+      R p1[5], p2[5], p3[5], pr[8], pq[5];
+      p1[0] = R(1); p2[0] = R(1); p3[0] = R(1); pr[0] = R(1); pq[0] = R(1);
       p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
 #pragma unroll
       for (int i = 2; i < 5; ++i) {
@@ -567,7 +569,7 @@ MHS_HD void image_q_eval(const Rule& q, const double* nrm, const double* x, doub
       }
 #pragma unroll
       for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
-      const double w = wN[k];
+      const R w = wN[k];
 #define MHS_QA(i, a, b, c, n, qq) bs[i] += ((((p1[a] * p2[b]) * p3[c]) * pr[n]) * pq[qq]) * w;
       if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QA) }
       else { MHS_Q_MONO_DDG(MHS_QA) }

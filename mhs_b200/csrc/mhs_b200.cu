@@ -100,6 +100,37 @@ struct SmemRules {
   __device__ QuadRule r8() const { return QuadRule{N8, e0 + N12, e1 + N12, wq + N12, Nq + N12 * K}; }
 };
 
+// Float copies of the element's far rules for the mixed form.
+template <int P>
+struct FloatRules {
+  static constexpr int N = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N +
+                           cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
+  float e0[N], e1[N], wq[N], Nq[N * n_nodes(P)];
+};
+struct NoRules {};
+
+// Float copies of a block's rules (the mixed form), as QuadRuleT<float>.
+template <int P>
+__device__ void float_rules(const SmemRules<P>& rd, FloatRules<P>& fr, int tid, int nthr) {
+  constexpr int N = FloatRules<P>::N, K = n_nodes(P);
+  for (int t = tid; t < N; t += nthr) {
+    fr.e0[t] = (float)rd.e0[t];
+    fr.e1[t] = (float)rd.e1[t];
+    fr.wq[t] = (float)rd.wq[t];
+  }
+  for (int t = tid; t < N * K; t += nthr) fr.Nq[t] = (float)rd.Nq[t];
+}
+template <int P>
+__device__ QuadRuleT<float> float_r12(const FloatRules<P>& fr) {
+  return QuadRuleT<float>{cst::FAR_GAUSS_N * cst::FAR_GAUSS_N, fr.e0, fr.e1, fr.wq, fr.Nq};
+}
+template <int P>
+__device__ QuadRuleT<float> float_r8(const FloatRules<P>& fr) {
+  constexpr int O = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
+  return QuadRuleT<float>{cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT, fr.e0 + O, fr.e1 + O,
+                          fr.wq + O, fr.Nq + O * n_nodes(P)};
+}
+
 // ---------------------------------------------------------------- k_coef
 __global__ void k_coef(double mu, double lam, double* out) {
   const Material m = make_material(mu, lam);
@@ -172,6 +203,8 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   __shared__ SmemRules<P> rd;
   __shared__ SmemRules<IMG ? P : 0> ri;
   __shared__ double sG[IMG ? G_SIZE : 1];
+  constexpr bool F32 = std::is_same<RF, float>::value;
+  __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rdf;
   if (threadIdx.x == 0) sp = prep[s];
   __syncthreads();
   rd.build(sp.f, threadIdx.x, TB);
@@ -180,6 +213,10 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     for (int i = threadIdx.x; i < G_SIZE; i += TB) sG[i] = Gall[s * G_SIZE + i];
   }
   __syncthreads();
+  if constexpr (F32) {
+    float_rules<P>(rd, rdf, threadIdx.x, TB);
+    __syncthreads();
+  }
   const int64_t oc = blockIdx.x * (int64_t)TB + threadIdx.x;
   if (oc >= n_chunk) return;
   const int64_t o = lo + oc;
@@ -189,7 +226,8 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   double* row = T + ((oc * n_src + s) * K) * NR;
   if constexpr (KC == KD_E) {
     double E[K] = {};
-    direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
+    if constexpr (F32) direct_eval<P, W_E, RF>(sp.f, float_r12<P>(rdf), float_r8<P>(rdf), x, eps, m, nullptr, nullptr, E);
+    else direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
     for (int k = 0; k < K; ++k) {
       row[k * NR + 0] = E[k];
       row[k * NR + 1] = 0.0;
@@ -198,10 +236,18 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   } else {
     constexpr int C = comps_of(KC);
     double A[K * C] = {}, E[K] = {};
-    if constexpr (KC == KD_DISP)
-      direct_eval<P, W_U, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
-    else
-      direct_eval<P, W_H | W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
+    if constexpr (F32) {
+      const QuadRuleT<float> f12 = float_r12<P>(rdf), f8 = float_r8<P>(rdf);
+      if constexpr (KC == KD_DISP)
+        direct_eval<P, W_U, RF>(sp.f, f12, f8, x, eps, m, A, nullptr, nullptr);
+      else
+        direct_eval<P, W_H | W_E, RF>(sp.f, f12, f8, x, eps, m, nullptr, A, E);
+    } else {
+      if constexpr (KC == KD_DISP)
+        direct_eval<P, W_U, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
+      else
+        direct_eval<P, W_H | W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
+    }
     const bool band = sp.straddle && fold_band(x, sp.centre, eps);
     if (!band) {
       double B[K * C] = {};
@@ -224,14 +270,14 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
 // Image Q-family of one pair, added to the scratch row.  The floor order
 // (8 x 8 points, almost every pair) reads a shared-memory rule; higher
 // orders generate their nodes on the fly.
-template <int P>
+template <int P, class E = double>
 struct QRuleSmem {
   static constexpr int K = n_nodes(P);
-  const double* y;
-  const double* wN;
+  const E* y;
+  const E* wN;
   int nq;
   __device__ int count() const { return nq; }
-  __device__ void node(int t, double* yy, double* w) const {
+  __device__ void node(int t, E* yy, E* w) const {
     yy[0] = y[3 * t];
     yy[1] = y[3 * t + 1];
     yy[2] = y[3 * t + 2];
@@ -258,7 +304,9 @@ struct QRuleFly {
   }
 };
 
-template <int P, int KC>
+// RF = float (the mixed form): pairs at the floor order -- at least about an
+// element from the image triangle -- sum their points in float.
+template <int P, int KC, class RF>
 __global__ void __launch_bounds__(TB)
 k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
          const SrcPrep* __restrict__ prep, const double* __restrict__ coef, double mu, double lam,
@@ -270,6 +318,9 @@ k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ 
   __shared__ SrcPrep sp;
   __shared__ double qy[QFLOOR * QFLOOR * 3];
   __shared__ double qw[QFLOOR * QFLOOR * K];
+  constexpr bool F32 = std::is_same<RF, float>::value;
+  __shared__ float qyf[F32 ? QFLOOR * QFLOOR * 3 : 1];
+  __shared__ float qwf[F32 ? QFLOOR * QFLOOR * K : 1];
   if (threadIdx.x == 0) sp = prep[s];
   __syncthreads();
   {
@@ -277,6 +328,11 @@ k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ 
     for (int t = threadIdx.x; t < QFLOOR * QFLOOR; t += TB) fly.node(t, qy + 3 * t, qw + K * t);
   }
   __syncthreads();
+  if constexpr (F32) {
+    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * 3; t += TB) qyf[t] = (float)qy[t];
+    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * K; t += TB) qwf[t] = (float)qw[t];
+    __syncthreads();
+  }
   const int64_t oc = blockIdx.x * (int64_t)TB + threadIdx.x;
   if (oc >= n_chunk) return;
   const int64_t o = lo + oc;
@@ -291,7 +347,16 @@ k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ 
   const int n = q_gauss_order(x, ti, eps, sp.f.L, P);
   double B[K * C] = {};
   constexpr int WANT = KC == KD_DISP ? W_U : W_H;
-  if (n == QFLOOR) {
+  bool done = false;
+  if constexpr (F32) {
+    if (n == QFLOOR) {
+      QRuleSmem<P, float> r{qyf, qwf, QFLOOR * QFLOOR};
+      image_q_eval<P, WANT, QRuleSmem<P, float>, float>(r, sp.f.n, x, eps, m, ic, B, B);
+      done = true;
+    }
+  }
+  if (done) {
+  } else if (n == QFLOOR) {
     QRuleSmem<P> r{qy, qw, QFLOOR * QFLOOR};
     image_q_eval<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
   } else {
@@ -388,15 +453,6 @@ struct FoldWarp {
   double R1;
   int nbrk;
 };
-
-// Float copies of the element's far rules for the mixed form.
-template <int P>
-struct FloatRules {
-  static constexpr int N = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N +
-                           cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
-  float e0[N], e1[N], wq[N], Nq[N * n_nodes(P)];
-};
-struct NoRules {};
 
 template <int P, int KC, class RF>
 struct FoldShared {
@@ -549,13 +605,7 @@ k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   }
   __syncthreads();
   if constexpr (std::is_same<RF, float>::value) {
-    constexpr int NQ = FloatRules<P>::N;
-    for (int t = threadIdx.x; t < NQ; t += 32 * FOLD_WARPS) {
-      sh.fr.e0[t] = (float)rd.e0[t];
-      sh.fr.e1[t] = (float)rd.e1[t];
-      sh.fr.wq[t] = (float)rd.wq[t];
-    }
-    for (int t = threadIdx.x; t < NQ * K; t += 32 * FOLD_WARPS) sh.fr.Nq[t] = (float)rd.Nq[t];
+    float_rules<P>(rd, sh.fr, threadIdx.x, 32 * FOLD_WARPS);
     __syncthreads();
   }
   const int bi = blockIdx.x * FOLD_WARPS + wid;
@@ -1075,7 +1125,7 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
     }
     if constexpr (KC != KD_E) {
       StageTimer t(MHS_STAGE_IMAGEQ, st);
-      k_imageq<P, KC><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, coef, r->mu, r->lam, T);
+      k_imageq<P, KC, RF><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, coef, r->mu, r->lam, T);
     }
     if (r->fold) {
       StageTimer t(MHS_STAGE_FOLD, st);
@@ -1131,8 +1181,10 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
 template <int P>
 int run_kind(const mhs_request* r, cudaStream_t st, const Layout& L) {
   // mixed: far-field quadrature of the direct term, the fold's surface
-  // loads and its mirror in float with float accumulation; near-field
-  // recursions, image terms and the eigenstress subtraction stay double
+  // loads and its mirror, and the image Q-family points of pairs at the
+  // floor order, in float with float accumulation; near-field recursions,
+  // the image R-family, higher-order image Q and the eigenstress
+  // subtraction stay double
   const bool mixed = r->precision == MHS_MIXED;
   switch (kind_class(r->kind)) {
     case KD_DISP:
