@@ -29,11 +29,27 @@ MHS_FI double ipow(double x, int e) {
 // on one side, the closed-form difference forms otherwise
 // (mhs/fullspace/primitives.py:131-504; rho > 0 always since eps > 0).
 
-template <class S>
+// FAST (the fold's near loads): the same forms with the radii from
+// reciprocal square roots and the divisions by R_a, R_b and rho2 taken as
+// products with their reciprocals (rounding-level differences).
+template <class S, bool FAST = false>
 MHS_HD void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
   constexpr Spec sp = S::spec;
-  const double Ra = sqrt(ua * ua + rho2);
-  const double Rb = sqrt(ub * ub + rho2);
+  double Ra, Rb, iRa, iRb, irho2;
+  if constexpr (FAST) {
+    const double qa = ua * ua + rho2, qb = ub * ub + rho2;
+    iRa = rsqrt_r(qa);
+    iRb = rsqrt_r(qb);
+    Ra = qa * iRa;
+    Rb = qb * iRb;
+    irho2 = 1.0 / rho2;
+  } else {
+    Ra = sqrt(ua * ua + rho2);
+    Rb = sqrt(ub * ub + rho2);
+    iRa = 1.0 / Ra;
+    iRb = 1.0 / Rb;
+    irho2 = 0.0;
+  }
   const double dR = (ub - ua) * (ub + ua) / (Ra + Rb);   // R_b - R_a
   double J[MS], Kk[MS];
   // Delta J_1: log1p forms on one side, the product form across the foot
@@ -43,19 +59,24 @@ MHS_HD void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
     else J[1] = log(((ub + Rb) * (Ra - ua)) / rho2);
   }
   if (sp.Jneed[2]) {
-    if (ua * ub > 0.0) J[2] = ((ub - ua) * (ub + ua)) / ((Ra * Rb) * (ub * Ra + ua * Rb));
-    else J[2] = (ub / Rb - ua / Ra) / rho2;
+    if constexpr (FAST) {
+      if (ua * ub > 0.0) J[2] = (((ub - ua) * (ub + ua)) * (iRa * iRb)) / (ub * Ra + ua * Rb);
+      else J[2] = (ub * iRb - ua * iRa) * irho2;
+    } else {
+      if (ua * ub > 0.0) J[2] = ((ub - ua) * (ub + ua)) / ((Ra * Rb) * (ub * Ra + ua * Rb));
+      else J[2] = (ub / Rb - ua / Ra) / rho2;
+    }
   }
   if (sp.Jneed[3]) {  // m = 5 from m = 3
-    const double iRa = 1.0 / Ra, iRb = 1.0 / Rb;
     const double duRm = ub * (iRb * iRb * iRb) - ua * (iRa * iRa * iRa);
-    J[3] = (duRm + 2.0 * J[2]) / (3.0 * rho2);
+    if constexpr (FAST) J[3] = (duRm + 2.0 * J[2]) * (irho2 * (1.0 / 3.0));
+    else J[3] = (duRm + 2.0 * J[2]) / (3.0 * rho2);
   }
   if (sp.Jneed[4]) {  // m = 7 from m = 5
-    const double iRa = 1.0 / Ra, iRb = 1.0 / Rb;
     const double a2 = iRa * iRa, b2 = iRb * iRb;
     const double duRm = ub * (b2 * b2 * iRb) - ua * (a2 * a2 * iRa);
-    J[4] = (duRm + 4.0 * J[3]) / (5.0 * rho2);
+    if constexpr (FAST) J[4] = (duRm + 4.0 * J[3]) * (irho2 * 0.2);
+    else J[4] = (duRm + 4.0 * J[3]) / (5.0 * rho2);
   }
   if (sp.Jneed[0]) {  // m = -1
     const double duR = 0.5 * (ub - ua) * (Ra + Rb) + 0.5 * (ua + ub) * dR;
@@ -64,15 +85,27 @@ MHS_HD void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
   // Delta K_m = Delta R^(2-m) / (2-m), factored through dR
   if (sp.Kneed[0]) Kk[0] = dR * ((Rb * Rb + Ra * Rb) + Ra * Ra) / 3.0;
   if (sp.Kneed[1]) Kk[1] = dR;
-  if (sp.Kneed[2]) Kk[2] = dR / (Ra * Rb);
-  if (sp.Kneed[3]) {
-    const double ab = Ra * Rb;
-    Kk[3] = dR * ((Rb * Rb + Ra * Rb) + Ra * Ra) / (3.0 * (ab * ab * ab));
-  }
-  if (sp.Kneed[4]) {
-    const double ab = Ra * Rb, a2 = Ra * Ra, b2 = Rb * Rb;
-    const double s = (((b2 * b2 + Ra * (b2 * Rb)) + a2 * b2) + (a2 * Ra) * Rb) + a2 * a2;
-    Kk[4] = dR * s / (5.0 * (ab * ab * ab * ab * ab));
+  if constexpr (FAST) {
+    const double iab = iRa * iRb;
+    if (sp.Kneed[2]) Kk[2] = dR * iab;
+    if (sp.Kneed[3]) Kk[3] = (dR * ((Rb * Rb + Ra * Rb) + Ra * Ra)) * ((iab * iab * iab) * (1.0 / 3.0));
+    if (sp.Kneed[4]) {
+      const double a2 = Ra * Ra, b2 = Rb * Rb;
+      const double s = (((b2 * b2 + Ra * (b2 * Rb)) + a2 * b2) + (a2 * Ra) * Rb) + a2 * a2;
+      const double i2 = iab * iab;
+      Kk[4] = (dR * s) * ((i2 * i2 * iab) * 0.2);
+    }
+  } else {
+    if (sp.Kneed[2]) Kk[2] = dR / (Ra * Rb);
+    if (sp.Kneed[3]) {
+      const double ab = Ra * Rb;
+      Kk[3] = dR * ((Rb * Rb + Ra * Rb) + Ra * Ra) / (3.0 * (ab * ab * ab));
+    }
+    if (sp.Kneed[4]) {
+      const double ab = Ra * Rb, a2 = Ra * Ra, b2 = Rb * Rb;
+      const double s = (((b2 * b2 + Ra * (b2 * Rb)) + a2 * b2) + (a2 * Ra) * Rb) + a2 * a2;
+      Kk[4] = dR * s / (5.0 * (ab * ab * ab * ab * ab));
+    }
   }
 #pragma unroll
   for (int k = 0; k < 8; ++k)
@@ -323,6 +356,24 @@ MHS_FI EdgeGeom edge_geom(const double pr[3][2], int e, double h2) {
   EdgeGeom g;
   g.s1 = ev0 / L;
   g.s2 = ev1 / L;
+  const double c1 = g.s2, c2 = -g.s1;
+  g.dp = pa0 * c1 + pa1 * c2;
+  g.ua = pa0 * g.s1 + pa1 * g.s2;
+  g.ub = pb0 * g.s1 + pb1 * g.s2;
+  g.rho2 = g.dp * g.dp + h2;
+  return g;
+}
+
+// edge_geom with the tangent from one reciprocal square root of the squared
+// length (the fold's near loads; rounding-level differences).
+MHS_FI EdgeGeom edge_geom_rcp(const double pr[3][2], int e, double h2) {
+  const int e2 = e == 2 ? 0 : e + 1;
+  const double pa0 = pr[e][0], pa1 = pr[e][1], pb0 = pr[e2][0], pb1 = pr[e2][1];
+  const double ev0 = pb0 - pa0, ev1 = pb1 - pa1;
+  const double iL = rsqrt_r(ev0 * ev0 + ev1 * ev1);
+  EdgeGeom g;
+  g.s1 = ev0 * iL;
+  g.s2 = ev1 * iL;
   const double c1 = g.s2, c2 = -g.s1;
   g.dp = pa0 * c1 + pa1 * c2;
   g.ua = pa0 * g.s1 + pa1 * g.s2;

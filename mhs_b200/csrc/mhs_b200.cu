@@ -497,7 +497,7 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
     for (int e = 0; e < 3; ++e) {
       int form = -1;
       if (active) {
-        const EdgeGeom g = edge_geom(pr, e, h2);
+        const EdgeGeom g = edge_geom_rcp(pr, e, h2);
         W.edge.eu[3 * lane + e][0] = g.ua;
         W.edge.eu[3 * lane + e][1] = g.ub;
         W.edge.eu[3 * lane + e][2] = g.rho2;
@@ -518,7 +518,7 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
           const int slot = W.elist[r][q + lane];
           const double ua = W.edge.eu[slot][0], ub = W.edge.eu[slot][1], rho2 = W.edge.eu[slot][2];
           double Pt[MS][8];
-          if (r == EDGE_CLOSED) edge_closed<S>(ua, ub, rho2, Pt);
+          if (r == EDGE_CLOSED) edge_closed<S, true>(ua, ub, rho2, Pt);
           else if (r == EDGE_SMALL) edge_small<S>(ua, ub, sqrt(rho2), Pt);
           else edge_large<S>(ua, ub, rho2, Pt);
           int o = 0;
@@ -544,7 +544,7 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
 #pragma unroll 1
       for (int e = 0; e < 3; ++e) {
         const int slot = 3 * lane + e;
-        const EdgeGeom g = edge_geom(pr, e, h2);   // as in the pass above
+        const EdgeGeom g = edge_geom_rcp(pr, e, h2);   // as in the pass above
         double Pt[MS][8] = {};
         int o = 0;
 #pragma unroll

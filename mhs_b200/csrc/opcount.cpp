@@ -115,7 +115,7 @@ template <int P>
 void edge_unit(int form, double ua, double ub, double rho2) {
   using S = SurfaceSpec<P>;
   CountD Pt[MS][8];
-  if (form == EDGE_CLOSED) edge_closed<S>(ua, ub, rho2, Pt);
+  if (form == EDGE_CLOSED) edge_closed<S, true>(ua, ub, rho2, Pt);   // the fold's form
   else if (form == EDGE_SMALL) edge_small<S>(ua, ub, sqrt(CountD(rho2)), Pt);
   else edge_large<S>(ua, ub, rho2, Pt);
 }
@@ -138,7 +138,7 @@ void near_rest(const Frame& f, const SurfaceLoadConsts& c, double px, double py,
   for (int i = 0; i < NB; ++i) BN1[i] = BN2[i] = 0.0;
   for (int j = 0; j < MS; ++j) BD[j] = 0.0;
   for (int e = 0; e < 3; ++e) {
-    const EdgeGeom g = edge_geom(pr, e, h2);
+    const EdgeGeom g = edge_geom_rcp(pr, e, h2);   // the fold's form
     (void)edge_regime(g.ua, g.ub, sqrt(g.rho2));
     CountD Pt[MS][8] = {};
     for (int j = 0; j < MS; ++j)

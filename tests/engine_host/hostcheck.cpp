@@ -211,4 +211,20 @@ int hc_surface_load(int P, int fast, const double* pts, int npts, const double* 
   DISPATCH_P(surface_load_all, 0, pts, npts, tri, mu, lam, eps, s)
 }
 
+// One closed-form edge of the surface-load spec: the plain form or the
+// fold's reciprocal form (fast = 1); P[j][k] for j < 5, k < 8 into out.
+int hc_edge_closed(int P, int fast, double ua, double ub, double rho2, double* out) {
+  double Pt[MS][8] = {};
+#define HC_EC(PP)                                                                   \
+  {                                                                                 \
+    if (fast) edge_closed<SurfaceSpec<PP>, true>(ua, ub, rho2, Pt);                 \
+    else edge_closed<SurfaceSpec<PP>, false>(ua, ub, rho2, Pt);                     \
+  }
+  if (P == 0) HC_EC(0) else if (P == 1) HC_EC(1) else HC_EC(2)
+#undef HC_EC
+  for (int j = 0; j < MS; ++j)
+    for (int k = 0; k < 8; ++k) out[8 * j + k] = Pt[j][k];
+  return 0;
+}
+
 }  // extern "C"

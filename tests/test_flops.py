@@ -32,7 +32,7 @@ def test_series_edges_cost_their_32_terms(units):
     for P, u in units.items():
         assert u["edge_small"]["flop"] > 10 * u["edge_closed"]["flop"]
         assert u["edge_large"]["flop"] > 10 * u["edge_closed"]["flop"]
-        assert u["edge_closed"]["div"] >= 5
+        assert 1 <= u["edge_closed"]["div"] <= 6
 
 
 def test_order_raises_the_work(units):
