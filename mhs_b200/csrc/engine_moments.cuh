@@ -287,6 +287,19 @@ MHS_HD void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
 enum : int { EDGE_CLOSED = 0, EDGE_SMALL = 1, EDGE_LARGE = 2 };
 
 // Which of the three forms evaluates an edge (rho = sqrt(rho2)).
+// The same test on squares (rho2 = rho^2), without the square root: the
+// fold's near batch (a borderline edge may take the other, equally accurate
+// form).
+MHS_FI int edge_regime_sq(double ua, double ub, double rho2) {
+  const double a2 = ua * ua, b2 = ub * ub;
+  const double umax2 = a2 > b2 ? a2 : b2;
+  const double umin2 = a2 < b2 ? a2 : b2;
+  const double s2 = 0.25, l2 = 4.0;   // SMALL_U_OVER_RHO^2, SERIES_U_OVER_RHO^2 (exact)
+  if (umax2 <= s2 * rho2) return EDGE_SMALL;
+  if (ua * ub > 0.0 && umin2 >= l2 * rho2) return EDGE_LARGE;
+  return EDGE_CLOSED;
+}
+
 MHS_FI int edge_regime(double ua, double ub, double rho) {
   const double aua = fabs(ua), aub = fabs(ub);
   const double umax = aua > aub ? aua : aub;
@@ -439,14 +452,35 @@ MHS_HD void edge_accumulate(const EdgeGeom& g, const double P[MS][8], double* BN
   }
 }
 
+template <class S, bool FAST>
+MHS_HD void closed_finish_t(const double pr[3][2], double h2, const double* BN1, const double* BN2,
+                            const double* BD, MomentTable<S>& T);
+
 // Seeds (solid angle, vertical identities) and the horizontal recursion
 // from the summed boundary terms.
 template <class S>
 MHS_HD void closed_finish(const double pr[3][2], double h2, const double* BN1, const double* BN2,
                           const double* BD, MomentTable<S>& T) {
+  closed_finish_t<S, false>(pr, h2, BN1, BN2, BD, T);
+}
+
+// FAST (the fold's near loads): 1/h from a reciprocal square root and the
+// seeds' divisions by n h^2 as products with 1/h^2 (rounding-level
+// differences).
+template <class S, bool FAST>
+MHS_HD void closed_finish_t(const double pr[3][2], double h2, const double* BN1, const double* BN2,
+                            const double* BD, MomentTable<S>& T) {
   constexpr Spec sp = S::spec;
-  const double h = sqrt(h2);
-  const double I3 = -solid_angle_local(pr, h) / h;
+  double h, I3, ih2 = 0.0;
+  if constexpr (FAST) {
+    const double ih = rsqrt_r(h2);
+    h = h2 * ih;
+    I3 = -solid_angle_local(pr, h) * ih;
+    ih2 = ih * ih;
+  } else {
+    h = sqrt(h2);
+    I3 = -solid_angle_local(pr, h) / h;
+  }
 #pragma unroll
   for (int i = 0; i < sp.m_off[NS]; ++i) T.M[i] = 0.0;
   T.at(nslot(3), 0, 0) = I3;
@@ -454,7 +488,10 @@ MHS_HD void closed_finish(const double pr[3][2], double h2, const double* BN1, c
 #pragma unroll
   for (int n = 3; n + 2 <= 9; n += 2) {
     if (sp.deg[nslot(n + 2)] < 0) break;
-    T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) / (n * h2);
+    if constexpr (FAST)
+      T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) * (ih2 * (1.0 / n));
+    else
+      T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) / (n * h2);
   }
   // downward seeds I_n = (E_n - n h^2 I_{n+2}) / (2 - n)
 #pragma unroll

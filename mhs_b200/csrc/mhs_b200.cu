@@ -501,7 +501,7 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
         W.edge.eu[3 * lane + e][0] = g.ua;
         W.edge.eu[3 * lane + e][1] = g.ub;
         W.edge.eu[3 * lane + e][2] = g.rho2;
-        form = edge_regime(g.ua, g.ub, sqrt(g.rho2));
+        form = edge_regime_sq(g.ua, g.ub, g.rho2);
       }
 #pragma unroll
       for (int r = 0; r < 3; ++r) warp_append(form == r, 3 * lane + e, W.elist[r], cnt[r], lane);
@@ -556,7 +556,7 @@ __device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const Surfac
         edge_accumulate<S>(g, Pt, BN1, BN2, BD);
       }
       MomentTable<S> T;
-      closed_finish<S>(pr, h2, BN1, BN2, BD, T);
+      closed_finish_t<S, true>(pr, h2, BN1, BN2, BD, T);
       double sl[NJ] = {};
       surface_load_near<P>(f, T, c, z, X0, X1, sl);
 #pragma unroll

@@ -139,14 +139,14 @@ void near_rest(const Frame& f, const SurfaceLoadConsts& c, double px, double py,
   for (int j = 0; j < MS; ++j) BD[j] = 0.0;
   for (int e = 0; e < 3; ++e) {
     const EdgeGeom g = edge_geom_rcp(pr, e, h2);   // the fold's form
-    (void)edge_regime(g.ua, g.ub, sqrt(g.rho2));
+    (void)edge_regime_sq(g.ua, g.ub, g.rho2);
     CountD Pt[MS][8] = {};
     for (int j = 0; j < MS; ++j)
       for (int k = 0; k < 8; ++k) Pt[j][k] = 0.5;
     edge_accumulate<S>(g, Pt, BN1, BN2, BD);
   }
   MomentTable<S> T;
-  closed_finish<S>(pr, h2, BN1, BN2, BD, T);
+  closed_finish_t<S, true>(pr, h2, BN1, BN2, BD, T);
   CountD s[3 * K];
   surface_load_near<P>(f, T, c, z, X0, X1, s);
 }

@@ -227,4 +227,21 @@ int hc_edge_closed(int P, int fast, double ua, double ub, double rho2, double* o
   return 0;
 }
 
+// Seeds and recursion of one near node (surface-load spec, P0) from given
+// boundary sums: the plain form or the fold's reciprocal form (fast = 1).
+int hc_closed_finish(int fast, const double* pr6, double h2, const double* bn, double* out) {
+  using S = SurfaceSpec<0>;
+  constexpr Spec sp = S::spec;
+  constexpr int NB = sp.b_off[MS];
+  double pr[3][2] = {{pr6[0], pr6[1]}, {pr6[2], pr6[3]}, {pr6[4], pr6[5]}};
+  double BN1[NB], BN2[NB], BD[MS];
+  for (int i = 0; i < NB; ++i) { BN1[i] = bn[i]; BN2[i] = bn[NB + i]; }
+  for (int j = 0; j < MS; ++j) BD[j] = bn[2 * NB + j];
+  MomentTable<S> T;
+  if (fast) closed_finish_t<S, true>(pr, h2, BN1, BN2, BD, T);
+  else closed_finish_t<S, false>(pr, h2, BN1, BN2, BD, T);
+  for (int i = 0; i < sp.m_off[NS]; ++i) out[i] = T.M[i];
+  return sp.m_off[NS];
+}
+
 }  // extern "C"

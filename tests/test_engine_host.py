@@ -153,3 +153,19 @@ def test_fold_closed_edge_form_matches_plain(hc, P):
         if scale > 0:
             worst = max(worst, np.abs(a - b).max() / scale)
     assert worst < 1e-13
+
+
+def test_fold_finish_form_matches_plain(hc):
+    """The fold's seeds and recursion (reciprocal 1/h, products with 1/h^2)
+    agree with the plain form to rounding."""
+    rng = np.random.default_rng(9)
+    worst = 0.0
+    for _ in range(200):
+        pr = np.ascontiguousarray(rng.uniform(-2, 2, 6))
+        bn = np.ascontiguousarray(rng.uniform(-1, 1, 64))
+        h2 = float(rng.uniform(0.01, 3.0))
+        a, b = np.zeros(64), np.zeros(64)
+        n = hc.hc_closed_finish(0, _p(pr), ctypes.c_double(h2), _p(bn), _p(a))
+        hc.hc_closed_finish(1, _p(pr), ctypes.c_double(h2), _p(bn), _p(b))
+        worst = max(worst, np.abs(a[:n] - b[:n]).max() / np.abs(a[:n]).max())
+    assert worst < 1e-13
