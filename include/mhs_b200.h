@@ -115,14 +115,17 @@ int mhs_assemble(const mhs_request* req, void* stream);
  * whose work overlaps on the GPU -- on different streams, or from
  * different threads -- race: serialise them.
  *
- * status_bits: NULL to return once queued; otherwise the call synchronises
+ * status_bits: NULL to return once queued (read the status later with
+ * mhs_read_status(NULL, stream, &bits)); otherwise the call synchronises
  * `stream` and stores the device status bits there.
  * No counterpart in mhs (which never runs on a device). */
 #define MHS_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits);
 
 /* Synchronise `stream` and return the device status bits of the last
- * request that used `workspace` (0 = clean), clearing them. */
+ * request that used `workspace` (0 = clean), clearing them.  workspace =
+ * NULL reads the status of the last mhs_assemble_noalloc call on the
+ * current device (the word lives in its scratch array). */
 int mhs_read_status(void* workspace, void* stream, int* bits);
 
 /* Host helper: the per-column gather plan of a continuous layout from its

@@ -54,6 +54,11 @@ constexpr double D_STAR_DISTANT = 40.0;
 constexpr double SERIES_U_OVER_RHO = 2.0;    // large-|u| edge series regime
 constexpr int SERIES_TERMS = 32;
 constexpr double SMALL_U_OVER_RHO = 0.5;     // small-|u| edge series regime
+// Squares of the two edge-regime thresholds (exact in binary), for the tests
+// on squared lengths; tied to the thresholds by a static_assert in the
+// device build (pipeline.cuh).
+constexpr double SERIES_U_OVER_RHO_SQ = 4.0;
+constexpr double SMALL_U_OVER_RHO_SQ = 0.25;
 constexpr double DEGENERATE_AREA_REL = 1e-14;
 constexpr double IMAGE_Q_BUDGET_C = 10.0;    // Q-family Gauss order law
 constexpr int IMAGE_Q_GAUSS_MIN = 8;

@@ -294,7 +294,7 @@ MHS_FI int edge_regime_sq(double ua, double ub, double rho2) {
   const double a2 = ua * ua, b2 = ub * ub;
   const double umax2 = a2 > b2 ? a2 : b2;
   const double umin2 = a2 < b2 ? a2 : b2;
-  const double s2 = 0.25, l2 = 4.0;   // SMALL_U_OVER_RHO^2, SERIES_U_OVER_RHO^2 (exact)
+  const double s2 = cst::SMALL_U_OVER_RHO_SQ, l2 = cst::SERIES_U_OVER_RHO_SQ;
   if (umax2 <= s2 * rho2) return EDGE_SMALL;
   if (ua * ub > 0.0 && umin2 >= l2 * rho2) return EDGE_LARGE;
   return EDGE_CLOSED;

@@ -31,6 +31,7 @@ from __future__ import annotations
 
 import ast
 import pathlib
+import os
 import sys
 from fractions import Fraction
 
@@ -182,6 +183,17 @@ def main(src: str) -> None:
           f"Q {len(qmono)} monomials")
 
 
+def _table_path() -> str:
+    """mhs/kernels/_image_table.py of the reference tree: the first argument,
+    else under $MHS_REFERENCE_SRC (the reference's src/ directory)."""
+    if len(sys.argv) > 1:
+        return sys.argv[1]
+    root = os.environ.get("MHS_REFERENCE_SRC")
+    if not root:
+        sys.exit("usage: gen_tables.py <mhs/kernels/_image_table.py> "
+                 "(or set MHS_REFERENCE_SRC to the reference's src/ directory)")
+    return os.path.join(root, "mhs", "kernels", "_image_table.py")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else
-         "/root/reference/src/mhs/kernels/_image_table.py")
+    main(_table_path())

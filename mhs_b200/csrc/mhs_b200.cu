@@ -1,979 +1,27 @@
-// CUDA kernels and C ABI of the B200 Green's-function assembler.
-//
-// One request runs as a short pipeline on the caller's stream, per chunk of
-// observers:
-//   k_coef   per-material image coefficients (once per request)
-//   k_prep   per-source frames, reflected frames, basis products, fold data
-//   k_pair   one thread per (observer, source): direct term + image R-family,
-//            per-source quadrature rules staged in shared memory
-//   k_imageq one thread per (observer, source): image Q-family
-//   k_band   per straddling source, the ordered list of band receivers
-//   k_fold   one warp per band pair: mirror element + Boussinesq surface
-//            quadrature over the receiver's polar grid, 32 nodes per step
-//   k_final  one thread per (observer, output column): eigenstress,
-//            traction / interaction contraction, continuous-layout gather,
-//            and the store in the caller's layout
-// Per-pair tensors travel between stages in an element-major scratch table
-// (workspace), so every stage writes disjoint rows and no result depends on
-// atomics or scheduling order.
+// Host unit of the B200 Green's-function assembler: the C ABI
+// (include/mhs_b200.h), request checks, the per-device tables, stage
+// timing, the fold census counters and the allocation-free scratch array.
+// The kernels live in the kernel units (unit.cu, one per order / readout /
+// precision); this unit dispatches to them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
-#include <type_traits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <vector>
 
-#include "../../include/mhs_b200.h"
-#include "engine_fold.cuh"
 #include "host_prep.h"
+#include "pipeline.cuh"
 
 using namespace mhs;
+using namespace mhs::pipe;
 
-namespace {
+namespace mhs {
+namespace pipe {
 
-// ------------------------------------------------------------ device data
-__device__ double d_glx[GL_TABLE];
-__device__ double d_glw[GL_TABLE];
-
-struct SrcPrep {
-  Frame f;        // element
-  Frame fi;       // reflected element (image R-family and fold mirror)
-  double eps;
-  double centre[2], r_f, diam;
-  int straddle;   // folded (fold requested and the source reaches the band)
-  int pad;
-};
-
-constexpr int TB = 128;          // threads per block for pair-parallel kernels
-constexpr int FOLD_WARPS = 4;    // band pairs per fold block (one source)
-constexpr int QFLOOR = cst::IMAGE_Q_GAUSS_MIN;
-
-enum : int { KD_DISP = 0, KD_HE = 1, KD_E = 2 };   // what the stages compute
-
-MHS_FI constexpr int kind_class(int kind) {
-  return kind == MHS_DISP ? KD_DISP : (kind == MHS_EIGENSTRESS ? KD_E : KD_HE);
-}
-MHS_FI constexpr int comps_of(int kc) { return kc == KD_DISP ? 9 : (kc == KD_HE ? 27 : 0); }
-// Scratch row per (observer, source, node): tensor comps, phi, phi_mirror.
-MHS_FI constexpr int row_of(int kc) { return comps_of(kc) + 2; }
-
-// --------------------------------------------------------------- helpers
-__device__ __forceinline__ void atomic_status(int* st, int bits) { atomicOr(st, bits); }
-
-// One node of the collapsed Gauss product rule of order n (q = i * n + j).
-template <int P>
-__device__ __forceinline__ void rule_node(const Frame& f, int n, int q, double& e0, double& e1,
-                                          double& wq, double* N) {
-  const double* x = d_glx + gl_offset(n);
-  const double* w = d_glw + gl_offset(n);
-  const int i = q / n, j = q % n;
-  const double gi = 0.5 * (x[i] + 1.0), wi = 0.5 * w[i];
-  const double gj = 0.5 * (x[j] + 1.0), wj = 0.5 * w[j];
-  const double x1 = gi, x2 = gj * (1.0 - gi);
-  const double ww = wi * wj * (1.0 - gi);
-  const double l0 = 1.0 - x1 - x2;
-  e0 = (l0 * f.p[0][0] + x1 * f.p[1][0]) + x2 * f.p[2][0];
-  e1 = (l0 * f.p[0][1] + x1 * f.p[1][1]) + x2 * f.p[2][1];
-  wq = ww * (2.0 * f.area);
-  shape_at<P>(f, e0, e1, N);
-}
-
-// Shared-memory far-field rules of one frame (orders 12 and 8).
-template <int P>
-struct SmemRules {
-  static constexpr int K = n_nodes(P);
-  static constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
-  static constexpr int N8 = cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
-  double e0[N12 + N8], e1[N12 + N8], wq[N12 + N8], Nq[(N12 + N8) * K];
-  __device__ void build(const Frame& f, int tid, int nthr) {
-    for (int t = tid; t < N12 + N8; t += nthr) {
-      const int n = t < N12 ? cst::FAR_GAUSS_N : cst::FAR_GAUSS_N_DISTANT;
-      const int q = t < N12 ? t : t - N12;
-      rule_node<P>(f, n, q, e0[t], e1[t], wq[t], Nq + t * K);
-    }
-  }
-  __device__ QuadRule r12() const { return QuadRule{N12, e0, e1, wq, Nq}; }
-  __device__ QuadRule r8() const { return QuadRule{N8, e0 + N12, e1 + N12, wq + N12, Nq + N12 * K}; }
-};
-
-// Float copies of the element's far rules for the mixed form.
-template <int P>
-struct FloatRules {
-  static constexpr int N = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N +
-                           cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
-  float e0[N], e1[N], wq[N], Nq[N * n_nodes(P)];
-};
-struct NoRules {};
-
-// Float copies of a block's rules (the mixed form), as QuadRuleT<float>.
-template <int P>
-__device__ void float_rules(const SmemRules<P>& rd, FloatRules<P>& fr, int tid, int nthr) {
-  constexpr int N = FloatRules<P>::N, K = n_nodes(P);
-  for (int t = tid; t < N; t += nthr) {
-    fr.e0[t] = (float)rd.e0[t];
-    fr.e1[t] = (float)rd.e1[t];
-    fr.wq[t] = (float)rd.wq[t];
-  }
-  for (int t = tid; t < N * K; t += nthr) fr.Nq[t] = (float)rd.Nq[t];
-}
-template <int P>
-__device__ QuadRuleT<float> float_r12(const FloatRules<P>& fr) {
-  return QuadRuleT<float>{cst::FAR_GAUSS_N * cst::FAR_GAUSS_N, fr.e0, fr.e1, fr.wq, fr.Nq};
-}
-template <int P>
-__device__ QuadRuleT<float> float_r8(const FloatRules<P>& fr) {
-  constexpr int O = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
-  return QuadRuleT<float>{cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT, fr.e0 + O, fr.e1 + O,
-                          fr.wq + O, fr.Nq + O * n_nodes(P)};
-}
-
-// ---------------------------------------------------------------- k_coef
-__global__ void k_coef(double mu, double lam, double* out) {
-  const Material m = make_material(mu, lam);
-  const double nu = m.nu_i, s = m.scale_c;
-  const double nup[3] = {1.0, nu, nu * nu};
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  double* r_dg = out;
-  double* r_ddg = r_dg + 3 * MHS_R_NDG;
-  double* q_dg = r_ddg + 3 * MHS_R_NDDG;
-  double* q_ddg = q_dg + MHS_Q_NDG;
-  if (t < MHS_R_NDG)
-    for (int pz = 0; pz < 3; ++pz) {
-      double v = 0.0;
-      for (int k = 0; k < 3; ++k) v += tab_d::mhs_r_dg_c[t][pz][k] * nup[k];
-      r_dg[3 * t + pz] = v * s;
-    }
-  if (t < MHS_R_NDDG)
-    for (int pz = 0; pz < 3; ++pz) {
-      double v = 0.0;
-      for (int k = 0; k < 3; ++k) v += tab_d::mhs_r_ddg_c[t][pz][k] * nup[k];
-      r_ddg[3 * t + pz] = v * s;
-    }
-  if (t < MHS_Q_NDG) {
-    double v = 0.0;
-    for (int k = 0; k < 3; ++k) v += tab_d::mhs_q_dg_c[t][k] * nup[k];
-    q_dg[t] = v;
-  }
-  if (t < MHS_Q_NDDG) {
-    double v = 0.0;
-    for (int k = 0; k < 3; ++k) v += tab_d::mhs_q_ddg_c[t][k] * nup[k];
-    q_ddg[t] = v;
-  }
-}
-
-// ---------------------------------------------------------------- k_prep
-__global__ void k_prep(int64_t n_src, const double* __restrict__ tris,
-                       const double* __restrict__ eps, int fold, int want_g,
-                       SrcPrep* __restrict__ prep, double* __restrict__ G) {
-  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (s >= n_src) return;
-  SrcPrep p;
-  const double* t = tris + 9 * s;
-  double ti[9];
-  for (int i = 0; i < 9; ++i) ti[i] = (i % 3 == 2) ? -t[i] : t[i];
-  make_frame(t, p.f);
-  make_frame(ti, p.fi);
-  p.eps = eps[s];
-  fold_crease(t, p.eps, p.centre, &p.r_f);
-  p.diam = tri_diameter(t);
-  p.straddle = (fold && fold_straddles(t, p.eps)) ? 1 : 0;
-  p.pad = 0;
-  prep[s] = p;
-  if (want_g) build_basis_products(p.fi, G + s * G_SIZE);
-}
-
-// ---------------------------------------------------------------- k_pair
-// Direct term and image R-family of one (observer, source) pair.
-// RF: arithmetic type of the far-field quadrature (double; float in the
-// mixed form).
-template <int P, int KC, class RF>
-__global__ void __launch_bounds__(TB)
-k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
-       const SrcPrep* __restrict__ prep, const double* __restrict__ Gall,
-       const double* __restrict__ coef, double mu, double lam, double* __restrict__ T) {
-  constexpr int K = n_nodes(P);
-  constexpr int NR = row_of(KC);
-  constexpr bool IMG = KC != KD_E;
-  const int64_t s = blockIdx.y;
-  __shared__ SrcPrep sp;
-  __shared__ SmemRules<P> rd;
-  __shared__ SmemRules<IMG ? P : 0> ri;
-  __shared__ double sG[IMG ? G_SIZE : 1];
-  constexpr bool F32 = std::is_same<RF, float>::value;
-  __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rdf;
-  if (threadIdx.x == 0) sp = prep[s];
-  __syncthreads();
-  rd.build(sp.f, threadIdx.x, TB);
-  if (IMG) {
-    ri.build(sp.fi, threadIdx.x, TB);
-    for (int i = threadIdx.x; i < G_SIZE; i += TB) sG[i] = Gall[s * G_SIZE + i];
-  }
-  __syncthreads();
-  if constexpr (F32) {
-    float_rules<P>(rd, rdf, threadIdx.x, TB);
-    __syncthreads();
-  }
-  const int64_t oc = blockIdx.x * (int64_t)TB + threadIdx.x;
-  if (oc >= n_chunk) return;
-  const int64_t o = lo + oc;
-  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const Material m = make_material(mu, lam);
-  const double eps = sp.eps;
-  double* row = T + ((oc * n_src + s) * K) * NR;
-  if constexpr (KC == KD_E) {
-    double E[K] = {};
-    if constexpr (F32) direct_eval<P, W_E, RF>(sp.f, float_r12<P>(rdf), float_r8<P>(rdf), x, eps, m, nullptr, nullptr, E);
-    else direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
-    for (int k = 0; k < K; ++k) {
-      row[k * NR + 0] = E[k];
-      row[k * NR + 1] = 0.0;
-    }
-    return;
-  } else {
-    constexpr int C = comps_of(KC);
-    double A[K * C] = {}, E[K] = {};
-    if constexpr (F32) {
-      const QuadRuleT<float> f12 = float_r12<P>(rdf), f8 = float_r8<P>(rdf);
-      if constexpr (KC == KD_DISP)
-        direct_eval<P, W_U, RF>(sp.f, f12, f8, x, eps, m, A, nullptr, nullptr);
-      else
-        direct_eval<P, W_H | W_E, RF>(sp.f, f12, f8, x, eps, m, nullptr, A, E);
-    } else {
-      if constexpr (KC == KD_DISP)
-        direct_eval<P, W_U, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
-      else
-        direct_eval<P, W_H | W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
-    }
-    const bool band = sp.straddle && fold_band(x, sp.centre, eps);
-    if (!band) {
-      double B[K * C] = {};
-      const ImageCoef ic = image_coef_view(coef);
-      if constexpr (KC == KD_DISP)
-        image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
-      else
-        image_r_eval<P, W_H>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, nullptr, B);
-      for (int i = 0; i < K * C; ++i) A[i] += B[i];
-    }
-    for (int k = 0; k < K; ++k) {
-      for (int c = 0; c < C; ++c) row[k * NR + c] = A[k * C + c];
-      row[k * NR + C] = (KC == KD_HE) ? E[k] : 0.0;
-      row[k * NR + C + 1] = 0.0;
-    }
-  }
-}
-
-// -------------------------------------------------------------- k_imageq
-// Image Q-family of one pair, added to the scratch row.  The floor order
-// (8 x 8 points, almost every pair) reads a shared-memory rule; higher
-// orders generate their nodes on the fly.
-template <int P, class E = double>
-struct QRuleSmem {
-  static constexpr int K = n_nodes(P);
-  const E* y;
-  const E* wN;
-  int nq;
-  __device__ int count() const { return nq; }
-  __device__ void node(int t, E* yy, E* w) const {
-    yy[0] = y[3 * t];
-    yy[1] = y[3 * t + 1];
-    yy[2] = y[3 * t + 2];
-    for (int k = 0; k < K; ++k) w[k] = wN[t * K + k];
-  }
-};
-
-template <int P>
-struct QRuleFly {
-  static constexpr int K = n_nodes(P);
-  const Frame* f;
-  int n;
-  __device__ int count() const { return n * n; }
-  __device__ void node(int t, double* yy, double* w) const {
-    double e0, e1, wq, N[K];
-    rule_node<P>(*f, n, t, e0, e1, wq, N);
-    // Cartesian node on the real element: barycentric (l0, x1, x2) @ tri
-    const double* x = d_glx + gl_offset(n);
-    const int i = t / n, j = t % n;
-    const double gi = 0.5 * (x[i] + 1.0), gj = 0.5 * (x[j] + 1.0);
-    const double x1 = gi, x2 = gj * (1.0 - gi), l0 = 1.0 - x1 - x2;
-    for (int c = 0; c < 3; ++c) yy[c] = (l0 * f->v[0][c] + x1 * f->v[1][c]) + x2 * f->v[2][c];
-    for (int k = 0; k < K; ++k) w[k] = wq * N[k];
-  }
-};
-
-// RF = float (the mixed form): pairs at the floor order -- at least about an
-// element from the image triangle -- sum their points in float.
-template <int P, int KC, class RF>
-__global__ void __launch_bounds__(TB)
-k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
-         const SrcPrep* __restrict__ prep, const double* __restrict__ coef, double mu, double lam,
-         double* __restrict__ T) {
-  constexpr int K = n_nodes(P);
-  constexpr int NR = row_of(KC);
-  constexpr int C = comps_of(KC);
-  const int64_t s = blockIdx.y;
-  __shared__ SrcPrep sp;
-  __shared__ double qy[QFLOOR * QFLOOR * 3];
-  __shared__ double qw[QFLOOR * QFLOOR * K];
-  constexpr bool F32 = std::is_same<RF, float>::value;
-  __shared__ float qyf[F32 ? QFLOOR * QFLOOR * 3 : 1];
-  __shared__ float qwf[F32 ? QFLOOR * QFLOOR * K : 1];
-  if (threadIdx.x == 0) sp = prep[s];
-  __syncthreads();
-  {
-    QRuleFly<P> fly{&sp.f, QFLOOR};
-    for (int t = threadIdx.x; t < QFLOOR * QFLOOR; t += TB) fly.node(t, qy + 3 * t, qw + K * t);
-  }
-  __syncthreads();
-  if constexpr (F32) {
-    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * 3; t += TB) qyf[t] = (float)qy[t];
-    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * K; t += TB) qwf[t] = (float)qw[t];
-    __syncthreads();
-  }
-  const int64_t oc = blockIdx.x * (int64_t)TB + threadIdx.x;
-  if (oc >= n_chunk) return;
-  const int64_t o = lo + oc;
-  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const double eps = sp.eps;
-  if (sp.straddle && fold_band(x, sp.centre, eps)) return;
-  const Material m = make_material(mu, lam);
-  const ImageCoef ic = image_coef_view(coef);
-  double ti[9];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) ti[3 * i + j] = sp.fi.v[i][j];
-  const int n = q_gauss_order(x, ti, eps, sp.f.L, P);
-  double B[K * C] = {};
-  constexpr int WANT = KC == KD_DISP ? W_U : W_H;
-  bool done = false;
-  if constexpr (F32) {
-    if (n == QFLOOR) {
-      QRuleSmem<P, float> r{qyf, qwf, QFLOOR * QFLOOR};
-      image_q_eval<P, WANT, QRuleSmem<P, float>, float>(r, sp.f.n, x, eps, m, ic, B, B);
-      done = true;
-    }
-  }
-  if (done) {
-  } else if (n == QFLOOR) {
-    QRuleSmem<P> r{qy, qw, QFLOOR * QFLOOR};
-    image_q_eval<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
-  } else {
-    QRuleFly<P> r{&sp.f, n};
-    image_q_eval<P, WANT>(r, sp.f.n, x, eps, m, ic, B, B);
-  }
-  double* row = T + ((oc * n_src + s) * K) * NR;
-  for (int k = 0; k < K; ++k)
-    for (int c = 0; c < C; ++c) row[k * NR + c] += B[k * C + c];
-}
-
-// ---------------------------------------------------------------- k_band
-// Ordered list of the band receivers of each straddling source, in slots
-// [s * n_chunk, s * n_chunk + cnt[s]).
-__global__ void __launch_bounds__(256)
-k_band(int64_t lo, int64_t n_chunk, const double* __restrict__ obs,
-       const SrcPrep* __restrict__ prep, int* __restrict__ cnt, int* __restrict__ list) {
-  const int64_t s = blockIdx.x;
-  __shared__ int warp_n[8];
-  __shared__ int base;
-  const SrcPrep& p = prep[s];
-  if (!p.straddle) {
-    if (threadIdx.x == 0) cnt[s] = 0;
-    return;
-  }
-  if (threadIdx.x == 0) base = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int64_t t0 = 0; t0 < n_chunk; t0 += 256) {
-    const int64_t oc = t0 + threadIdx.x;
-    bool pred = false;
-    if (oc < n_chunk) {
-      const double x[3] = {obs[3 * (lo + oc)], obs[3 * (lo + oc) + 1], obs[3 * (lo + oc) + 2]};
-      pred = fold_band(x, p.centre, p.eps);
-    }
-    const unsigned bal = __ballot_sync(0xffffffffu, pred);
-    if (lane == 0) warp_n[wid] = __popc(bal);
-    __syncthreads();
-    int off = base;
-    for (int w = 0; w < wid; ++w) off += warp_n[w];
-    if (pred) list[s * n_chunk + off + __popc(bal & ((1u << lane) - 1u))] = (int)oc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int tot = 0;
-      for (int w = 0; w < 8; ++w) tot += warp_n[w];
-      base += tot;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) cnt[s] = base;
-}
-
-// ---------------------------------------------------------------- k_fold
-// Work census (measurement only): pairs, panels, nodes per class, near
-// edges per form; counted when the kernel is given a non-null pointer.
-__device__ unsigned long long g_census[MHS_CENSUS_N];
-std::atomic<int> g_census_on{0};
-
-// Grid nodes are processed in pages of FOLD_PAGE.  Each page is split by
-// surface-load class (closed form, 12 x 12 rule, 8 x 8 rule) and every
-// 32-node batch of one class runs one code path; the edges of a batch of
-// near nodes are sorted again by edge form (closed, small-|u| series,
-// large-|u| series) before their integrals are taken.  The weighted
-// point-load products are then summed in grid order, 32 nodes at a time.
-constexpr int FOLD_PAGE = 128;
-
-// Packed size of one edge's integrals P[j][0..edge[j]].
-MHS_FI constexpr int edge_pack_size(const Spec& sp) {
-  int o = 0;
-  for (int j = 0; j < MS; ++j) o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
-  return o;
-}
-
-template <int P, int KC>
-struct FoldWarp {
-  static constexpr int K = n_nodes(P);
-  static constexpr int NC = KC == KD_HE ? 6 : 3;
-  static constexpr int NJ = 3 * K;
-  static constexpr int NP = edge_pack_size(SurfaceSpec<P>::spec);
-  double px[FOLD_PAGE], py[FOLD_PAGE], wt[FOLD_PAGE];
-  double sS[FOLD_PAGE][NJ + 1];      // load minus the load at the foot
-  union {
-    struct {
-      double eu[96][3];              // (ua, ub, rho2) of one near batch's edges (node * 3 + e)
-      double eP[96][NP];             // their packed integrals
-    } edge;
-    double sB[32][NC + 1];           // weighted point-load tensor (after the loads)
-  };
-  unsigned char list[3][FOLD_PAGE];  // page nodes per class
-  unsigned char elist[3][96];        // batch edges per form
-  double brk[FOLD_MAX_BREAKS];
-  double sh_load[NJ];
-  double outv[NC * NJ];
-  double R1;
-  int nbrk;
-};
-
-template <int P, int KC, class RF>
-struct FoldShared {
-  SrcPrep sp;
-  SmemRules<P> rd;       // element (surface load)
-  SurfaceLoadConsts slc; // sigma_zz row of the element's H, per slip component
-  std::conditional_t<std::is_same<RF, float>::value, FloatRules<P>, NoRules> fr;
-  FoldWarp<P, KC> w[FOLD_WARPS];
-};
-
-// Append `val` to `list` for every lane where pred holds, in lane order.
-__device__ __forceinline__ void warp_append(bool pred, int val, unsigned char* list, int& count,
-                                            int lane) {
-  const unsigned mask = __ballot_sync(0xffffffffu, pred);
-  if (pred) list[count + __popc(mask & ((1u << lane) - 1u))] = (unsigned char)val;
-  count += __popc(mask);
-}
-
-// Surface loads of the near nodes list[0..n) of a page into W.sS.
-template <int P, int KC>
-__device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const SurfaceLoadConsts& c,
-                                double eps, int n, int lane, unsigned long long* census) {
-  using S = SurfaceSpec<P>;
-  constexpr Spec sp = S::spec;
-  constexpr int K = n_nodes(P);
-  constexpr int NJ = 3 * K;
-  constexpr int NB = sp.b_off[MS] > 0 ? sp.b_off[MS] : 1;
-  for (int b = 0; b < n; b += 32) {
-    const int i = b + lane;
-    const bool active = i < n;
-    const int u = active ? W.list[SL_NEAR][i] : 0;
-    double z = 0.0, X0 = 0.0, X1 = 0.0, h2 = 1.0;
-    double pr[3][2] = {};
-    int cnt[3] = {0, 0, 0};
-    if (active) {
-      const double x[3] = {W.px[u], W.py[u], 0.0};
-      to_plane(f, x, z, X0, X1);
-      h2 = z * z + eps * eps;
-      foot_vertices(f, X0, X1, pr);
-    }
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-      int form = -1;
-      if (active) {
-        const EdgeGeom g = edge_geom_rcp(pr, e, h2);
-        W.edge.eu[3 * lane + e][0] = g.ua;
-        W.edge.eu[3 * lane + e][1] = g.ub;
-        W.edge.eu[3 * lane + e][2] = g.rho2;
-        form = edge_regime_sq(g.ua, g.ub, g.rho2);
-      }
-#pragma unroll
-      for (int r = 0; r < 3; ++r) warp_append(form == r, 3 * lane + e, W.elist[r], cnt[r], lane);
-    }
-    if (census && lane == 0)
-      for (int r = 0; r < 3; ++r)
-        atomicAdd(census + MHS_CENSUS_EDGE_CLOSED + r, (unsigned long long)cnt[r]);
-    __syncwarp();
-    // edge integrals, one form per pass
-#pragma unroll 1
-    for (int r = 0; r < 3; ++r) {
-      for (int q = 0; q < cnt[r]; q += 32) {
-        if (q + lane < cnt[r]) {
-          const int slot = W.elist[r][q + lane];
-          const double ua = W.edge.eu[slot][0], ub = W.edge.eu[slot][1], rho2 = W.edge.eu[slot][2];
-          double Pt[MS][8];
-          if (r == EDGE_CLOSED) edge_closed<S, true>(ua, ub, rho2, Pt);
-          else if (r == EDGE_SMALL) edge_small<S>(ua, ub, sqrt(rho2), Pt);
-          else edge_large<S>(ua, ub, rho2, Pt);
-          int o = 0;
-#pragma unroll
-          for (int j = 0; j < MS; ++j) {
-#pragma unroll
-            for (int k = 0; k <= sp.edge[j]; ++k) W.edge.eP[slot][o + k] = Pt[j][k];
-            o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
-          }
-        }
-      }
-    }
-    __syncwarp();
-    if (active) {
-      double BN1[NB], BN2[NB], BD[MS];
-#pragma unroll
-      for (int t = 0; t < NB; ++t) {
-        BN1[t] = 0.0;
-        BN2[t] = 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < MS; ++j) BD[j] = 0.0;
-#pragma unroll 1
-      for (int e = 0; e < 3; ++e) {
-        const int slot = 3 * lane + e;
-        const EdgeGeom g = edge_geom_rcp(pr, e, h2);   // as in the pass above
-        double Pt[MS][8] = {};
-        int o = 0;
-#pragma unroll
-        for (int j = 0; j < MS; ++j) {
-#pragma unroll
-          for (int k = 0; k <= sp.edge[j]; ++k) Pt[j][k] = W.edge.eP[slot][o + k];
-          o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
-        }
-        edge_accumulate<S>(g, Pt, BN1, BN2, BD);
-      }
-      MomentTable<S> T;
-      closed_finish_t<S, true>(pr, h2, BN1, BN2, BD, T);
-      double sl[NJ] = {};
-      surface_load_near<P>(f, T, c, z, X0, X1, sl);
-#pragma unroll
-      for (int jj = 0; jj < NJ; ++jj) W.sS[u][jj] = sl[jj] - W.sh_load[jj];
-    }
-    __syncwarp();
-  }
-}
-
-// One warp per band pair.
-template <int P, int KC, class RF>
-__global__ void __launch_bounds__(32 * FOLD_WARPS)
-k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
-       const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
-       const int* __restrict__ list, double mu, double lam, double* __restrict__ T,
-       int* __restrict__ status, unsigned long long* __restrict__ census) {
-  constexpr int K = n_nodes(P);
-  constexpr int NR = row_of(KC);
-  constexpr int C = comps_of(KC);
-  constexpr bool WH = KC == KD_HE;
-  constexpr int NC = WH ? 6 : 3;          // point-load components
-  constexpr int NJ = 3 * K;               // load components (node x slip)
-  constexpr int NOUT = NC * NJ;
-  constexpr int PER_LANE = (NOUT + 31) / 32;
-  const int64_t s = blockIdx.y;
-  const int n_band = cnt[s];
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if ((int64_t)blockIdx.x * FOLD_WARPS >= n_band) return;
-  extern __shared__ __align__(16) unsigned char fold_smem[];
-  FoldShared<P, KC, RF>& sh = *reinterpret_cast<FoldShared<P, KC, RF>*>(fold_smem);
-  SrcPrep& sp = sh.sp;
-  SmemRules<P>& rd = sh.rd;
-  FoldWarp<P, KC>& W = sh.w[wid];
-  const Material m = make_material(mu, lam);
-  if (threadIdx.x == 0) sp = prep[s];
-  __syncthreads();
-  rd.build(sp.f, threadIdx.x, 32 * FOLD_WARPS);
-  {
-    static_assert(NLIFT <= 32 * FOLD_WARPS, "one thread per lifted slot");
-    if (threadIdx.x < NLIFT) {
-      double col[3] = {};
-      szz_coefficient(sp.f, sp.eps, m, threadIdx.x, col);
-      for (int j = 0; j < 3; ++j) sh.slc.coef[j][threadIdx.x] = col[j];
-    }
-    if (threadIdx.x == 32) surface_load_ezz(sp.f, sp.eps, m, sh.slc);
-  }
-  __syncthreads();
-  if constexpr (std::is_same<RF, float>::value) {
-    float_rules<P>(rd, sh.fr, threadIdx.x, 32 * FOLD_WARPS);
-    __syncthreads();
-  }
-  const int bi = blockIdx.x * FOLD_WARPS + wid;
-  if (bi >= n_band) return;
-  const int64_t oc = list[s * n_chunk + bi];
-  const int64_t o = lo + oc;
-  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const double eps = sp.eps;
-  double* row = T + ((oc * n_src + s) * K) * NR;
-  const QuadRule r12 = rd.r12(), r8 = rd.r8();
-  static_assert(KC != KD_E, "the eigen-only readout has no Boussinesq term");
-  {
-    const SurfaceLoadConsts& slc = sh.slc;
-    FoldPair fp;
-    fold_pair_setup(x, sp.centre, sp.r_f, eps, fp);
-    if (lane == 0) {
-      double R1;
-      W.nbrk = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, W.brk, &R1);
-      if (census) atomicAdd(census + MHS_CENSUS_PAIRS, 1ull);
-      W.R1 = R1;
-      double sl[NJ] = {};
-      fold_surface_load_fast<P, RF>(sp.f, r12, r8, slc, x[0], x[1], eps, sl);
-      for (int j = 0; j < NJ; ++j) W.sh_load[j] = sl[j];
-    }
-    __syncwarp();
-    const int nb = W.nbrk;
-    if (nb < 0) {
-      if (lane == 0) atomic_status(status, MHS_DEV_FOLD_GRID_OVERFLOW);
-      return;
-    }
-    fp.R1 = W.R1;
-    const double* gx6 = d_glx + gl_offset(cst::FOLD_N_RADIAL);
-    const double* gw6 = d_glw + gl_offset(cst::FOLD_N_RADIAL);
-    const double* gx4 = d_glx + gl_offset(cst::FOLD_N_ANGULAR);
-    const double* gw4 = d_glw + gl_offset(cst::FOLD_N_ANGULAR);
-    double acc[PER_LANE];
-#pragma unroll
-    for (int i = 0; i < PER_LANE; ++i) acc[i] = 0.0;
-    for (int pi = 0; pi + 1 < nb; ++pi) {
-      const double ra = W.brk[pi], rb = W.brk[pi + 1];
-      if (rb - ra < 1e-9 * eps) continue;
-      AngRule A;
-      fold_panel_rule(fp, ra, rb, A);
-      if (A.n < 0) {  // uniform across the warp: every lane built the same rule
-        if (lane == 0) atomic_status(status, MHS_DEV_FOLD_GRID_OVERFLOW);
-        return;
-      }
-      const int npts = cst::FOLD_N_RADIAL * A.n;
-      if (census && lane == 0) atomicAdd(census + MHS_CENSUS_PANELS, 1ull);
-      for (int p0 = 0; p0 < npts; p0 += FOLD_PAGE) {
-        const int np = min(FOLD_PAGE, npts - p0);
-        // nodes of the page and their classes
-        int ncls[3] = {0, 0, 0};
-#pragma unroll
-        for (int r = 0; r < FOLD_PAGE / 32; ++r) {
-          const int u = 32 * r + lane;
-          int cls = -1;
-          if (u < np) {
-            const int t = p0 + u;
-            const int ir = t / A.n, j = t % A.n;
-            const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
-            const double wr = (rb - ra) * (0.5 * gw6[ir]);
-            double th, wt;
-            fold_ang_node(A, gx4, gw4, j, &th, &wt);
-            double sn, cs;
-            sincos(th, &sn, &cs);
-            const double px = fp.xh0 + R * cs, py = fp.xh1 + R * sn;
-            W.px[u] = px;
-            W.py[u] = py;
-            W.wt[u] = wr * wt * R;
-            cls = surface_class(sp.f, px, py, eps);
-          }
-#pragma unroll
-          for (int c = 0; c < 3; ++c) warp_append(cls == c, u, W.list[c], ncls[c], lane);
-        }
-        if (census && lane == 0)
-          for (int c = 0; c < 3; ++c)
-            atomicAdd(census + MHS_CENSUS_NEAR + c, (unsigned long long)ncls[c]);
-        __syncwarp();
-        // far loads
-#pragma unroll 1
-        for (int c = SL_FAR12; c <= SL_FAR8; ++c) {
-          constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
-          const QuadRule& qd = c == SL_FAR8 ? r8 : r12;
-          QuadRuleT<RF> q;
-          if constexpr (std::is_same<RF, float>::value) {
-            const int off = c == SL_FAR8 ? N12 : 0;
-            q = QuadRuleT<float>{qd.nq, sh.fr.e0 + off, sh.fr.e1 + off, sh.fr.wq + off,
-                                 sh.fr.Nq + off * K};
-          } else {
-            q = qd;
-          }
-          for (int b = 0; b < ncls[c]; b += 32) {
-            if (b + lane < ncls[c]) {
-              const int u = W.list[c][b + lane];
-              const double xx[3] = {W.px[u], W.py[u], 0.0};
-              double z, X0, X1;
-              to_plane(sp.f, xx, z, X0, X1);
-              double sl[NJ] = {};
-              surface_load_far<P, RF>(q, slc, z, X0, X1, z * z + eps * eps, sl);
-#pragma unroll
-              for (int jj = 0; jj < NJ; ++jj) W.sS[u][jj] = sl[jj] - W.sh_load[jj];
-            }
-          }
-        }
-        // near loads
-        fold_near_batch<P, KC>(W, sp.f, slc, eps, ncls[SL_NEAR], lane, census);
-        __syncwarp();
-        // weighted point loads and the ordered sum, 32 nodes at a time
-        for (int c0 = 0; c0 < np; c0 += 32) {
-          const int u = c0 + lane;
-          if (u < np) {
-            const double px = W.px[u], py = W.py[u], w = W.wt[u];
-            double Bv[NC] = {};
-            if (WH) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, Bv);
-            else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, Bv);
-            for (int c = 0; c < NC; ++c) W.sB[lane][c] = w * Bv[c];
-          }
-          __syncwarp();
-          const int nvalid = min(32, np - c0);
-#pragma unroll
-          for (int i = 0; i < PER_LANE; ++i) {
-            const int oi = lane + 32 * i;
-            if (oi < NOUT) {
-              const int c = oi / NJ, jj = oi % NJ;
-              double a = acc[i];
-              for (int v = 0; v < nvalid; ++v) a += W.sB[v][c] * W.sS[c0 + v][jj];
-              acc[i] = a;
-            }
-          }
-          __syncwarp();
-        }
-      }
-    }
-    // gather the lane partials into the scratch row
-#pragma unroll
-    for (int i = 0; i < PER_LANE; ++i) {
-      const int oi = lane + 32 * i;
-      if (oi < NOUT) W.outv[oi] = acc[i];
-    }
-    __syncwarp();
-    if (lane == 0) {
-      if constexpr (WH) {
-        double srr, szz;
-        disk_stress(fp.R1, fp.zeta, m.nu_f, &srr, &szz);
-        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
-        for (int k = 0; k < K; ++k)
-          for (int mm = 0; mm < 3; ++mm) {
-            double Hb[3][3];
-            for (int c = 0; c < 6; ++c) {
-              const double v = W.outv[c * NJ + 3 * k + mm];
-              Hb[ia[c]][ib[c]] = v;
-              Hb[ib[c]][ia[c]] = v;
-            }
-            const double shv = W.sh_load[3 * k + mm];
-            Hb[0][0] += shv * srr;
-            Hb[1][1] += shv * srr;
-            Hb[2][2] += shv * szz;
-            for (int a = 0; a < 3; ++a)
-              for (int b = 0; b < 3; ++b) row[k * NR + 9 * a + 3 * b + mm] += Hb[a][b];
-          }
-      } else {
-        const double uz = disk_disp_z(fp.R1, fp.zeta, m.mu, m.nu_f);
-        for (int k = 0; k < K; ++k)
-          for (int mm = 0; mm < 3; ++mm)
-            for (int i = 0; i < 3; ++i)
-              row[k * NR + 3 * i + mm] += W.outv[i * NJ + 3 * k + mm] +
-                                          (i == 2 ? W.sh_load[3 * k + mm] * uz : 0.0);
-      }
-    }
-  }
-}
-
-// --------------------------------------------------------- k_fold_mirror
-// The mirror element of every band pair, one thread per pair: its
-// full-space field with the slip signs of the reflection (fold.py:334-350)
-// added to the pair's row, and its blob weight (the mirror eigenstress).
-template <int P, int KC, class RF>
-__global__ void __launch_bounds__(TB)
-k_fold_mirror(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
-              const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
-              const int* __restrict__ list, double mu, double lam, double* __restrict__ T) {
-  constexpr int K = n_nodes(P);
-  constexpr int NR = row_of(KC);
-  constexpr int C = comps_of(KC);
-  const int64_t s = blockIdx.y;
-  const int n_band = cnt[s];
-  if ((int64_t)blockIdx.x * TB >= n_band) return;
-  __shared__ SrcPrep sp;
-  __shared__ SmemRules<P> rm;
-  if (threadIdx.x == 0) sp = prep[s];
-  __syncthreads();
-  rm.build(sp.fi, threadIdx.x, TB);
-  __syncthreads();
-  const int bi = blockIdx.x * TB + threadIdx.x;
-  if (bi >= n_band) return;
-  const int64_t oc = list[s * n_chunk + bi];
-  const int64_t o = lo + oc;
-  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const Material m = make_material(mu, lam);
-  const double eps = sp.eps;
-  double* row = T + ((oc * n_src + s) * K) * NR;
-  double E[K] = {};
-  if constexpr (KC == KD_E) {
-    direct_eval<P, W_E, RF>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, nullptr, E);
-    for (int k = 0; k < K; ++k) row[k * NR + 1] = E[k];
-  } else if constexpr (KC == KD_HE) {
-    double Mv[K * 27] = {};
-    direct_eval<P, W_H | W_E, RF>(sp.fi, rm.r12(), rm.r8(), x, eps, m, nullptr, Mv, E);
-    for (int k = 0; k < K; ++k) {
-      for (int i = 0; i < 27; ++i) row[k * NR + i] += Mv[27 * k + i] * mirror_slip_sign(i % 3);
-      row[k * NR + C + 1] = E[k];
-    }
-  } else {
-    double Mv[K * 9] = {};
-    direct_eval<P, W_U, RF>(sp.fi, rm.r12(), rm.r8(), x, eps, m, Mv, nullptr, nullptr);
-    for (int k = 0; k < K; ++k)
-      for (int i = 0; i < 9; ++i) row[k * NR + i] += Mv[9 * k + i] * mirror_slip_sign(i % 3);
-  }
-}
-
-// --------------------------------------------------------------- k_final
-struct FinalArgs {
-  int kind, subtract, out_f32, n_a, n_b;
-  int64_t lo, n_chunk, n_src, n_obs, n_dof;
-  const double* normals;
-  const double* rec_basis;
-  const double* src_basis;
-  const int32_t* col_ptr;
-  const int32_t* col_ent;
-  double mu, lam;
-  void* out;
-};
-
-// Eigenstress C:sym(slip (x) n) of one row: phi C(n) + phi_m C(n_m) sign.
-__device__ __forceinline__ double eig_comp(const SrcPrep& p, double phi, double phim, double mu,
-                                           double lam, int a, int b, int m) {
-  const double* n = p.f.n;
-  const double* nm = p.fi.n;
-  const double c = (a == b ? lam * n[m] : 0.0) + mu * ((a == m ? n[b] : 0.0) + (b == m ? n[a] : 0.0));
-  const double cm = (a == b ? lam * nm[m] : 0.0) + mu * ((a == m ? nm[b] : 0.0) + (b == m ? nm[a] : 0.0));
-  return phi * c + phim * (cm * mirror_slip_sign(m));
-}
-
-template <class OUT>
-__device__ __forceinline__ void store(void* out, int64_t i, double v) {
-  reinterpret_cast<OUT*>(out)[i] = (OUT)v;
-}
-
-// Value of output component `comp` of one (observer, source, node) row.
-template <int KC>
-__device__ void row_values(const FinalArgs& a, const SrcPrep& p, const double* row, int64_t o,
-                           int64_t scol, double* v, int nv) {
-  constexpr int C = comps_of(KC);
-  const double phi = row[C], phim = row[C + 1];
-  const double mu = a.mu, lam = a.lam;
-  switch (a.kind) {
-    case MHS_DISP:
-      for (int i = 0; i < 9; ++i) v[i] = row[i];
-      break;
-    case MHS_TOTAL_STRESS:
-      for (int i = 0; i < 27; ++i) v[i] = row[i];
-      break;
-    case MHS_EIGENSTRESS:
-      for (int aa = 0; aa < 3; ++aa)
-        for (int b = 0; b < 3; ++b)
-          for (int m = 0; m < 3; ++m) v[9 * aa + 3 * b + m] = eig_comp(p, row[0], row[1], mu, lam, aa, b, m);
-      break;
-    case MHS_STRESS:
-    case MHS_STRAIN:
-      for (int aa = 0; aa < 3; ++aa)
-        for (int b = 0; b < 3; ++b)
-          for (int m = 0; m < 3; ++m) {
-            double s = row[9 * aa + 3 * b + m];
-            if (a.subtract) s -= eig_comp(p, phi, phim, mu, lam, aa, b, m);
-            v[9 * aa + 3 * b + m] = s;
-          }
-      if (a.kind == MHS_STRAIN)
-        for (int m = 0; m < 3; ++m) {
-          const double tr = v[m] + v[12 + m] + v[24 + m];
-          const double tre = tr / (3.0 * lam + 2.0 * mu);
-          for (int d = 0; d < 3; ++d) v[12 * d + m] -= lam * tre;
-          for (int i = 0; i < 9; ++i) v[3 * i + m] /= (2.0 * mu);
-        }
-      break;
-    default: {  // traction / interaction
-      const double* n = a.normals + 3 * o;
-      double t[3][3];
-      for (int i = 0; i < 3; ++i)
-        for (int m = 0; m < 3; ++m) {
-          double s = row[9 * i + 3 * 0 + m] * n[0] + row[9 * i + 3 * 1 + m] * n[1] + row[9 * i + 3 * 2 + m] * n[2];
-          if (a.subtract) {
-            double e = 0.0;
-            for (int j = 0; j < 3; ++j) e += eig_comp(p, phi, phim, mu, lam, i, j, m) * n[j];
-            s -= e;
-          }
-          t[i][m] = s;
-        }
-      if (a.kind == MHS_TRACTION) {
-        for (int i = 0; i < 3; ++i)
-          for (int m = 0; m < 3; ++m) v[3 * i + m] = t[i][m];
-      } else {
-        const double* rb = a.rec_basis + o * a.n_a * 3;
-        const double* sb = a.src_basis + scol * a.n_b * 3;
-        for (int ia = 0; ia < a.n_a; ++ia)
-          for (int ib = 0; ib < a.n_b; ++ib) {
-            double acc = 0.0;
-            for (int i = 0; i < 3; ++i)
-              for (int m = 0; m < 3; ++m) acc += rb[3 * ia + i] * t[i][m] * sb[3 * ib + m];
-            v[ia * a.n_b + ib] = acc;
-          }
-      }
-    }
-  }
-}
-
-template <int P, int KC, class OUT, bool CONT>
-__global__ void __launch_bounds__(TB)
-k_final(FinalArgs a, const SrcPrep* __restrict__ prep, const double* __restrict__ T) {
-  constexpr int K = n_nodes(P);
-  constexpr int NR = row_of(KC);
-  const int64_t col = blockIdx.x * (int64_t)TB + threadIdx.x;
-  const int64_t oc = blockIdx.y;
-  if (col >= a.n_dof) return;
-  const int64_t o = a.lo + oc;
-  int nv;
-  switch (a.kind) {
-    case MHS_DISP:
-    case MHS_TRACTION: nv = 9; break;
-    case MHS_INTERACTION: nv = a.n_a * a.n_b; break;
-    default: nv = 27;
-  }
-  double v[27];
-  if (!CONT) {
-    const int64_t s = col / K;
-    const double* row = T + (oc * a.n_src * K + col) * NR;
-    row_values<KC>(a, prep[s], row, o, s, v, nv);
-  } else {
-    for (int i = 0; i < nv; ++i) v[i] = 0.0;
-    for (int e = a.col_ptr[col]; e < a.col_ptr[col + 1]; ++e) {
-      const int ent = a.col_ent[e];
-      const int64_t s = ent / 6;
-      const double* row = T + (oc * a.n_src * K + ent) * NR;
-      double w[27];
-      row_values<KC>(a, prep[s], row, o, col, w, nv);
-      for (int i = 0; i < nv; ++i) v[i] += w[i];
-    }
-  }
-  // store in the caller's layout
-  switch (a.kind) {
-    case MHS_DISP:
-    case MHS_TRACTION:  // (N, 3, n_dof, 3)
-      for (int i = 0; i < 3; ++i)
-        for (int m = 0; m < 3; ++m)
-          store<OUT>(a.out, ((o * 3 + i) * a.n_dof + col) * 3 + m, v[3 * i + m]);
-      break;
-    case MHS_INTERACTION:  // (N, n_dof, n_a, n_b)
-      for (int i = 0; i < nv; ++i) store<OUT>(a.out, (o * a.n_dof + col) * nv + i, v[i]);
-      break;
-    default:  // (N, 3, 3, n_dof, 3)
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-          for (int m = 0; m < 3; ++m)
-            store<OUT>(a.out, (((o * 3 + i) * 3 + j) * a.n_dof + col) * 3 + m, v[9 * i + 3 * j + m]);
-  }
-}
-
-// ----------------------------------------------------------------- host
 thread_local char g_err[512] = "";
 
 int fail(int code, const char* fmt, ...) {
@@ -983,31 +31,6 @@ int fail(int code, const char* fmt, ...) {
   va_end(ap);
   return code;
 }
-
-#define CUDA_TRY(x)                                                            \
-  do {                                                                         \
-    cudaError_t e_ = (x);                                                      \
-    if (e_ != cudaSuccess) return fail(MHS_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
-  } while (0)
-
-std::mutex g_init_mu;
-std::vector<int> g_init_done;
-
-int ensure_device_tables() {
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lk(g_init_mu);
-  if ((int)g_init_done.size() <= dev) g_init_done.resize(dev + 1, 0);
-  if (g_init_done[dev]) return MHS_OK;
-  std::vector<double> x(GL_TABLE), w(GL_TABLE);
-  gauss_table(x.data(), w.data());
-  CUDA_TRY(cudaMemcpyToSymbol(d_glx, x.data(), sizeof(double) * GL_TABLE));
-  CUDA_TRY(cudaMemcpyToSymbol(d_glw, w.data(), sizeof(double) * GL_TABLE));
-  g_init_done[dev] = 1;
-  return MHS_OK;
-}
-
-size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
 // ------------------------------------------------------ stage timing
 // When enabled, each stage launch is bracketed by CUDA events on the
@@ -1020,29 +43,59 @@ std::mutex g_prof_mu;
 std::vector<ProfRec> g_prof;
 int g_prof_on = 0;
 
-struct StageTimer {
-  int stage;
-  cudaStream_t st;
-  cudaEvent_t a = nullptr, b = nullptr;
-  StageTimer(int s, cudaStream_t stream) : stage(s), st(stream) {
-    if (__atomic_load_n(&g_prof_on, __ATOMIC_RELAXED)) {
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      cudaEventRecord(a, st);
-    }
-  }
-  ~StageTimer() {
-    if (a) {
-      cudaEventRecord(b, st);
-      std::lock_guard<std::mutex> lk(g_prof_mu);
-      g_prof.push_back({stage, a, b});
-    }
-  }
+bool prof_enabled() { return __atomic_load_n(&g_prof_on, __ATOMIC_RELAXED) != 0; }
+
+void prof_record(int stage, cudaEvent_t a, cudaEvent_t b) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof.push_back({stage, a, b});
+}
+
+}  // namespace pipe
+}  // namespace mhs
+
+namespace {
+
+#define CUDA_TRY MHS_CUDA_TRY
+
+// ------------------------------------------------------ kernel units
+struct UnitEntry {
+  int P, KC, RF;
+  UnitInit init;
+  UnitRun run;
 };
+#define MHS_UNIT_ENTRY(P, KC, RF) {P, KC, RF, unit_init_##P##_##KC##_##RF, unit_run_##P##_##KC##_##RF},
+const UnitEntry g_units[] = {MHS_UNIT_LIST(MHS_UNIT_ENTRY)};
+#undef MHS_UNIT_ENTRY
+const UnitInit g_terms_init[3] = {unit_init_terms_0, unit_init_terms_1, unit_init_terms_2};
+const UnitTerms g_terms[3] = {unit_terms_0, unit_terms_1, unit_terms_2};
+
+std::mutex g_init_mu;
+std::vector<int> g_init_done;
+
+// Gauss-Legendre tables of every unit on the current device, once.
+int ensure_device_tables() {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if ((int)g_init_done.size() <= dev) g_init_done.resize(dev + 1, 0);
+  if (g_init_done[dev]) return MHS_OK;
+  std::vector<double> x(GL_TABLE), w(GL_TABLE);
+  gauss_table(x.data(), w.data());
+  for (const UnitEntry& u : g_units) {
+    const int rc = u.init(x.data(), w.data());
+    if (rc) return rc;
+  }
+  for (UnitInit f : g_terms_init) {
+    const int rc = f(x.data(), w.data());
+    if (rc) return rc;
+  }
+  g_init_done[dev] = 1;
+  return MHS_OK;
+}
 
 // Independent FMA chains: the FP64 (or FP32) issue ceiling of the device.
 template <class R>
-__global__ void k_fma_peak(R* out, int iters, R b, R c) {
+__device__ __forceinline__ void fma_chains(R* out, int iters, R b, R c) {
   R a0 = R(threadIdx.x) * R(1e-9), a1 = a0 + R(1e-9), a2 = a0 + R(2e-9), a3 = a0 + R(3e-9);
   R a4 = a0 + R(4e-9), a5 = a0 + R(5e-9), a6 = a0 + R(6e-9), a7 = a0 + R(7e-9);
   for (int i = 0; i < iters; ++i) {
@@ -1052,29 +105,11 @@ __global__ void k_fma_peak(R* out, int iters, R b, R c) {
   const R s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
   if (s == R(-1)) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
-
-struct Layout {
-  size_t status, coef, prep, G, cnt, list, T, total;
-  int64_t chunk;
-};
-
-// Workspace carve-up for a chunk of `chunk` observers.
-Layout plan(const mhs_request* r, int64_t chunk) {
-  const int kc = kind_class(r->kind);
-  const int K = n_nodes(r->order);
-  Layout L;
-  size_t off = 0;
-  L.status = off; off = align_up(off + 256);
-  L.coef = off; off = align_up(off + sizeof(double) * IMAGE_COEF_SIZE);
-  L.prep = off; off = align_up(off + sizeof(SrcPrep) * (size_t)r->n_src);
-  L.G = off;
-  if (kc != KD_E) off = align_up(off + sizeof(double) * G_SIZE * (size_t)r->n_src);
-  L.cnt = off; off = align_up(off + sizeof(int) * (size_t)r->n_src);
-  L.list = off; off = align_up(off + sizeof(int) * (size_t)r->n_src * (size_t)chunk);
-  L.T = off; off = align_up(off + sizeof(double) * (size_t)chunk * r->n_src * K * row_of(kc));
-  L.total = off;
-  L.chunk = chunk;
-  return L;
+__global__ void k_fma_peak_f64(double* out, int iters, double b, double c) {
+  fma_chains<double>(out, iters, b, c);
+}
+__global__ void k_fma_peak_f32(float* out, int iters, float b, float c) {
+  fma_chains<float>(out, iters, b, c);
 }
 
 int check_request(const mhs_request* r) {
@@ -1082,7 +117,7 @@ int check_request(const mhs_request* r) {
   if (r->kind < MHS_DISP || r->kind > MHS_INTERACTION) return fail(MHS_ERR_ARG, "bad kind %d", r->kind);
   if (r->order < 0 || r->order > 2) return fail(MHS_ERR_ARG, "order must be 0, 1 or 2");
   if (r->n_obs <= 0 || r->n_src <= 0) return fail(MHS_ERR_ARG, "empty request");
-  if (r->n_src > 65535) return fail(MHS_ERR_ARG, "n_src %lld above 65535", (long long)r->n_src);
+  if (r->n_src > INT32_MAX / 6) return fail(MHS_ERR_ARG, "n_src %lld above %d", (long long)r->n_src, INT32_MAX / 6);
   if (!r->obs || !r->tris || !r->eps || !r->out) return fail(MHS_ERR_ARG, "null array");
   if (!(r->mu > 0.0)) return fail(MHS_ERR_ARG, "mu must be positive");
   if ((r->kind == MHS_TRACTION || r->kind == MHS_INTERACTION) && !r->normals)
@@ -1096,104 +131,33 @@ int check_request(const mhs_request* r) {
   return MHS_OK;
 }
 
-template <int P, int KC, class RF>
-int run(const mhs_request* r, cudaStream_t st, const Layout& L) {
-  char* ws = (char*)r->workspace;
-  int* status = (int*)(ws + L.status);
-  double* coef = (double*)(ws + L.coef);
-  SrcPrep* prep = (SrcPrep*)(ws + L.prep);
-  double* G = (double*)(ws + L.G);
-  int* cnt = (int*)(ws + L.cnt);
-  int* list = (int*)(ws + L.list);
-  double* T = (double*)(ws + L.T);
-  constexpr int K = n_nodes(P);
-  CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
-  {
-    StageTimer t(MHS_STAGE_PREP, st);
-    k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(r->mu, r->lam, coef);
-    k_prep<<<(unsigned)((r->n_src + 127) / 128), 128, 0, st>>>(r->n_src, r->tris, r->eps, r->fold,
-                                                                KC != KD_E, prep, G);
-  }
-  const bool cont = r->ids != nullptr;
-  const int64_t n_dof = cont ? r->n_cols : r->n_src * K;
-  for (int64_t lo = 0; lo < r->n_obs; lo += L.chunk) {
-    const int64_t nc = std::min<int64_t>(L.chunk, r->n_obs - lo);
-    dim3 g((unsigned)((nc + TB - 1) / TB), (unsigned)r->n_src);
-    {
-      StageTimer t(MHS_STAGE_PAIR, st);
-      k_pair<P, KC, RF><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, G, coef, r->mu, r->lam, T);
-    }
-    if constexpr (KC != KD_E) {
-      StageTimer t(MHS_STAGE_IMAGEQ, st);
-      k_imageq<P, KC, RF><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, coef, r->mu, r->lam, T);
-    }
-    if (r->fold) {
-      StageTimer t(MHS_STAGE_FOLD, st);
-      k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
-      if constexpr (KC != KD_E) {
-        dim3 gf((unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS), (unsigned)r->n_src);
-        const size_t fsm = sizeof(FoldShared<P, KC, RF>);
-        CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)fsm));
-        unsigned long long* census = nullptr;
-        if (g_census_on.load(std::memory_order_relaxed))
-          CUDA_TRY(cudaGetSymbolAddress((void**)&census, g_census));
-        k_fold<P, KC, RF><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
-                                                        r->mu, r->lam, T, status, census);
-      }
-      dim3 gm((unsigned)((nc + TB - 1) / TB), (unsigned)r->n_src);
-      k_fold_mirror<P, KC, RF><<<gm, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list, r->mu,
-                                              r->lam, T);
-    }
-    StageTimer tfin(MHS_STAGE_FINAL, st);
-    FinalArgs a;
-    a.kind = r->kind;
-    a.subtract = r->subtract_eigenstress;
-    a.out_f32 = r->out_f32;
-    a.n_a = r->n_a;
-    a.n_b = r->n_b;
-    a.lo = lo;
-    a.n_chunk = nc;
-    a.n_src = r->n_src;
-    a.n_obs = r->n_obs;
-    a.n_dof = n_dof;
-    a.normals = r->normals;
-    a.rec_basis = r->rec_basis;
-    a.src_basis = r->src_basis;
-    a.col_ptr = r->col_ptr;
-    a.col_ent = r->col_ent;
-    a.mu = r->mu;
-    a.lam = r->lam;
-    a.out = r->out;
-    dim3 gfin((unsigned)((n_dof + TB - 1) / TB), (unsigned)nc);
-    if (r->out_f32) {
-      if (cont) k_final<P, KC, float, true><<<gfin, TB, 0, st>>>(a, prep, T);
-      else k_final<P, KC, float, false><<<gfin, TB, 0, st>>>(a, prep, T);
-    } else {
-      if (cont) k_final<P, KC, double, true><<<gfin, TB, 0, st>>>(a, prep, T);
-      else k_final<P, KC, double, false><<<gfin, TB, 0, st>>>(a, prep, T);
-    }
-  }
-  CUDA_TRY(cudaGetLastError());
-  return MHS_OK;
+// ------------------------------------------------------ fold census
+__device__ unsigned long long g_census[MHS_CENSUS_N];
+std::atomic<int> g_census_on{0};
+
+// Queue the request on the unit of its (order, readout, precision).
+int run_request(const mhs_request* r, cudaStream_t st, const Layout& L) {
+  const int kc = kind_class(r->kind);
+  const int rf = r->precision == MHS_MIXED ? 1 : 0;
+  unsigned long long* census = nullptr;
+  if (g_census_on.load(std::memory_order_relaxed))
+    CUDA_TRY(cudaGetSymbolAddress((void**)&census, g_census));
+  for (const UnitEntry& u : g_units)
+    if (u.P == r->order && u.KC == kc && u.RF == rf) return u.run(r, st, L, census);
+  return fail(MHS_ERR_ARG, "no kernel unit for order %d", r->order);
 }
 
-template <int P>
-int run_kind(const mhs_request* r, cudaStream_t st, const Layout& L) {
-  // mixed: far-field quadrature of the direct term, the fold's surface
-  // loads and its mirror, and the image Q-family points of pairs at the
-  // floor order, in float with float accumulation; near-field recursions,
-  // the image R-family, higher-order image Q and the eigenstress
-  // subtraction stay double
-  const bool mixed = r->precision == MHS_MIXED;
-  switch (kind_class(r->kind)) {
-    case KD_DISP:
-      return mixed ? run<P, KD_DISP, float>(r, st, L) : run<P, KD_DISP, double>(r, st, L);
-    case KD_HE:
-      return mixed ? run<P, KD_HE, float>(r, st, L) : run<P, KD_HE, double>(r, st, L);
-    default:
-      return mixed ? run<P, KD_E, float>(r, st, L) : run<P, KD_E, double>(r, st, L);
+// Largest observer chunk whose workspace fits `bytes` (plan() is monotone
+// in the chunk); 0 when not even one row fits.
+int64_t fit_chunk(const mhs_request* r, size_t bytes) {
+  if (plan(r, 1).total > bytes) return 0;
+  int64_t lo = 1, hi = std::min<int64_t>(r->n_obs, 65535);
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo + 1) / 2;
+    if (plan(r, mid).total <= bytes) lo = mid;
+    else hi = mid - 1;
   }
+  return lo;
 }
 
 constexpr size_t GOOD_T_BYTES = size_t(2) << 30;
@@ -1223,84 +187,6 @@ int noalloc_scratch(void** out) {
   return MHS_OK;
 }
 
-// ---------------------------------------------------- per-term diagnostics
-// One source, n observers, one thread per observer: a single influence term
-// exactly as the pipeline evaluates it.  term 0 direct (H + E or U), 1 image
-// R-family, 2 image Q-family, 3 folded image (mirror + Boussinesq); with
-// H, 4 and 5 the fold's surface load at (x, y, 0) (K x 3 values), from the
-// sigma_zz row and from the full H.
-// out per observer: K x C tensor values, then K blob weights (direct only).
-template <int P, int WANT>
-__global__ void k_terms(int term, int n, const double* __restrict__ obs,
-                        const double* __restrict__ tri, double mu, double lam, double eps,
-                        const double* __restrict__ coef, double* __restrict__ out) {
-  constexpr int K = n_nodes(P);
-  constexpr int C = (WANT & W_U) ? 9 : 27;
-  __shared__ Frame f, fi;
-  __shared__ SmemRules<P> rd, ri;
-  __shared__ double sG[G_SIZE];
-  if (threadIdx.x == 0) {
-    double ti[9];
-    for (int i = 0; i < 9; ++i) ti[i] = (i % 3 == 2) ? -tri[i] : tri[i];
-    make_frame(tri, f);
-    make_frame(ti, fi);
-    build_basis_products(fi, sG);
-  }
-  __syncthreads();
-  rd.build(f, threadIdx.x, blockDim.x);
-  ri.build(fi, threadIdx.x, blockDim.x);
-  __syncthreads();
-  const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= n) return;
-  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const Material m = make_material(mu, lam);
-  const ImageCoef ic = image_coef_view(coef);
-  double A[K * C] = {}, E[K] = {};
-  for (int k = 0; k < K; ++k) E[k] = 0.0;
-  if (term == 0) {
-    if (WANT & W_U) direct_eval<P, W_U>(f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
-    else direct_eval<P, W_H | W_E>(f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
-  } else if (term == 1) {
-    image_r_eval<P, WANT>(fi, sG, f.n, ri.r12(), ri.r8(), x, eps, m, ic, A, A);
-  } else if (term == 2) {
-    double ti[9];
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) ti[3 * i + j] = fi.v[i][j];
-    const int nq = q_gauss_order(x, ti, eps, f.L, P);
-    QRuleFly<P> r{&f, nq};
-    image_q_eval<P, WANT>(r, f.n, x, eps, m, ic, A, A);
-  } else if (term >= 4) {
-    if (!(WANT & W_U)) {
-      if (term == 4) {
-        SurfaceLoadConsts c;
-        surface_load_consts(f, eps, m, c);
-        fold_surface_load_fast<P>(f, rd.r12(), rd.r8(), c, x[0], x[1], eps, A);
-      } else {
-        fold_surface_load<P>(f, rd.r12(), rd.r8(), x[0], x[1], eps, m, A);
-      }
-    }
-  } else {
-    double Mv[K * C] = {}, Bq[K * C] = {};
-    if (WANT & W_U) direct_eval<P, W_U>(fi, ri.r12(), ri.r8(), x, eps, m, Mv, nullptr, nullptr);
-    else direct_eval<P, W_H>(fi, ri.r12(), ri.r8(), x, eps, m, nullptr, Mv, nullptr);
-    fold_boussinesq_scalar<P, !(WANT & W_U)>(f, rd.r12(), rd.r8(), tri, x, eps, m, d_glx, d_glw, Bq);
-    for (int i = 0; i < K * C; ++i) A[i] = Mv[i] * mirror_slip_sign(i % 3) + Bq[i];
-  }
-  for (int i = 0; i < K * C; ++i) out[o * (K * C + K) + i] = A[i];
-  for (int k = 0; k < K; ++k) out[o * (K * C + K) + K * C + k] = E[k];
-}
-
-template <int P>
-int debug_terms(int term, int want_u, int n, const double* obs, const double* tri, double mu,
-                double lam, double eps, double* coef, double* out, cudaStream_t st) {
-  k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(mu, lam, coef);
-  const int nb = (n + 63) / 64;
-  if (want_u) k_terms<P, W_U><<<nb, 64, 0, st>>>(term, n, obs, tri, mu, lam, eps, coef, out);
-  else k_terms<P, W_H><<<nb, 64, 0, st>>>(term, n, obs, tri, mu, lam, eps, coef, out);
-  CUDA_TRY(cudaGetLastError());
-  return MHS_OK;
-}
-
 }  // namespace
 
 extern "C" {
@@ -1326,23 +212,11 @@ int mhs_assemble(const mhs_request* req, void* stream) {
   rc = ensure_device_tables();
   if (rc) return rc;
   // largest chunk the workspace holds
-  const Layout one = plan(req, 1);
-  if (!req->workspace || req->workspace_bytes < one.total)
+  const int64_t chunk = req->workspace ? fit_chunk(req, req->workspace_bytes) : 0;
+  if (chunk == 0)
     return fail(MHS_ERR_WORKSPACE, "workspace %zu bytes, need at least %zu", req->workspace_bytes,
-                one.total);
-  int64_t lo = 1, hi = std::min<int64_t>(req->n_obs, 65535);
-  while (lo < hi) {  // plan() is monotone in chunk
-    const int64_t mid = lo + (hi - lo + 1) / 2;
-    if (plan(req, mid).total <= req->workspace_bytes) lo = mid;
-    else hi = mid - 1;
-  }
-  const Layout L = plan(req, lo);
-  cudaStream_t st = (cudaStream_t)stream;
-  switch (req->order) {
-    case 0: return run_kind<0>(req, st, L);
-    case 1: return run_kind<1>(req, st, L);
-    default: return run_kind<2>(req, st, L);
-  }
+                plan(req, 1).total);
+  return run_request(req, (cudaStream_t)stream, plan(req, chunk));
 }
 
 int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits) {
@@ -1354,29 +228,19 @@ int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits)
   rc = noalloc_scratch(&scratch);
   if (rc) return rc;
   const size_t cap = MHS_NOALLOC_SCRATCH_BYTES;
-  const Layout one = plan(req, 1);
-  if (one.total > cap)
+  const int64_t chunk = fit_chunk(req, cap);
+  if (chunk == 0)
     return fail(MHS_ERR_WORKSPACE,
                 "request needs %zu bytes of scratch for one observer row, above the %zu-byte "
                 "array of the allocation-free entry point (MHS_NOALLOC_SCRATCH_BYTES); pass "
                 "fewer sources per call or use mhs_assemble with a caller workspace",
-                one.total, cap);
-  int64_t lo = 1, hi = std::min<int64_t>(req->n_obs, 65535);
-  while (lo < hi) {
-    const int64_t mid = lo + (hi - lo + 1) / 2;
-    if (plan(req, mid).total <= cap) lo = mid;
-    else hi = mid - 1;
-  }
+                plan(req, 1).total, cap);
   mhs_request r = *req;
   r.workspace = scratch;
   r.workspace_bytes = cap;
-  const Layout L = plan(&r, lo);
+  const Layout L = plan(&r, chunk);
   cudaStream_t st = (cudaStream_t)stream;
-  switch (r.order) {
-    case 0: rc = run_kind<0>(&r, st, L); break;
-    case 1: rc = run_kind<1>(&r, st, L); break;
-    default: rc = run_kind<2>(&r, st, L); break;
-  }
+  rc = run_request(&r, st, L);
   if (rc || !status_bits) return rc;
   CUDA_TRY(cudaMemcpyAsync(status_bits, (char*)scratch + L.status, sizeof(int),
                            cudaMemcpyDeviceToHost, st));
@@ -1386,6 +250,10 @@ int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits)
 
 int mhs_read_status(void* workspace, void* stream, int* bits) {
   cudaStream_t st = (cudaStream_t)stream;
+  if (!workspace) {  // the allocation-free entry point's array on this device
+    const int rc = noalloc_scratch(&workspace);
+    if (rc) return rc;
+  }
   int h = 0;
   CUDA_TRY(cudaMemcpyAsync(&h, workspace, sizeof(int), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -1416,13 +284,9 @@ int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, c
   if (n <= 0 || term < 0 || term > 5 || (term >= 4 && want_u) || !obs || !tri || !coef_scratch ||
       !out)
     return fail(MHS_ERR_ARG, "debug_terms args");
-  cudaStream_t st = (cudaStream_t)stream;
-  switch (order) {
-    case 0: return debug_terms<0>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
-    case 1: return debug_terms<1>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
-    case 2: return debug_terms<2>(term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out, st);
-  }
-  return fail(MHS_ERR_ARG, "order");
+  if (order < 0 || order > 2) return fail(MHS_ERR_ARG, "order");
+  return g_terms[order](term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out,
+                        (cudaStream_t)stream);
 }
 
 int mhs_census_enable(int on) {
@@ -1488,8 +352,8 @@ int mhs_fp_peak(int fp64, int iters, double* tflops, void* stream) {
   float ms = 0.0f;
   for (int rep = 0; rep < 2; ++rep) {  // first pass warms up
     CUDA_TRY(cudaEventRecord(a, st));
-    if (fp64) k_fma_peak<double><<<blocks, threads, 0, st>>>(nullptr, iters, 0.999999, 1e-7);
-    else k_fma_peak<float><<<blocks, threads, 0, st>>>(nullptr, iters, 0.999999f, 1e-7f);
+    if (fp64) k_fma_peak_f64<<<blocks, threads, 0, st>>>(nullptr, iters, 0.999999, 1e-7);
+    else k_fma_peak_f32<<<blocks, threads, 0, st>>>(nullptr, iters, 0.999999f, 1e-7f);
     CUDA_TRY(cudaEventRecord(b, st));
     CUDA_TRY(cudaEventSynchronize(b));
     CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
@@ -1506,3 +370,4 @@ const char* mhs_last_error(void) { return g_err; }
 const char* mhs_version(void) { return "mhs_b200 0.1.0"; }
 
 }  // extern "C"
+

@@ -1,0 +1,155 @@
+// Declarations shared by the host translation unit (mhs_b200.cu, the C ABI)
+// and the kernel units (unit.cu, compiled once per order / readout /
+// precision so the library builds in parallel).
+//
+// A request runs as a short pipeline on the caller's stream, per chunk of
+// observers (kernels.cuh):
+//   k_coef   per-material image coefficients (once per request)
+//   k_prep   per-source frames, reflected frames, basis products, fold data
+//   k_pair   one thread per (observer, source): direct term + image R-family
+//   k_imageq one thread per (observer, source): image Q-family
+//   k_band   per straddling source, the ordered list of band receivers
+//   k_fold*  the folded image of every band pair
+//   k_final  one thread per (observer, output column): eigenstress,
+//            traction / interaction contraction, continuous-layout gather,
+//            and the store in the caller's layout
+// Per-pair tensors travel between stages in an element-major scratch table
+// (workspace), so every stage writes disjoint rows and no result depends on
+// atomics or scheduling order.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/mhs_b200.h"
+#include "engine_fold.cuh"
+#include "host_prep.h"
+
+namespace mhs {
+
+static_assert(cst::SMALL_U_OVER_RHO_SQ == cst::SMALL_U_OVER_RHO * cst::SMALL_U_OVER_RHO &&
+                  cst::SERIES_U_OVER_RHO_SQ == cst::SERIES_U_OVER_RHO * cst::SERIES_U_OVER_RHO,
+              "edge-regime thresholds and their squares disagree");
+
+namespace pipe {
+
+struct SrcPrep {
+  Frame f;        // element
+  Frame fi;       // reflected element (image R-family and fold mirror)
+  double eps;
+  double centre[2], r_f, diam;
+  int straddle;   // folded (fold requested and the source reaches the band)
+  int pad;
+};
+
+constexpr int TB = 128;          // threads per block for pair-parallel kernels
+constexpr int QFLOOR = cst::IMAGE_Q_GAUSS_MIN;
+
+enum : int { KD_DISP = 0, KD_HE = 1, KD_E = 2 };   // what the stages compute
+
+MHS_FI constexpr int kind_class(int kind) {
+  return kind == MHS_DISP ? KD_DISP : (kind == MHS_EIGENSTRESS ? KD_E : KD_HE);
+}
+MHS_FI constexpr int comps_of(int kc) { return kc == KD_DISP ? 9 : (kc == KD_HE ? 27 : 0); }
+// Scratch row per (observer, source, node): tensor comps, phi, phi_mirror.
+MHS_FI constexpr int row_of(int kc) { return comps_of(kc) + 2; }
+
+inline size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Workspace carve-up for a chunk of `chunk` observers.
+struct Layout {
+  size_t status, coef, prep, G, cnt, list, T, total;
+  int64_t chunk;
+};
+
+inline Layout plan(const mhs_request* r, int64_t chunk) {
+  const int kc = kind_class(r->kind);
+  const int K = n_nodes(r->order);
+  Layout L;
+  size_t off = 0;
+  L.status = off; off = align_up(off + 256);
+  L.coef = off; off = align_up(off + sizeof(double) * IMAGE_COEF_SIZE);
+  L.prep = off; off = align_up(off + sizeof(SrcPrep) * (size_t)r->n_src);
+  L.G = off;
+  if (kc != KD_E) off = align_up(off + sizeof(double) * G_SIZE * (size_t)r->n_src);
+  L.cnt = off; off = align_up(off + sizeof(int) * (size_t)r->n_src);
+  L.list = off; off = align_up(off + sizeof(int) * (size_t)r->n_src * (size_t)chunk);
+  L.T = off; off = align_up(off + sizeof(double) * (size_t)chunk * r->n_src * K * row_of(kc));
+  L.total = off;
+  L.chunk = chunk;
+  return L;
+}
+
+// ------------------------------------------- services of the host unit
+// Error text of this thread (mhs_last_error); returns `code`.
+int fail(int code, const char* fmt, ...);
+// Stage timing: whether it is on, and the record of one stage's events.
+bool prof_enabled();
+void prof_record(int stage, cudaEvent_t a, cudaEvent_t b);
+
+#define MHS_CUDA_TRY(x)                                                                     \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess)                                                                  \
+      return ::mhs::pipe::fail(MHS_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_));          \
+  } while (0)
+
+// Brackets one stage's launches with CUDA events on the request's stream
+// while stage timing is on.
+struct StageTimer {
+  int stage;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  StageTimer(int s, cudaStream_t stream) : stage(s), st(stream) {
+    if (prof_enabled()) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~StageTimer() {
+    if (a) {
+      cudaEventRecord(b, st);
+      prof_record(stage, a, b);
+    }
+  }
+};
+
+// ------------------------------------------------ kernel unit entry points
+// Each kernel unit holds its own copy of the Gauss-Legendre table (device
+// globals are per translation unit): `init` copies it in on the current
+// device; `run` queues one request's pipeline.  census: device counters
+// of the fold's work units, or null.
+using UnitInit = int (*)(const double* glx, const double* glw);
+using UnitRun = int (*)(const mhs_request* r, cudaStream_t st, const Layout& L,
+                        unsigned long long* census);
+using UnitTerms = int (*)(int term, int want_u, int n, const double* obs, const double* tri,
+                          double mu, double lam, double eps, double* coef, double* out,
+                          cudaStream_t st);
+
+#define MHS_UNIT_LIST(X) \
+  X(0, 0, 0) X(0, 0, 1) X(0, 1, 0) X(0, 1, 1) X(0, 2, 0) X(0, 2, 1) \
+  X(1, 0, 0) X(1, 0, 1) X(1, 1, 0) X(1, 1, 1) X(1, 2, 0) X(1, 2, 1) \
+  X(2, 0, 0) X(2, 0, 1) X(2, 1, 0) X(2, 1, 1) X(2, 2, 0) X(2, 2, 1)
+
+#define MHS_UNIT_DECL(P, KC, RF)                                                     \
+  int unit_init_##P##_##KC##_##RF(const double* glx, const double* glw);             \
+  int unit_run_##P##_##KC##_##RF(const mhs_request* r, cudaStream_t st, const Layout& L, \
+                                 unsigned long long* census);
+MHS_UNIT_LIST(MHS_UNIT_DECL)
+#undef MHS_UNIT_DECL
+
+#define MHS_TERMS_DECL(P)                                                                \
+  int unit_init_terms_##P(const double* glx, const double* glw);                         \
+  int unit_terms_##P(int term, int want_u, int n, const double* obs, const double* tri,  \
+                     double mu, double lam, double eps, double* coef, double* out,       \
+                     cudaStream_t st);
+MHS_TERMS_DECL(0)
+MHS_TERMS_DECL(1)
+MHS_TERMS_DECL(2)
+#undef MHS_TERMS_DECL
+
+}  // namespace pipe
+}  // namespace mhs

@@ -1,0 +1,53 @@
+// One kernel unit of the library.  The build compiles this file once per
+// (order P, readout class KC, far-field type RF) with
+//   -DMHS_UNIT_P=<0|1|2> -DMHS_UNIT_KC=<0 disp|1 stress+blob|2 blob> -DMHS_UNIT_RF=<0 double|1 float>
+// and once per order with -DMHS_UNIT_TERMS=<P> for the per-term diagnostics,
+// so the units compile in parallel; the host unit (mhs_b200.cu) dispatches.
+#include "kernels.cuh"
+
+#define MHS_CAT4_(a, b, c, d) a##b##_##c##_##d
+#define MHS_CAT4(a, b, c, d) MHS_CAT4_(a, b, c, d)
+#define MHS_CAT2_(a, b) a##b
+#define MHS_CAT2(a, b) MHS_CAT2_(a, b)
+
+namespace mhs {
+namespace pipe {
+
+namespace {
+int copy_tables(const double* glx, const double* glw) {
+  MHS_CUDA_TRY(cudaMemcpyToSymbol(d_glx, glx, sizeof(double) * GL_TABLE));
+  MHS_CUDA_TRY(cudaMemcpyToSymbol(d_glw, glw, sizeof(double) * GL_TABLE));
+  return MHS_OK;
+}
+}  // namespace
+
+#if defined(MHS_UNIT_TERMS)
+
+int MHS_CAT2(unit_init_terms_, MHS_UNIT_TERMS)(const double* glx, const double* glw) {
+  return copy_tables(glx, glw);
+}
+
+int MHS_CAT2(unit_terms_, MHS_UNIT_TERMS)(int term, int want_u, int n, const double* obs,
+                                          const double* tri, double mu, double lam, double eps,
+                                          double* coef, double* out, cudaStream_t st) {
+  return debug_terms<MHS_UNIT_TERMS>(term, want_u, n, obs, tri, mu, lam, eps, coef, out, st);
+}
+
+#else
+
+int MHS_CAT4(unit_init_, MHS_UNIT_P, MHS_UNIT_KC, MHS_UNIT_RF)(const double* glx,
+                                                               const double* glw) {
+  return copy_tables(glx, glw);
+}
+
+int MHS_CAT4(unit_run_, MHS_UNIT_P, MHS_UNIT_KC, MHS_UNIT_RF)(const mhs_request* r,
+                                                              cudaStream_t st, const Layout& L,
+                                                              unsigned long long* census) {
+  using RF = std::conditional_t<MHS_UNIT_RF == 1, float, double>;
+  return run<MHS_UNIT_P, MHS_UNIT_KC, RF>(r, st, L, census);
+}
+
+#endif
+
+}  // namespace pipe
+}  // namespace mhs

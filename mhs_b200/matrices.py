@@ -174,14 +174,31 @@ def _precision(precision) -> int:
 
 # ------------------------------------------------------------ the device
 class _Workspace:
-    """Per-device scratch buffer, grown on demand and reused across calls."""
+    """Per-device scratch buffer, grown on demand and reused across calls.
+
+    A call holds its device's lock from taking the buffer until its stream
+    has synchronised (``lock(device)``), so threads that assemble on the same
+    device take turns: none writes the buffer, or frees it by growing it,
+    while another's kernels still use it."""
 
     def __init__(self):
         self.buf = {}
+        self.locks = {}
+        self.guard = threading.Lock()
+
+    @staticmethod
+    def _key(device):
+        return device.index if device.index is not None else _torch().cuda.current_device()
+
+    def lock(self, device) -> threading.Lock:
+        key = self._key(device)
+        with self.guard:
+            return self.locks.setdefault(key, threading.Lock())
 
     def get(self, device, nbytes: int):
+        """The device's buffer, at least `nbytes` long; call with lock(device) held."""
         torch = _torch()
-        key = device.index if device.index is not None else torch.cuda.current_device()
+        key = self._key(device)
         b = self.buf.get(key)
         if b is None or b.numel() < nbytes:
             b = None
@@ -192,6 +209,13 @@ class _Workspace:
 
 
 _WS = _Workspace()
+
+#: Largest device staging buffer of a host (numpy / memmap) ``out=``: the
+#: output is assembled in observer-row blocks of at most this many bytes
+#: (and at most a quarter of the free device memory), each copied into its
+#: rows of ``out`` through pinned memory, so an output larger than the
+#: device's memory streams instead of failing.
+STREAM_BYTES = 1 << 30
 
 
 def _device(*xs):
@@ -242,6 +266,7 @@ class Pending:
         self.out = None
         self.ws = None
         self.ready = None   # event after which the staged inputs are on the device
+        self.consumer = None  # stream the result is handed to (set by the server)
 
     @property
     def out_bytes(self) -> int:
@@ -294,6 +319,9 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
     defer = getattr(_defer, "on", False)
     if defer and out is not None:
         raise ValueError("a served request returns its own device tensor: out= does not apply")
+    if out is not None and not _is_torch(out):
+        return _launch_streamed(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out,
+                                fold, subtract, normals, rec_basis, src_basis, precision, device)
     # output buffer
     dev_out = None
     if out is not None and _is_torch(out) and out.is_cuda:
@@ -353,28 +381,60 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
         for d in out_shape:
             entries *= int(d)
         return Pending(req, keep, tuple(out_shape), torch.float64, device, good.value, entries)
-    ws = _WS.get(device, good.value)
-    req.workspace = ctypes.c_void_p(ws.data_ptr())
-    req.workspace_bytes = ws.numel()
-    with torch.cuda.device(device):
-        stream = torch.cuda.current_stream(device)
-        _native.check(lib.mhs_assemble(ctypes.byref(req), ctypes.c_void_p(stream.cuda_stream)))
-        bits = ctypes.c_int(0)
-        _native.check(lib.mhs_read_status(ctypes.c_void_p(ws.data_ptr()),
-                                          ctypes.c_void_p(stream.cuda_stream), ctypes.byref(bits)))
+    with _WS.lock(device):
+        ws = _WS.get(device, good.value)
+        req.workspace = ctypes.c_void_p(ws.data_ptr())
+        req.workspace_bytes = ws.numel()
+        with torch.cuda.device(device):
+            stream = torch.cuda.current_stream(device)
+            _native.check(lib.mhs_assemble(ctypes.byref(req), ctypes.c_void_p(stream.cuda_stream)))
+            bits = ctypes.c_int(0)
+            _native.check(lib.mhs_read_status(ctypes.c_void_p(ws.data_ptr()),
+                                              ctypes.c_void_p(stream.cuda_stream),
+                                              ctypes.byref(bits)))
     if bits.value & _native.DEV_FOLD_GRID_OVERFLOW:
         raise RuntimeError("a fold polar grid exceeded its capacity (FOLD_MAX_BREAKS); "
                            "the source is far larger than its eps")
     del keep
     if out is not None:
-        if dev_out is out:
-            return out
-        if _is_torch(out):
+        if dev_out is not out:
             out.copy_(dev_out)
-            return out
-        np.copyto(out, dev_out.cpu().numpy())
         return out
     return dev_out if return_torch else dev_out.cpu().numpy()
+
+
+def _launch_streamed(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fold,
+                     subtract, normals, rec_basis, src_basis, precision, device):
+    """A host ``out=`` (numpy array or memmap, possibly larger than the
+    device): assemble blocks of observer rows into a device staging buffer
+    and copy each into its rows of ``out`` through pinned memory.  Every
+    layout's first axis is the observer (receiver) row, so a block of rows
+    is a contiguous slab of ``out``; the columns (sources) are whole in each
+    block, so the result equals the one-pass assembly (mhs/chunking.py:85-106
+    plans the same observer-axis slabs for its own ``out=``)."""
+    torch = _torch()
+    n_obs = out_shape[0]
+    dt = torch.float32 if out.dtype == np.float32 else torch.float64
+    row_bytes = int(np.prod(out_shape[1:])) * (4 if dt == torch.float32 else 8)
+    free, _ = torch.cuda.mem_get_info(device)
+    rows = chunking.stream_rows(n_obs, row_bytes, free, STREAM_BYTES)
+    stage = torch.empty((rows,) + tuple(out_shape[1:]), dtype=dt, device=device)
+    pinned = torch.empty(stage.shape, dtype=dt, pin_memory=True)
+
+    def part(a, lo, hi):
+        return None if a is None else a[lo:hi]
+
+    for lo in range(0, n_obs, rows):
+        hi = min(n_obs, lo + rows)
+        dev = stage[: hi - lo]
+        _launch(kind, obs[lo:hi], tri, mu, lam, eps_arr, p, ids, n_dof,
+                (hi - lo,) + tuple(out_shape[1:]), dev, fold, subtract=subtract,
+                normals=part(normals, lo, hi), rec_basis=part(rec_basis, lo, hi),
+                src_basis=src_basis, precision=precision, like=None)
+        host = pinned[: hi - lo]
+        host.copy_(dev)
+        np.copyto(out[lo:hi], host.numpy())
+    return out
 
 
 def _check_out(out, shape, n_obs, n_src, kind, parts):

@@ -76,9 +76,11 @@ class Server:
             pend = fn(*args, **kwargs)
             if not isinstance(pend, matrices.Pending):
                 raise TypeError(f"{getattr(fn, '__name__', fn)} is not a servable matrix function")
-            # the inputs were staged on this thread's current stream
+            # the inputs were staged on this thread's current stream, which is
+            # also the stream the result is handed to
             pend.ready = self.torch.cuda.Event()
             pend.ready.record()
+            pend.consumer = self.torch.cuda.current_stream(self.device)
         if pend.device_bytes > self.budget:
             raise MemoryError(f"request needs {pend.device_bytes / 2**30:.2f} GiB on the device, "
                               f"above the serving budget of {self.budget / 2**30:.2f} GiB; "
@@ -168,6 +170,12 @@ class Server:
                 need = pend.device_bytes
                 try:
                     res = pend.finish(self.streams[si])
+                    # the result was allocated on a serving stream: record the
+                    # consumer's stream so that, when the caller frees it, the
+                    # allocator waits for the caller's work before a later
+                    # request on that serving stream reuses the memory
+                    if res is not None and getattr(pend, "consumer", None) is not None:
+                        res.record_stream(pend.consumer)
                     t1 = time.perf_counter()
                     with self.cv:
                         self.lat.append(t1 - t0)

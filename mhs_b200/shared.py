@@ -1,13 +1,19 @@
-"""Shared-node table of a continuous quadratic slip (the ``layout="continuous"``
-source axis), host-side geometry with mhs's numbering (mhs/shared.py:80-273).
+"""The shared-node table of a continuous quadratic slip: the column axis of
+``layout="continuous"`` matrices, built on the host.
 
-Vertices are welded by rounding to ``WELD_TOL_OVER_H`` x the shortest edge,
-within a group (a fault network passes its fault ids so faults meeting along
-a line keep separate nodes there); the nodes are the welded vertices in
-lexicographic key order, then one midpoint per unique edge in lexicographic
-(sorted vertex pair) order.  Element ``s``'s nodes are ``ids[s]`` in the
-kernels' order ``v1 v2 v3 m12 m23 m31``.  The numbering has to equal mhs's so
-that a matrix's columns mean the same nodes in both libraries.
+The columns must mean the same nodes as mhs's (mhs/shared.py:80-273), so
+the numbering follows its rules: vertices are welded by rounding their
+coordinates to ``tol_over_h`` x the shortest edge, with the group id as a
+fourth key (faults of a network that meet along a line keep separate nodes
+there); welded vertices are numbered in lexicographic order of those keys,
+then come the edge midpoints in lexicographic order of their sorted vertex
+pairs.  Element ``s`` names its nodes ``ids[s]`` in the kernels' order
+``v1 v2 v3 m12 m23 m31``.  Tilings that cannot carry one slip per node are
+refused with mhs's messages: a collapsed triangle, an edge on three or more
+triangles, a soup with no shared edge, and neighbours wound opposite ways.
+
+Both numberings come from one helper, ``_rank_rows``: a lexicographic sort
+of integer key rows and a dense rank per distinct row.
 """
 from __future__ import annotations
 
@@ -20,13 +26,20 @@ from . import defaults, tdcs
 #: The one order the continuous layout exists for.
 CONTINUOUS_ORDER = 2
 LAYOUTS = ("discontinuous", "continuous")
+_LOCAL_EDGES = ((0, 1), (1, 2), (2, 0))   # m12, m23, m31
 
 
 @dataclasses.dataclass(frozen=True)
 class SharedNodes:
-    """Nodes of a continuous P2 slip: ``coords`` (n, 3) vertices then edge
-    midpoints, ``ids`` (n_tri, 6), upward ``normals`` (n, 3), ``boundary``
-    (rim nodes), ``weights`` (exact quadratic integration), ``group``."""
+    """Nodes of a continuous P2 slip on one triangulated surface.
+
+    ``coords`` (n, 3): the welded vertices, then the edge midpoints;
+    ``ids`` (n_tri, 6): each element's nodes; ``normals`` (n, 3): unit,
+    upward, the area-weighted mean of the adjoining elements' normals;
+    ``boundary`` (n,): nodes on edges that belong to one triangle only;
+    ``weights`` (n,): the exact quadrature of a quadratic field (area / 3 at
+    each edge midpoint, zero at the vertices); ``group`` (n,): the group a
+    node was welded in; ``n_vertices``; ``tol``: the weld tolerance."""
 
     coords: np.ndarray
     ids: np.ndarray
@@ -39,11 +52,12 @@ class SharedNodes:
 
     @property
     def n(self) -> int:
-        return int(self.coords.shape[0])
+        """Number of nodes (vertices + edges)."""
+        return len(self.coords)
 
     @property
     def n_tri(self) -> int:
-        return int(self.ids.shape[0])
+        return len(self.ids)
 
     @property
     def n_edges(self) -> int:
@@ -51,119 +65,127 @@ class SharedNodes:
 
     @property
     def frames(self) -> np.ndarray:
-        """``(n, 3, 3)`` [strike, dip, tensile] rows on each node normal."""
+        """``(n, 3, 3)`` cutde frames (rows strike, dip, tensile) on the node
+        normals (mhs.tdcs)."""
         return tdcs.frame_from_normals(self.normals)
 
     @property
     def trace(self) -> np.ndarray:
-        """Boundary nodes on the free surface."""
+        """Boundary nodes that lie on the free surface z = 0 (within tol)."""
         return self.boundary & (self.coords[:, 2] >= -self.tol)
 
     @property
     def front(self) -> np.ndarray:
-        """Boundary nodes inside the body (crack fronts, rooted edges)."""
+        """Boundary nodes below the surface: crack fronts and rooted edges."""
         return self.boundary & ~self.trace
 
-    def expand(self, values) -> np.ndarray:
-        """Nodal values (n, ...) -> element-major (n_tri * 6, ...)."""
-        v = np.asarray(values)
-        if v.shape[0] != self.n:
+    def _nodal(self, values, dtype=None) -> np.ndarray:
+        v = np.asarray(values, dtype=dtype)
+        if len(v) != self.n:
             raise ValueError(f"expected {self.n} nodal values, got {v.shape[0]}")
-        return v[self.ids].reshape((self.n_tri * 6,) + v.shape[1:])
+        return v
+
+    def expand(self, values) -> np.ndarray:
+        """Nodal values (n, ...) as the element-major source axis of the
+        discontinuous layout (n_tri * 6, ...), node index fastest."""
+        v = self._nodal(values)
+        return v[self.ids.ravel()]
 
     def integrate(self, values) -> np.ndarray:
-        """Exact integral of a quadratic nodal field over the surface."""
-        v = np.asarray(values, float)
-        if v.shape[0] != self.n:
-            raise ValueError(f"expected {self.n} nodal values, got {v.shape[0]}")
-        return np.tensordot(self.weights, v, axes=(0, 0))
+        """Integral of a quadratic nodal field over the whole surface."""
+        return np.tensordot(self.weights, self._nodal(values, float), axes=(0, 0))
 
     def element_mean(self, values) -> np.ndarray:
-        """Per-element mean by the three-midpoint rule."""
-        v = np.asarray(values, float)
-        return v[self.ids[:, 3:]].mean(axis=1)
+        """Mean of a nodal field over each element (its three midpoints)."""
+        return np.asarray(values, float)[self.ids[:, 3:]].mean(axis=1)
+
+
+def _rank_rows(keys: np.ndarray):
+    """Dense lexicographic rank of each row of an integer matrix, the number
+    of rows sharing each rank, and one representative row per rank (in rank
+    order)."""
+    order = np.lexsort(keys.T[::-1])
+    ranked = keys[order]
+    starts = np.ones(len(ranked), dtype=bool)
+    starts[1:] = np.any(ranked[1:] != ranked[:-1], axis=1)
+    rank = np.empty(len(keys), dtype=np.int64)
+    rank[order] = np.cumsum(starts) - 1
+    return rank, np.bincount(rank), ranked[starts]
+
+
+def _sum_by(index: np.ndarray, values: np.ndarray, n: int) -> np.ndarray:
+    """Per-index sums of the rows of `values` (added in row order)."""
+    values = values.reshape(len(index), -1)
+    return np.stack([np.bincount(index, weights=values[:, c], minlength=n)
+                     for c in range(values.shape[1])], axis=1)
 
 
 def shared_nodes(tris, *, groups=None, tol_over_h: float = defaults.WELD_TOL_OVER_H) -> SharedNodes:
-    """Build the :class:`SharedNodes` of ``tris (n_tri, 3, 3)``; refuses
-    non-manifold tilings, inconsistent winding and unconnected soups."""
+    """The :class:`SharedNodes` of ``tris`` (n_tri, 3, 3); ``groups``
+    (n_tri,) keeps the nodes of different groups (faults) apart."""
     t = np.ascontiguousarray(np.asarray(tris, dtype=np.float64))
     if t.ndim != 3 or t.shape[1:] != (3, 3) or t.shape[0] == 0:
         raise ValueError(f"tris must have shape (n_tri, 3, 3), got {t.shape}")
-    if not np.all(np.isfinite(t)):
+    if not np.isfinite(t).all():
         raise ValueError("tris must be finite")
-    n_tri = t.shape[0]
-    grp = (np.zeros(n_tri, dtype=np.int64) if groups is None
-           else np.asarray(groups).reshape(-1).astype(np.int64))
-    if grp.shape[0] != n_tri:
+    n_tri = len(t)
+    grp = np.zeros(n_tri, np.int64) if groups is None else \
+        np.asarray(groups).reshape(-1).astype(np.int64)
+    if len(grp) != n_tri:
         raise ValueError(f"groups has {grp.shape[0]} entries for {n_tri} triangles")
-    edge_len = np.linalg.norm(t - np.roll(t, 1, axis=1), axis=2)
-    h_min = float(edge_len.min())
+    h_min = float(np.linalg.norm(t - np.roll(t, 1, axis=1), axis=2).min())
     if not h_min > 0.0:
         raise ValueError("a triangle has a zero-length edge")
     tol = float(tol_over_h) * h_min
 
-    # --- weld: integer keys (rounded coordinates, group), unique in key order
-    pts = t.reshape(-1, 3)
-    keys = np.empty((pts.shape[0], 4), dtype=np.int64)
-    keys[:, :3] = np.round(pts / tol).astype(np.int64)
-    keys[:, 3] = np.repeat(grp, 3)
-    _, vid = np.unique(keys, axis=0, return_inverse=True)
-    vid = vid.reshape(-1)
-    n_v = int(vid.max()) + 1
-    cnt = np.bincount(vid, minlength=n_v).astype(float)
-    verts = np.zeros((n_v, 3))
-    np.add.at(verts, vid, pts)
-    verts /= cnt[:, None]
-    tv = vid.reshape(-1, 3)
-    if np.any(tv[:, 0] == tv[:, 1]) or np.any(tv[:, 1] == tv[:, 2]) or np.any(tv[:, 2] == tv[:, 0]):
+    # vertices: weld keys (rounded coordinates, group), ranked
+    corners = t.reshape(-1, 3)
+    keys = np.column_stack([np.round(corners / tol).astype(np.int64), np.repeat(grp, 3)])
+    vid, mult, _ = _rank_rows(keys)
+    n_v = len(mult)
+    verts = _sum_by(vid, corners, n_v) / mult[:, None]
+    tv = vid.reshape(n_tri, 3)
+    if any(np.any(tv[:, a] == tv[:, b]) for a, b in _LOCAL_EDGES):
         raise ValueError(f"a triangle has two vertices within the weld tolerance {tol:.3e}: "
                          f"degenerate, or tol_over_h too loose for this mesh")
 
-    # --- edges 12, 23, 31 of every element, unique in sorted-pair order
-    loc = np.stack([tv[:, [0, 1]], tv[:, [1, 2]], tv[:, [2, 0]]], axis=1).reshape(-1, 2)
-    pairs = np.sort(loc, axis=1)
-    edges, eid, ecount = np.unique(pairs, axis=0, return_inverse=True, return_counts=True)
-    eid = eid.reshape(-1)
-    if np.any(ecount > 2):
-        bad = int(np.argmax(ecount))
+    # edges: each element's 12, 23, 31 as sorted vertex pairs, ranked
+    walked = np.stack([tv[:, [a, b]] for a, b in _LOCAL_EDGES], axis=1).reshape(-1, 2)
+    eid, used, edges = _rank_rows(np.sort(walked, axis=1))
+    if used.max() > 2:
+        bad = int(np.argmax(used))
         raise ValueError(f"non-manifold: edge {edges[bad].tolist()} is shared by "
-                         f"{int(ecount[bad])} triangles, so a node on it has no single "
+                         f"{int(used[bad])} triangles, so a node on it has no single "
                          f"tangent plane. The continuous layout needs a manifold tiling.")
-    if n_tri > 1 and not np.any(ecount == 2):
+    if n_tri > 1 and not (used == 2).any():
         raise ValueError(f"nothing is shared: {n_tri} triangles and no common edge. A soup "
                          f"of separate elements wants the discontinuous layout; the "
                          f"continuous one welds vertices at {tol:.3e} (tol_over_h "
                          f"{tol_over_h:g} x the shortest edge {h_min:.3e}).")
-    forward = (loc[:, 0] < loc[:, 1]).astype(float)
-    n_fwd = np.bincount(eid, weights=forward, minlength=edges.shape[0])
-    bad_wind = (ecount == 2) & (n_fwd != 1)
-    if np.any(bad_wind):
-        bad = int(np.argmax(bad_wind))
+    # an interior edge is walked once in each direction by its two triangles
+    ascending = np.bincount(eid, weights=walked[:, 0] < walked[:, 1], minlength=len(edges))
+    flipped = (used == 2) & (ascending != 1)
+    if flipped.any():
+        bad = int(np.argmax(flipped))
         raise ValueError(f"inconsistent winding: the two triangles on edge {edges[bad].tolist()} "
                          f"traverse it the same way, so their vertex-order normals disagree "
                          f"and one Cartesian slip at a shared node would mean opposite jumps "
                          f"on the two sides. Wind the mesh consistently (every normal up is "
                          f"the usual choice).")
 
-    n_e = edges.shape[0]
-    coords = np.concatenate([verts, 0.5 * (verts[edges[:, 0]] + verts[edges[:, 1]])])
-    ids = np.concatenate([tv, n_v + eid.reshape(-1, 3)], axis=1)
-
-    boundary = np.zeros(n_v + n_e, bool)
-    rim = ecount == 1
+    n = n_v + len(edges)
+    ids = np.hstack([tv, n_v + eid.reshape(n_tri, 3)])
+    coords = np.vstack([verts, 0.5 * (verts[edges[:, 0]] + verts[edges[:, 1]])])
+    rim = used == 1
+    boundary = np.zeros(n, dtype=bool)
+    boundary[edges[rim].ravel()] = True
     boundary[n_v + np.flatnonzero(rim)] = True
-    boundary[edges[rim].reshape(-1)] = True
-
-    up = tdcs.unit_normals(t)
     area = 0.5 * np.linalg.norm(np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]), axis=1)
-    normals = np.zeros((n_v + n_e, 3))
-    np.add.at(normals, ids.reshape(-1), np.repeat(area[:, None] * up, 6, axis=0))
-    normals /= np.linalg.norm(normals, axis=1, keepdims=True)
-    weights = np.zeros(n_v + n_e)
-    np.add.at(weights, ids[:, 3:].reshape(-1), np.repeat(area / 3.0, 3))
-    group = np.zeros(n_v + n_e, dtype=np.int64)
-    group[ids.reshape(-1)] = np.repeat(grp, 6)
+    nsum = _sum_by(ids.ravel(), np.repeat(area[:, None] * tdcs.unit_normals(t), 6, axis=0), n)
+    normals = nsum / np.linalg.norm(nsum, axis=1, keepdims=True)
+    weights = np.bincount(ids[:, 3:].ravel(), weights=np.repeat(area / 3.0, 3), minlength=n)
+    group = np.zeros(n, dtype=np.int64)
+    group[ids.ravel()] = np.repeat(grp, 6)
     return SharedNodes(coords=coords, ids=ids, normals=normals, boundary=boundary,
                        weights=weights, group=group, n_vertices=int(n_v), tol=tol)
 

@@ -3,13 +3,15 @@
 Test infrastructure: the oracle reads its image coefficients from this file,
 taken straight from mhs's generated table (mhs/kernels/_image_table.py), so
 it shares no generated data with the CUDA library.  Run where the reference
-tree exists::
+tree exists, with its path as the argument or its ``src/`` directory in
+``MHS_REFERENCE_SRC``::
 
     python oracle/make_table.py [path to mhs/kernels/_image_table.py]
 """
 from __future__ import annotations
 
 import ast
+import os
 import pathlib
 import sys
 
@@ -44,4 +46,10 @@ def main(src: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/mhs/kernels/_image_table.py")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("MHS_REFERENCE_SRC"):
+        main(os.path.join(os.environ["MHS_REFERENCE_SRC"], "mhs", "kernels", "_image_table.py"))
+    else:
+        sys.exit("usage: make_table.py <mhs/kernels/_image_table.py> "
+                 "(or set MHS_REFERENCE_SRC to the reference's src/ directory)")

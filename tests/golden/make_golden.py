@@ -1,8 +1,7 @@
 """Generate the golden fixtures: inputs and mhs's own outputs, as .npz.
 
-Run where the reference package is importable (its source tree on
-``MHS_REFERENCE_SRC``, default the read-only checkout used to build this
-repository)::
+Run where the reference package is importable, with its ``src/`` directory
+in ``MHS_REFERENCE_SRC``::
 
     python tests/golden/make_golden.py [case ...]
 
@@ -23,7 +22,9 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
-sys.path.insert(0, os.environ.get("MHS_REFERENCE_SRC", "/root/reference/src"))
+if not os.environ.get("MHS_REFERENCE_SRC"):
+    sys.exit("set MHS_REFERENCE_SRC to the reference's src/ directory (the tree that holds mhs/)")
+sys.path.insert(0, os.environ["MHS_REFERENCE_SRC"])
 
 import mhs  # noqa: E402  (the reference)
 
@@ -152,9 +153,99 @@ def case_rough_surface():
     _save("rough_surface", tris=c["tris"], eps=c["eps"], mu=c["mu"], lam=c["lam"], int_p0=K)
 
 
+def case_signatures():
+    """The public functions' signatures as mhs declares them (parameter
+    names, kinds and defaults), for the CPU test that pins the drop-in's."""
+    import inspect
+    import json
+    names = ["disp_matrix", "stress_matrix", "total_stress_matrix", "eigenstress_matrix",
+             "elastic_strain_matrix", "traction_matrix", "interaction_matrix",
+             "collocation_points", "shared_nodes"]
+    sig = {}
+    for n in names:
+        sig[n] = [[p.name, p.kind.name, None if p.default is inspect.Parameter.empty
+                   else repr(p.default)] for p in inspect.signature(getattr(mhs, n)).parameters.values()]
+    (HERE / "signatures.json").write_text(json.dumps(sig, indent=1) + "\n")
+
+
+def case_c1_full():
+    """Config 1 in full: 600 observers x 100 triangles, disp and stress P0."""
+    c = synthetic.config1(seed=0)
+    mat = mhs.Material(c["mu"], c["lam"])
+    U = mhs.disp_matrix(c["obs"], c["tris"], mat, c["eps"])
+    S = mhs.stress_matrix(c["obs"], c["tris"], mat, c["eps"])
+    _save("c1_full", obs=c["obs"], tris=c["tris"], mu=c["mu"], lam=c["lam"], eps=c["eps"],
+          disp=U, stress=S)
+
+
+def _band_rows(pts, tris, eps):
+    """Receivers that take the folded image of at least one source."""
+    from mhs.kernels import fold
+    eps = np.broadcast_to(np.asarray(eps, float), (tris.shape[0],))
+    hit = np.zeros(pts.shape[0], bool)
+    for s in range(tris.shape[0]):
+        if fold.straddles(tris[s], eps[s]):
+            hit[fold.band(pts, tris[s], eps[s])] = True
+    return np.flatnonzero(hit)
+
+
+def _one_row(args):
+    """Worker: one receiver row of an interaction matrix through rows=."""
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    r, tris, mu, lam, eps, kw = args
+    import mhs as m
+    kw = dict(kw)
+    if kw.get("layout") == "continuous":
+        kw["shared"] = m.shared_nodes(tris, groups=kw.pop("groups"))
+    return m.interaction_matrix(tris, m.Material(mu, lam), eps, rows=(r, r + 1), **kw)[0]
+
+
+def _rows(tris, mu, lam, eps, rows, kw, workers=8):
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with cf.ProcessPoolExecutor(workers, mp_context=ctx) as ex:
+        return np.stack(list(ex.map(_one_row, [(int(r), tris, mu, lam, eps, kw) for r in rows])))
+
+
+def case_c2_rows():
+    """Config 2 at its full size (2,400 triangles, per-triangle eps, fold on):
+    8 seeded fold-band receiver rows and 8 other rows of the full 3x3
+    interaction matrix, each through rows=(r, r + 1)."""
+    c = synthetic.config2(seed=0)
+    tris, eps = c["tris"], c["eps"]
+    pts = mhs.collocation_points(tris)
+    band = _band_rows(pts, tris, eps)
+    other = np.setdiff1d(np.arange(pts.shape[0]), band)
+    rng = np.random.default_rng(2)
+    rows = np.concatenate([np.sort(rng.choice(band, 8, replace=False)),
+                           np.sort(rng.choice(other, 8, replace=False))])
+    K = _rows(tris, c["mu"], c["lam"], eps, rows, {})
+    _save("c2_rows", tris=tris, eps=eps, mu=c["mu"], lam=c["lam"], rows=rows, n_band=8, K=K)
+
+
+def case_c4_rows():
+    """Config 4 at its full size (3-fault network, continuous P2, source =
+    (strike, dip), fold on at the trace): 4 seeded fold-band rows and 4
+    other rows, each through rows=(r, r + 1)."""
+    c = synthetic.config4()
+    tris, groups = c["tris"], c["groups"]
+    sn = mhs.shared_nodes(tris, groups=groups)
+    band = _band_rows(sn.coords, tris, c["eps"])
+    other = np.setdiff1d(np.arange(sn.n), band)
+    rng = np.random.default_rng(4)
+    rows = np.concatenate([np.sort(rng.choice(band, 4, replace=False)),
+                           np.sort(rng.choice(other, 4, replace=False))])
+    kw = dict(order=2, layout="continuous", groups=groups, source=("strike", "dip"))
+    K = _rows(tris, c["mu"], c["lam"], c["eps"], rows, kw)
+    _save("c4_rows", tris=tris, groups=groups, eps=c["eps"], mu=c["mu"], lam=c["lam"],
+          rows=rows, n_band=4, n_cols=sn.n, K=K)
+
+
 CASES = {f.__name__[5:]: f for f in (case_c1_subset, case_orders, case_eps_per_tri,
                                      case_interaction, case_fold, case_continuous,
-                                     case_rough_surface)}
+                                     case_rough_surface, case_signatures, case_c1_full,
+                                     case_c2_rows, case_c4_rows)}
 
 if __name__ == "__main__":
     names = sys.argv[1:] or list(CASES)

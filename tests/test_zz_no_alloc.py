@@ -30,6 +30,14 @@ def _lib():
     return lib
 
 
+def _device_memory():
+    """Free device bytes and the count of torch allocations made so far."""
+    import torch
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    return free, torch.cuda.memory_stats().get("allocation.all.allocated", 0)
+
+
 def _request(kind, obs, tris, eps, mu, lam, out, keep, normals=None, rec=None, src=None):
     import torch
     from mhs_b200 import _native
@@ -55,14 +63,32 @@ def _request(kind, obs, tris, eps, mu, lam, out, keep, normals=None, rec=None, s
 
 
 def _run_twice(lib, req, out):
+    """A set-up call, then two calls in a row.  The first call on a device
+    looks up the scratch array's device address, and the kernels' modules
+    load on their first launch; after it, a call must leave the device's
+    free memory and torch's allocation count exactly as they were.  The
+    second of the measured calls reads its status word through
+    mhs_read_status(NULL, ...), the array's own status."""
     import torch
-    got = []
-    for _ in range(2):
+    bits = ctypes.c_int(-1)
+    assert lib.mhs_assemble_noalloc(ctypes.byref(req), None, ctypes.byref(bits)) == 0, \
+        lib.mhs_last_error()
+    assert bits.value == 0
+    got = [out.cpu().numpy().copy()]
+    for i in range(2):
         out.fill_(float("nan"))
+        before = _device_memory()
         bits = ctypes.c_int(-1)
-        rc = lib.mhs_assemble_noalloc(ctypes.byref(req), None, ctypes.byref(bits))
+        if i == 0:
+            rc = lib.mhs_assemble_noalloc(ctypes.byref(req), None, ctypes.byref(bits))
+        else:
+            rc = lib.mhs_assemble_noalloc(ctypes.byref(req), None, None)
+            assert rc == 0, lib.mhs_last_error()
+            rc = lib.mhs_read_status(None, None, ctypes.byref(bits))
         assert rc == 0, lib.mhs_last_error()
         assert bits.value == 0
+        after = _device_memory()
+        assert after == before, f"device memory changed across the call: {before} -> {after}"
         torch.cuda.synchronize()
         got.append(out.cpu().numpy().copy())
     return got
