@@ -33,7 +33,7 @@ MHS_FI double ipow(double x, int e) {
 // reciprocal square roots and the divisions by R_a, R_b and rho2 taken as
 // products with their reciprocals (rounding-level differences).
 template <class S, bool FAST = false>
-MHS_HD void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
+MHS_FI void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
   constexpr Spec sp = S::spec;
   double Ra, Rb, iRa, iRb, irho2;
   if constexpr (FAST) {
@@ -123,7 +123,7 @@ MHS_HD void edge_closed(double ua, double ub, double rho2, double P[MS][8]) {
 // and every term goes to its sum as it appears: for each (m, k) the terms
 // arrive in increasing t, the order of the plain double loop.
 template <class S>
-MHS_HD void edge_small(double ua, double ub, double rho, double P[MS][8]) {
+MHS_FI void edge_small(double ua, double ub, double rho, double P[MS][8]) {
   constexpr Spec sp = S::spec;
   constexpr int T = cst::SERIES_TERMS;
   constexpr int PWMAX = sp.kmax + 2 * (T - 1) + 1;
@@ -197,7 +197,7 @@ MHS_FI constexpr int spec_max_need0(const Spec& sp) {
 // increasing -q; the sum over t keeps a window of them in registers, and each
 // (m, k) sum takes its terms in increasing t as the plain double loop does.
 template <class S>
-MHS_HD void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
+MHS_FI void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
   constexpr Spec sp = S::spec;
   constexpr int T = cst::SERIES_TERMS;
   constexpr int QHI = series_qhi(sp);             // largest s
@@ -407,7 +407,7 @@ MHS_FI void foot_vertices(const Frame& f, double X0, double X1, double pr[3][2])
 // components of xi_1^a xi_2^b / R^m along the edge, BN1/BN2, expanded as
 // polynomials in u (xi_1 = dp c1 + u s1, xi_2 = dp c2 + u s2).
 template <class S>
-MHS_HD void edge_accumulate(const EdgeGeom& g, const double P[MS][8], double* BN1, double* BN2,
+MHS_FI void edge_accumulate(const EdgeGeom& g, const double P[MS][8], double* BN1, double* BN2,
                             double* BD) {
   constexpr Spec sp = S::spec;
   const double s1 = g.s1, s2 = g.s2, dp = g.dp;
@@ -464,11 +464,70 @@ MHS_HD void closed_finish(const double pr[3][2], double h2, const double* BN1, c
   closed_finish_t<S, false>(pr, h2, BN1, BN2, BD, T);
 }
 
+// One slot's part of the closed-form table: its upward vertical seed
+// I_{n+2} = (E_n + (n-2) I_n) / (n h^2) (slot s = nslot(n + 2)), its
+// downward seed I_n = (E_n - n h^2 I_{n+2}) / (2 - n), and its horizontal
+// recursion.  The slot and its degree are template constants so every
+// index into the tables is a compile-time constant (no local memory).
+template <class S, bool FAST, int n>
+MHS_FI void seed_up(double h2, double ih2, const double* BD, MomentTable<S>& T) {
+  constexpr Spec sp = S::spec;
+  if constexpr (n + 2 <= 9) {
+    if constexpr (sp.deg[nslot(n + 2)] >= 0) {
+      if constexpr (FAST)
+        T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) * (ih2 * (1.0 / n));
+      else
+        T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) / (n * h2);
+      seed_up<S, FAST, n + 2>(h2, ih2, BD, T);
+    }
+  }
+}
+
+template <class S, int n>
+MHS_FI void seed_down(double h2, const double* BD, MomentTable<S>& T) {
+  constexpr Spec sp = S::spec;
+  if constexpr (n >= -1) {
+    if constexpr (sp.deg[nslot(n)] >= 0) {
+      const double corr = n * h2 * T.at(nslot(n + 2), 0, 0);
+      T.at(nslot(n), 0, 0) = (BD[nslot(n)] - corr) / (2.0 - n);
+      seed_down<S, n - 2>(h2, BD, T);
+    }
+  }
+}
+
+template <class S, int s>
+MHS_FI void recur_slot(const double* BN1, const double* BN2, MomentTable<S>& T) {
+  constexpr Spec sp = S::spec;
+  if constexpr (s < NS) {
+    constexpr int d = sp.deg[s];
+    if constexpr (d > 0) {
+      constexpr int n = slot_n(s), mj = s - 1;   // m = n - 2
+      const double inv = 1.0 / (double)(n - 2);
+#pragma unroll
+      for (int q = 1; q <= d; ++q)
+#pragma unroll
+        for (int a = q; a >= 0; --a) {
+          const int b = q - a;
+          double val;
+          if (a >= 1) {
+            val = -BN1[sp.b_off[mj] + tri_idx(a - 1, b)];
+            if (a >= 2) val = val + (a - 1) * T.at(s - 1, a - 2, b);
+          } else {
+            val = -BN2[sp.b_off[mj] + tri_idx(0, b - 1)];
+            if (b >= 2) val = val + (b - 1) * T.at(s - 1, 0, b - 2);
+          }
+          T.at(s, a, b) = val * inv;
+        }
+    }
+    recur_slot<S, s + 1>(BN1, BN2, T);
+  }
+}
+
 // FAST (the fold's near loads): 1/h from a reciprocal square root and the
 // seeds' divisions by n h^2 as products with 1/h^2 (rounding-level
 // differences).
 template <class S, bool FAST>
-MHS_HD void closed_finish_t(const double pr[3][2], double h2, const double* BN1, const double* BN2,
+MHS_FI void closed_finish_t(const double pr[3][2], double h2, const double* BN1, const double* BN2,
                             const double* BD, MomentTable<S>& T) {
   constexpr Spec sp = S::spec;
   double h, I3, ih2 = 0.0;
@@ -484,45 +543,9 @@ MHS_HD void closed_finish_t(const double pr[3][2], double h2, const double* BN1,
 #pragma unroll
   for (int i = 0; i < sp.m_off[NS]; ++i) T.M[i] = 0.0;
   T.at(nslot(3), 0, 0) = I3;
-  // upward seeds I_{n+2} = (E_n + (n-2) I_n) / (n h^2)
-#pragma unroll
-  for (int n = 3; n + 2 <= 9; n += 2) {
-    if (sp.deg[nslot(n + 2)] < 0) break;
-    if constexpr (FAST)
-      T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) * (ih2 * (1.0 / n));
-    else
-      T.at(nslot(n + 2), 0, 0) = (BD[nslot(n)] + (n - 2) * T.at(nslot(n), 0, 0)) / (n * h2);
-  }
-  // downward seeds I_n = (E_n - n h^2 I_{n+2}) / (2 - n)
-#pragma unroll
-  for (int n = 1; n >= -1; n -= 2) {
-    if (sp.deg[nslot(n)] < 0) break;
-    const double corr = n * h2 * T.at(nslot(n + 2), 0, 0);
-    T.at(nslot(n), 0, 0) = (BD[nslot(n)] - corr) / (2.0 - n);
-  }
-  // horizontal recursion, ascending n
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const int d = sp.deg[s];
-    if (d <= 0) continue;
-    const int n = slot_n(s), mj = s - 1;   // m = n - 2
-    const double inv = 1.0 / (double)(n - 2);
-#pragma unroll
-    for (int q = 1; q <= d; ++q)
-#pragma unroll
-      for (int a = q; a >= 0; --a) {
-        const int b = q - a;
-        double val;
-        if (a >= 1) {
-          val = -BN1[sp.b_off[mj] + tri_idx(a - 1, b)];
-          if (a >= 2) val = val + (a - 1) * T.at(s - 1, a - 2, b);
-        } else {
-          val = -BN2[sp.b_off[mj] + tri_idx(0, b - 1)];
-          if (b >= 2) val = val + (b - 1) * T.at(s - 1, 0, b - 2);
-        }
-        T.at(s, a, b) = val * inv;
-      }
-  }
+  seed_up<S, FAST, 3>(h2, ih2, BD, T);    // upward seeds from I_3
+  seed_down<S, 1>(h2, BD, T);             // downward seeds I_1, I_-1
+  recur_slot<S, 0>(BN1, BN2, T);          // horizontal recursion, ascending n
 }
 
 template <class S>
@@ -551,26 +574,32 @@ MHS_HD void closed_moments(const Frame& f, double X0, double X1, double h2, Mome
 
 // W_k[n](a, b) = sum_{a'+b'<=P} c_k(a', b') M_n(a + a', b + b'), at the
 // constant-slip degrees (mhs/fullspace/moments.py:370-398).
-template <class S, int P>
-MHS_HD void weight_closed(const MomentTable<S>& T, const double c[][ntri(P)], int k, double* W) {
+template <class S, int P, int s>
+MHS_FI void weight_slot(const MomentTable<S>& T, const double c[][ntri(P)], int k, double* W) {
   constexpr Spec sp = S::spec;
+  if constexpr (s < NS) {
+    constexpr int d = sp.need0[s];
+    if constexpr (d >= 0) {
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const int d = sp.need0[s];
-    if (d < 0) continue;
+      for (int a = 0; a <= d; ++a)
 #pragma unroll
-    for (int a = 0; a <= d; ++a)
+        for (int b = 0; a + b <= d; ++b) {
+          double acc = 0.0;
 #pragma unroll
-      for (int b = 0; a + b <= d; ++b) {
-        double acc = 0.0;
+          for (int ap = 0; ap <= P; ++ap)
 #pragma unroll
-        for (int ap = 0; ap <= P; ++ap)
-#pragma unroll
-          for (int bp = 0; ap + bp <= P; ++bp)
-            acc += c[k][tri_idx(ap, bp)] * T.at(s, a + ap, b + bp);
-        W[sp.w_off[s] + tri_idx(a, b)] = acc;
-      }
+            for (int bp = 0; ap + bp <= P; ++bp)
+              acc += c[k][tri_idx(ap, bp)] * T.at(s, a + ap, b + bp);
+          W[sp.w_off[s] + tri_idx(a, b)] = acc;
+        }
+    }
+    weight_slot<S, P, s + 1>(T, c, k, W);
   }
+}
+
+template <class S, int P>
+MHS_FI void weight_closed(const MomentTable<S>& T, const double c[][ntri(P)], int k, double* W) {
+  weight_slot<S, P, 0>(T, c, k, W);
 }
 
 // ----------------------------------------------------- far-field quadrature

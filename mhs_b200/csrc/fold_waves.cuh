@@ -1,0 +1,920 @@
+// The fold as a planned multi-kernel pipeline (mhs/kernels/fold.py:
+// 290-367): the Boussinesq correction of every band pair -- a source that
+// reaches the surface seen from a receiver in its band -- is the weighted
+// sum, over the receiver's polar grid on z = 0, of the point-load response
+// times the element's surface load there minus the load at the receiver's
+// foot.  Each stage runs as its own kernel, so each gets the registers and
+// occupancy its own arithmetic needs:
+//
+//   plan     per pair: radial breaks and angular rules -> panels and nodes
+//            (counts, then prefix sums); the host reads the totals back
+//   foot     per pair: the surface load at the receiver's foot
+//   nodes    per panel: node positions and weights; each node classified as
+//            a far node (12 x 12 or 8 x 8 rule) or a near node keyed by the
+//            forms of its three edges (how many take the small-|u| and the
+//            large-|u| series), so that every warp of the load kernels runs
+//            one code path
+//   scatter  stable-enough class lists (order inside a list does not enter
+//            any sum: loads are stored per node)
+//   far/near the surface loads, one thread per node
+//   accum    per pair, panel by panel in grid order: the weighted
+//            point-load products of each panel reduced in a fixed tree
+//            order and added to the pair's running sum, so the result does
+//            not depend on how panels were grouped into waves
+//   finish   per pair: the disk term and the add into the pair's table row
+//
+// Nodes live in bounded waves of whole panels (the workspace's fold
+// region), pairs in batches; both sizes come from the totals read back
+// after the plan, one short stream synchronisation per batch.
+#pragma once
+
+namespace fold_waves {
+
+constexpr int NCLS = 12;          // 10 near signatures, far 12 x 12, far 8 x 8
+constexpr int CLS_FAR12 = 10;
+constexpr int CLS_FAR8 = 11;
+
+// Near signature of a node from its edge-form counts (n_small, n_large),
+// n_small + n_large <= 3; the inverse tables give the counts back.
+MHS_FI int near_sig(int ns, int nl) {
+  // rows ns = 0..3, columns nl = 0..3 (entries with ns + nl > 3 unused)
+  const int base[4] = {0, 4, 7, 9};
+  return base[ns] + nl;
+}
+__device__ const int kSigSmall[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+__device__ const int kSigLarge[10] = {0, 1, 2, 3, 0, 1, 2, 0, 1, 0};
+
+// Device-side counters shared by the fold kernels of one request chunk.
+struct Hdr {
+  long long n_st, n_pairs;               // straddling sources, band pairs (chunk)
+  long long q_batch, n_batch, max_panel; // panels, nodes, largest panel (batch)
+  long long wave_q0, wave_q1;            // panels of the current wave
+  long long wave_n0, wave_nodes;         // first node and node count of the wave
+  long long cls_off[NCLS + 1];           // class offsets in the list array
+  int cls_count[NCLS];
+  int cls_fill[NCLS];
+};
+
+// Per straddling source: far rules (double, and float for the mixed form)
+// and the sigma_zz row of the surface load.
+template <int P, class RF>
+struct Src {
+  SmemRules<P> rd;
+  std::conditional_t<std::is_same<RF, float>::value, FloatRules<P>, NoRules> fr;
+  SurfaceLoadConsts slc;
+};
+
+// ------------------------------------------------------------- band scan
+// One block: straddle ranks, their sources and the prefix of band pairs by
+// straddle rank; totals into the header.
+__global__ void __launch_bounds__(1024)
+k_band_scan(int64_t n_src, const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
+            int* __restrict__ st_rank, int* __restrict__ st_src, long long* __restrict__ st_off,
+            Hdr* __restrict__ hdr) {
+  __shared__ long long s_pairs[1024];
+  __shared__ int s_st[1024];
+  __shared__ long long base_pairs;
+  __shared__ int base_st;
+  if (threadIdx.x == 0) {
+    base_pairs = 0;
+    base_st = 0;
+  }
+  __syncthreads();
+  for (int64_t s0 = 0; s0 < n_src; s0 += 1024) {
+    const int64_t s = s0 + threadIdx.x;
+    const int is_st = (s < n_src && prep[s].straddle) ? 1 : 0;
+    const long long np = is_st ? (long long)cnt[s] : 0;
+    s_st[threadIdx.x] = is_st;
+    s_pairs[threadIdx.x] = np;
+    __syncthreads();
+    // inclusive Hillis-Steele scans
+    for (int d = 1; d < 1024; d <<= 1) {
+      const int a = threadIdx.x >= d ? s_st[threadIdx.x - d] : 0;
+      const long long b = threadIdx.x >= d ? s_pairs[threadIdx.x - d] : 0;
+      __syncthreads();
+      s_st[threadIdx.x] += a;
+      s_pairs[threadIdx.x] += b;
+      __syncthreads();
+    }
+    if (s < n_src) {
+      const int rank = base_st + s_st[threadIdx.x] - is_st;
+      st_rank[s] = is_st ? rank : -1;
+      if (is_st) {
+        st_src[rank] = (int)s;
+        st_off[rank] = base_pairs + s_pairs[threadIdx.x] - np;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 1023) {
+      base_st += s_st[1023];
+      base_pairs += s_pairs[1023];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    st_off[base_st] = base_pairs;
+    hdr->n_st = base_st;
+    hdr->n_pairs = base_pairs;
+  }
+}
+
+// ----------------------------------------------------------- source data
+template <int P, int KC, class RF>
+__global__ void __launch_bounds__(128)
+k_src(int j0, int nj, const int* __restrict__ st_src, const SrcPrep* __restrict__ prep, double mu,
+      double lam, Src<P, RF>* __restrict__ out) {
+  const int j = blockIdx.x;
+  if (j >= nj) return;
+  const SrcPrep& sp = prep[st_src[j0 + j]];
+  Src<P, RF>& d = out[j];
+  const Material m = make_material(mu, lam);
+  d.rd.build(sp.f, threadIdx.x, blockDim.x);
+  if (threadIdx.x < NLIFT) {
+    double col[3] = {};
+    szz_coefficient(sp.f, sp.eps, m, threadIdx.x, col);
+    for (int c = 0; c < 3; ++c) d.slc.coef[c][threadIdx.x] = col[c];
+  }
+  if (threadIdx.x == NLIFT) surface_load_ezz(sp.f, sp.eps, m, d.slc);
+  if constexpr (std::is_same<RF, float>::value) {
+    __syncthreads();
+    float_rules<P>(d.rd, d.fr, threadIdx.x, blockDim.x);
+  }
+}
+
+// ------------------------------------------------------------- the plan
+// Straddle rank of global pair p (st_off ascending, st_off[j] <= p).
+__device__ __forceinline__ int pair_straddler(const long long* st_off, int n_st, long long p) {
+  int lo = 0, hi = n_st - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (st_off[mid] <= p) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct PairGeom {
+  FoldPair fp;
+  double diam;
+};
+
+__device__ __forceinline__ void pair_geom(const double* obs, int64_t lo, int oc, const SrcPrep& sp,
+                                          FoldPair& fp) {
+  const int64_t o = lo + oc;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  fold_pair_setup(x, sp.centre, sp.r_f, sp.eps, fp);
+}
+
+// Panels and nodes of each pair of the batch [p0, p0 + np): band pair ->
+// (straddler, receiver), breaks, kept panels and their angular rules.  One
+// thread per pair; the largest panel's node count goes to hdr->max_panel.
+__global__ void __launch_bounds__(128)
+k_pairs(long long p0, int np, int64_t lo, int64_t n_chunk, const double* __restrict__ obs,
+        const SrcPrep* __restrict__ prep, const int* __restrict__ list,
+        const int* __restrict__ st_src, const long long* __restrict__ st_off,
+        Hdr* __restrict__ hdr, int* __restrict__ pair_st, int* __restrict__ pair_oc,
+        long long* __restrict__ pair_npanel, long long* __restrict__ pair_nnode,
+        int* __restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const long long p = p0 + i;
+  const int j = pair_straddler(st_off, (int)hdr->n_st, p);
+  const int s = st_src[j];
+  const int oc = list[(int64_t)s * n_chunk + (p - st_off[j])];
+  pair_st[i] = j;
+  pair_oc[i] = oc;
+  const SrcPrep& sp = prep[s];
+  FoldPair fp;
+  pair_geom(obs, lo, oc, sp, fp);
+  double br[FOLD_MAX_BREAKS];
+  double R1;
+  const int nb = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, sp.eps, sp.diam, br, &R1);
+  long long npan = 0, nnode = 0, big = 0;
+  if (nb < 0) {
+    atomicOr(status, MHS_DEV_FOLD_GRID_OVERFLOW);
+  } else {
+    for (int k = 0; k + 1 < nb; ++k) {
+      if (br[k + 1] - br[k] < 1e-9 * sp.eps) continue;
+      AngRule A;
+      fold_panel_rule(fp, br[k], br[k + 1], A);
+      ++npan;
+      if (A.n < 0) {
+        atomicOr(status, MHS_DEV_FOLD_GRID_OVERFLOW);
+        continue;
+      }
+      const long long n = (long long)cst::FOLD_N_RADIAL * A.n;
+      nnode += n;
+      big = n > big ? n : big;
+    }
+  }
+  pair_npanel[i] = npan;
+  pair_nnode[i] = nnode;
+  if (big) atomicMax(reinterpret_cast<unsigned long long*>(&hdr->max_panel), (unsigned long long)big);
+}
+
+// Exclusive prefix sum in place over a[0..n) (a[n] receives the total),
+// one block; optionally the maximum of the inputs into *mx.
+__global__ void __launch_bounds__(1024)
+k_scan(long long* __restrict__ a, long long n, long long* __restrict__ total,
+       long long* __restrict__ mx) {
+  __shared__ long long sh[1024];
+  __shared__ long long base, best;
+  if (threadIdx.x == 0) {
+    base = 0;
+    best = 0;
+  }
+  __syncthreads();
+  for (long long i0 = 0; i0 < n; i0 += 1024) {
+    const long long i = i0 + threadIdx.x;
+    const long long v = i < n ? a[i] : 0;
+    sh[threadIdx.x] = v;
+    if (mx && v > 0) atomicMax(reinterpret_cast<unsigned long long*>(&best), (unsigned long long)v);
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+      const long long t = threadIdx.x >= d ? sh[threadIdx.x - d] : 0;
+      __syncthreads();
+      sh[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < n) a[i] = base + sh[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) base += sh[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a[n] = base;
+    if (total) *total = base;
+    if (mx) *mx = best;
+  }
+}
+
+// Radial interval and first node of every kept panel (one thread per pair;
+// the pair's panels start at pair_poff[i], its nodes at pair_noff[i]).
+__global__ void __launch_bounds__(128)
+k_panels(int np, int64_t lo, const double* __restrict__ obs, const SrcPrep* __restrict__ prep,
+         const int* __restrict__ st_src, const int* __restrict__ pair_st,
+         const int* __restrict__ pair_oc, const long long* __restrict__ pair_poff,
+         const long long* __restrict__ pair_noff, double* __restrict__ pan_ra,
+         double* __restrict__ pan_rb, long long* __restrict__ pan_noff) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > np) return;
+  if (i == np) {  // closing entry: the batch's node total
+    pan_noff[pair_poff[np]] = pair_noff[np];
+    return;
+  }
+  const SrcPrep& sp = prep[st_src[pair_st[i]]];
+  FoldPair fp;
+  pair_geom(obs, lo, pair_oc[i], sp, fp);
+  double br[FOLD_MAX_BREAKS];
+  double R1;
+  const int nb = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, sp.eps, sp.diam, br, &R1);
+  long long q = pair_poff[i], u = pair_noff[i];
+  for (int k = 0; k + 1 < nb; ++k) {
+    const double ra = br[k], rb = br[k + 1];
+    if (rb - ra < 1e-9 * sp.eps) continue;
+    AngRule A;
+    fold_panel_rule(fp, ra, rb, A);
+    pan_ra[q] = ra;
+    pan_rb[q] = rb;
+    pan_noff[q] = u;
+    u += A.n < 0 ? 0 : (long long)cst::FOLD_N_RADIAL * A.n;
+    ++q;
+  }
+}
+
+// Surface load at each receiver's foot (one thread per pair).
+template <int P, int KC, class RF>
+__global__ void __launch_bounds__(128)
+k_foot(int np, int j0, int64_t lo, const double* __restrict__ obs,
+       const SrcPrep* __restrict__ prep, const int* __restrict__ st_src,
+       const int* __restrict__ pair_st, const int* __restrict__ pair_oc,
+       const Src<P, RF>* __restrict__ srcs, double* __restrict__ foot) {
+  constexpr int NJ = 3 * n_nodes(P);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int j = pair_st[i];
+  const SrcPrep& sp = prep[st_src[j]];
+  const Src<P, RF>& d = srcs[j - j0];
+  const int64_t o = lo + pair_oc[i];
+  double sl[NJ] = {};
+  fold_surface_load_fast<P, RF>(sp.f, d.rd.r12(), d.rd.r8(), d.slc, obs[3 * o], obs[3 * o + 1],
+                                sp.eps, sl);
+  for (int jj = 0; jj < NJ; ++jj) foot[(size_t)i * NJ + jj] = sl[jj];
+}
+
+// --------------------------------------------------------------- a wave
+// Panels [q0, q1) of the batch whose first node lies in
+// [w * span, (w + 1) * span); the first node of the wave and its count.
+__global__ void k_wave_begin(long long w, long long span, long long nq,
+                             const long long* __restrict__ pan_noff, Hdr* __restrict__ hdr) {
+  auto first_at = [&](long long v) {  // first panel q with pan_noff[q] >= v
+    long long a = 0, b = nq;
+    while (a < b) {
+      const long long m = (a + b) >> 1;
+      if (pan_noff[m] < v) a = m + 1;
+      else b = m;
+    }
+    return a;
+  };
+  const long long q0 = first_at(w * span), q1 = first_at((w + 1) * span);
+  hdr->wave_q0 = q0;
+  hdr->wave_q1 = q1;
+  hdr->wave_n0 = pan_noff[q0];
+  hdr->wave_nodes = pan_noff[q1] - pan_noff[q0];
+  for (int c = 0; c < NCLS; ++c) {
+    hdr->cls_count[c] = 0;
+    hdr->cls_fill[c] = 0;
+  }
+}
+
+// Pair of panel q (pair_poff ascending).
+__device__ __forceinline__ int panel_pair(const long long* pair_poff, int np, long long q) {
+  int a = 0, b = np - 1;
+  while (a < b) {
+    const int m = (a + b + 1) >> 1;
+    if (pair_poff[m] <= q) a = m;
+    else b = m - 1;
+  }
+  return a;
+}
+
+// Nodes of the wave's panels: position, weight, pair, class.  One block per
+// panel (grid-stride over the wave's panels).
+template <int P>
+__global__ void __launch_bounds__(256)
+k_nodes(int np, int64_t lo, const double* __restrict__ obs, const SrcPrep* __restrict__ prep,
+        const int* __restrict__ st_src, const int* __restrict__ pair_st,
+        const int* __restrict__ pair_oc, const long long* __restrict__ pair_poff,
+        const double* __restrict__ pan_ra, const double* __restrict__ pan_rb,
+        const long long* __restrict__ pan_noff, Hdr* __restrict__ hdr,
+        double* __restrict__ npx, double* __restrict__ npy, double* __restrict__ nw,
+        int* __restrict__ npair, unsigned char* __restrict__ ncls) {
+  __shared__ AngRule A;
+  __shared__ FoldPair fp;
+  __shared__ int s_pair;
+  __shared__ int s_cnt[NCLS];
+  const long long q0 = hdr->wave_q0, q1 = hdr->wave_q1, n0 = hdr->wave_n0;
+  const double* gx6 = d_glx + gl_offset(cst::FOLD_N_RADIAL);
+  const double* gw6 = d_glw + gl_offset(cst::FOLD_N_RADIAL);
+  const double* gx4 = d_glx + gl_offset(cst::FOLD_N_ANGULAR);
+  const double* gw4 = d_glw + gl_offset(cst::FOLD_N_ANGULAR);
+  for (long long q = q0 + blockIdx.x; q < q1; q += gridDim.x) {
+    if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+      const int i = panel_pair(pair_poff, np, q);
+      const SrcPrep& sp = prep[st_src[pair_st[i]]];
+      FoldPair f;
+      pair_geom(obs, lo, pair_oc[i], sp, f);
+      fold_panel_rule(f, pan_ra[q], pan_rb[q], A);
+      fp = f;
+      s_pair = i;
+    }
+    __syncthreads();
+    const int i = s_pair;
+    const SrcPrep& sp = prep[st_src[pair_st[i]]];
+    const double ra = pan_ra[q], rb = pan_rb[q];
+    const int na = A.n;
+    const long long npts = (long long)cst::FOLD_N_RADIAL * (na > 0 ? na : 0);
+    const long long base = pan_noff[q] - n0;
+    for (long long t = threadIdx.x; t < npts; t += blockDim.x) {
+      const int ir = (int)(t / na), jn = (int)(t % na);
+      const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
+      const double wr = (rb - ra) * (0.5 * gw6[ir]);
+      double th, wt;
+      fold_ang_node(A, gx4, gw4, jn, &th, &wt);
+      double sn, cs;
+      sincos(th, &sn, &cs);
+      const double px = fp.xh0 + R * cs, py = fp.xh1 + R * sn;
+      int cls = surface_class(sp.f, px, py, sp.eps);
+      if (cls == SL_NEAR) {
+        const double xx[3] = {px, py, 0.0};
+        double z, X0, X1;
+        to_plane(sp.f, xx, z, X0, X1);
+        const double h2 = z * z + sp.eps * sp.eps;
+        double pr[3][2];
+        foot_vertices(sp.f, X0, X1, pr);
+        int ns = 0, nl = 0;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const EdgeGeom g = edge_geom_rcp(pr, e, h2);
+          const int form = edge_regime_sq(g.ua, g.ub, g.rho2);
+          ns += form == EDGE_SMALL;
+          nl += form == EDGE_LARGE;
+        }
+        cls = near_sig(ns, nl);
+      } else {
+        cls = cls == SL_FAR8 ? CLS_FAR8 : CLS_FAR12;
+      }
+      const long long u = base + t;
+      npx[u] = px;
+      npy[u] = py;
+      nw[u] = wr * wt * R;
+      npair[u] = i;
+      ncls[u] = (unsigned char)cls;
+      atomicAdd(&s_cnt[cls], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < NCLS && s_cnt[threadIdx.x])
+      atomicAdd(&hdr->cls_count[threadIdx.x], s_cnt[threadIdx.x]);
+    __syncthreads();
+  }
+}
+
+// Class offsets of the wave (and the census of its nodes and near edges).
+__global__ void k_wave_classes(Hdr* __restrict__ hdr, unsigned long long* __restrict__ census) {
+  long long off = 0;
+  for (int c = 0; c < NCLS; ++c) {
+    hdr->cls_off[c] = off;
+    off += hdr->cls_count[c];
+  }
+  hdr->cls_off[NCLS] = off;
+  if (census) {
+    unsigned long long near = 0, es = 0, el = 0, ec = 0;
+    for (int c = 0; c < 10; ++c) {
+      const unsigned long long n = (unsigned long long)hdr->cls_count[c];
+      near += n;
+      es += n * kSigSmall[c];
+      el += n * kSigLarge[c];
+      ec += n * (3 - kSigSmall[c] - kSigLarge[c]);
+    }
+    census[MHS_CENSUS_NEAR] += near;
+    census[MHS_CENSUS_FAR12] += (unsigned long long)hdr->cls_count[CLS_FAR12];
+    census[MHS_CENSUS_FAR8] += (unsigned long long)hdr->cls_count[CLS_FAR8];
+    census[MHS_CENSUS_EDGE_CLOSED] += ec;
+    census[MHS_CENSUS_EDGE_SMALL] += es;
+    census[MHS_CENSUS_EDGE_LARGE] += el;
+  }
+}
+
+// Node indices into their class lists (one thread per node; warp-aggregated
+// appends).
+__global__ void __launch_bounds__(256)
+k_scatter(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls, int* __restrict__ nlist) {
+  const long long n = hdr->wave_nodes;
+  const int lane = threadIdx.x & 31;
+  for (long long u0 = (long long)blockIdx.x * blockDim.x; u0 < n; u0 += (long long)gridDim.x * blockDim.x) {
+    const long long u = u0 + threadIdx.x;
+    const int cls = u < n ? ncls[u] : -1;
+#pragma unroll 1
+    for (int c = 0; c < NCLS; ++c) {
+      const unsigned m = __ballot_sync(0xffffffffu, cls == c);
+      if (!m) continue;
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(&hdr->cls_fill[c], __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (cls == c) nlist[hdr->cls_off[c] + base + __popc(m & ((1u << lane) - 1u))] = (int)u;
+    }
+  }
+}
+
+// Far loads: one thread per node of the far lists.
+template <int P, int KC, class RF>
+__global__ void __launch_bounds__(128)
+k_far(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* __restrict__ npx,
+      const double* __restrict__ npy, const int* __restrict__ npair,
+      const int* __restrict__ pair_st, int j0, const int* __restrict__ st_src,
+      const SrcPrep* __restrict__ prep, const Src<P, RF>* __restrict__ srcs,
+      double* __restrict__ load, long long cap) {
+  constexpr int K = n_nodes(P);
+  constexpr int NJ = 3 * K;
+  constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
+  const long long a = hdr->cls_off[CLS_FAR12], b = hdr->cls_off[CLS_FAR8 + 1];
+  for (long long e = a + (long long)blockIdx.x * blockDim.x + threadIdx.x; e < b;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int u = nlist[e];
+    const int j = pair_st[npair[u]];
+    const SrcPrep& sp = prep[st_src[j]];
+    const Src<P, RF>& d = srcs[j - j0];
+    const bool r8 = e >= hdr->cls_off[CLS_FAR8];
+    const double xx[3] = {npx[u], npy[u], 0.0};
+    double z, X0, X1;
+    to_plane(sp.f, xx, z, X0, X1);
+    double sl[NJ] = {};
+    if constexpr (std::is_same<RF, float>::value) {
+      const int off = r8 ? N12 : 0;
+      const QuadRuleT<float> q{r8 ? cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT : N12,
+                               d.fr.e0 + off, d.fr.e1 + off, d.fr.wq + off, d.fr.Nq + off * K};
+      surface_load_far<P, RF>(q, d.slc, z, X0, X1, z * z + sp.eps * sp.eps, sl);
+    } else {
+      surface_load_far<P, RF>(r8 ? d.rd.r8() : d.rd.r12(), d.slc, z, X0, X1,
+                              z * z + sp.eps * sp.eps, sl);
+    }
+#pragma unroll
+    for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sl[jj];
+  }
+}
+
+// Near loads: one thread per node of the near lists.  Every node of one
+// list has the same number of small-|u| and large-|u| edges, so a warp
+// (away from list boundaries) takes one path through the edge forms: its
+// edges are visited small-series ones first, then large-series ones, then
+// closed-form ones.
+template <int P, int KC>
+__global__ void __launch_bounds__(128, P == 0 ? 4 : 1)
+k_near(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* __restrict__ npx,
+       const double* __restrict__ npy, const int* __restrict__ npair,
+       const int* __restrict__ pair_st, int j0, const int* __restrict__ st_src,
+       const SrcPrep* __restrict__ prep, const SurfaceLoadConsts* __restrict__ slcs,
+       long long slc_stride, double* __restrict__ load, long long cap) {
+  using S = SurfaceSpec<P>;
+  constexpr Spec spc = S::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NJ = 3 * K;
+  constexpr int NB = spc.b_off[MS] > 0 ? spc.b_off[MS] : 1;
+  const long long a = hdr->cls_off[0], b = hdr->cls_off[10];
+  for (long long e = a + (long long)blockIdx.x * blockDim.x + threadIdx.x; e < b;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int u = nlist[e];
+    const int j = pair_st[npair[u]];
+    const SrcPrep& sp = prep[st_src[j]];
+    const SurfaceLoadConsts& c =
+        *reinterpret_cast<const SurfaceLoadConsts*>(reinterpret_cast<const char*>(slcs) +
+                                                    (size_t)(j - j0) * slc_stride);
+    const double eps = sp.eps;
+    const double xx[3] = {npx[u], npy[u], 0.0};
+    double z, X0, X1;
+    to_plane(sp.f, xx, z, X0, X1);
+    const double h2 = z * z + eps * eps;
+    double pr[3][2];
+    foot_vertices(sp.f, X0, X1, pr);
+    // edge slots ordered small-series, large-series, closed; the form of
+    // position i depends only on the node's list, so it is warp-uniform
+    EdgeGeom g[3];
+    int form[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      g[k] = edge_geom_rcp(pr, k, h2);
+      form[k] = edge_regime_sq(g[k].ua, g[k].ub, g[k].rho2);
+    }
+    int order[3] = {0, 0, 0}, no = 0;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const int want = f == 0 ? EDGE_SMALL : (f == 1 ? EDGE_LARGE : EDGE_CLOSED);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const bool hit = form[k] == want;
+        // branch-free append: positions 0..2 as selects
+        order[0] = (hit && no == 0) ? k : order[0];
+        order[1] = (hit && no == 1) ? k : order[1];
+        order[2] = (hit && no == 2) ? k : order[2];
+        no += hit ? 1 : 0;
+      }
+    }
+    const int ns = (form[0] == EDGE_SMALL) + (form[1] == EDGE_SMALL) + (form[2] == EDGE_SMALL);
+    const int nl = (form[0] == EDGE_LARGE) + (form[1] == EDGE_LARGE) + (form[2] == EDGE_LARGE);
+    double BN1[NB], BN2[NB], BD[MS];
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      BN1[t] = 0.0;
+      BN2[t] = 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < MS; ++t) BD[t] = 0.0;
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+      const int k = i == 0 ? order[0] : (i == 1 ? order[1] : order[2]);
+      const EdgeGeom ge = k == 0 ? g[0] : (k == 1 ? g[1] : g[2]);
+      double Pt[MS][8];
+      if (i < ns) edge_small<S>(ge.ua, ge.ub, sqrt(ge.rho2), Pt);
+      else if (i < ns + nl) edge_large<S>(ge.ua, ge.ub, ge.rho2, Pt);
+      else edge_closed<S, true>(ge.ua, ge.ub, ge.rho2, Pt);
+      edge_accumulate<S>(ge, Pt, BN1, BN2, BD);
+    }
+    MomentTable<S> T;
+    closed_finish_t<S, true>(pr, h2, BN1, BN2, BD, T);
+    double sl[NJ] = {};
+    surface_load_near<P>(sp.f, T, c, z, X0, X1, sl);
+#pragma unroll
+    for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sl[jj];
+  }
+}
+
+// Accumulation of the wave: one warp per pair with panels in the wave,
+// panel by panel in grid order.  The lanes form G groups; group g holds the
+// load components jj in [g * NJG, (g + 1) * NJG) of all NC point-load
+// components and strides over the panel's nodes; each panel's partial sums
+// are reduced across the group in a fixed tree and added, in panel order,
+// to the pair's running sums acc[pair][c * NJ + jj].
+template <int P, int KC>
+struct AccumShape {
+  static constexpr int K = n_nodes(P);
+  static constexpr int NJ = 3 * K;
+  static constexpr int NC = KC == KD_HE ? 6 : 3;
+  static constexpr int G = NJ * NC > 60 ? 2 : 1;    // lane groups
+  static constexpr int NJG = (NJ + G - 1) / G;
+  static constexpr int LANES = 32 / G;
+  static constexpr int NOUT = NC * NJ;
+};
+
+template <int P, int KC>
+__global__ void __launch_bounds__(128)
+k_accum(int np, int64_t lo, const double* __restrict__ obs, const SrcPrep* __restrict__ prep,
+        const int* __restrict__ st_src, const int* __restrict__ pair_st,
+        const int* __restrict__ pair_oc, const long long* __restrict__ pair_poff,
+        const long long* __restrict__ pan_noff, const Hdr* __restrict__ hdr,
+        const double* __restrict__ npx, const double* __restrict__ npy,
+        const double* __restrict__ nw, const double* __restrict__ load, long long cap,
+        const double* __restrict__ foot, double mu, double lam, double* __restrict__ acc) {
+  using A = AccumShape<P, KC>;
+  constexpr int NJ = A::NJ, NC = A::NC, NJG = A::NJG, LANES = A::LANES;
+  const Material m = make_material(mu, lam);
+  const long long q0 = hdr->wave_q0, q1 = hdr->wave_q1, n0 = hdr->wave_n0;
+  if (q1 <= q0) return;
+  const int pa = panel_pair(pair_poff, np, q0), pb = panel_pair(pair_poff, np, q1 - 1);
+  const int lane = threadIdx.x & 31, grp = lane / LANES, gl = lane % LANES;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = pa + warp; i <= pb; i += nwarps) {
+    const SrcPrep& sp = prep[st_src[pair_st[i]]];
+    const int64_t o = lo + pair_oc[i];
+    const double xh0 = obs[3 * o], xh1 = obs[3 * o + 1];
+    const double zeta = -obs[3 * o + 2] > 0.0 ? -obs[3 * o + 2] : 0.0;
+    (void)sp;
+    double sh[NJG];
+#pragma unroll
+    for (int t = 0; t < NJG; ++t) {
+      const int jj = grp * NJG + t;
+      sh[t] = jj < NJ ? foot[(size_t)i * NJ + jj] : 0.0;
+    }
+    double run[NC][NJG];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int t = 0; t < NJG; ++t) {
+        const int jj = grp * NJG + t;
+        run[c][t] = jj < NJ ? acc[(size_t)i * A::NOUT + c * NJ + jj] : 0.0;
+      }
+    const long long qa = pair_poff[i] > q0 ? pair_poff[i] : q0;
+    const long long qb = pair_poff[i + 1] < q1 ? pair_poff[i + 1] : q1;
+    for (long long q = qa; q < qb; ++q) {
+      double part[NC][NJG];
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int t = 0; t < NJG; ++t) part[c][t] = 0.0;
+      const long long ua = pan_noff[q] - n0, ub = pan_noff[q + 1] - n0;
+      for (long long u = ua + gl; u < ub; u += LANES) {
+        const double px = npx[u], py = npy[u], w = nw[u];
+        double Bv[NC];
+        if constexpr (KC == KD_HE) point_stress6(xh0 - px, xh1 - py, zeta, m.nu_f, Bv);
+        else point_disp3(xh0 - px, xh1 - py, zeta, m.mu, m.nu_f, Bv);
+#pragma unroll
+        for (int t = 0; t < NJG; ++t) {
+          const int jj = grp * NJG + t;
+          if (jj < NJ) {
+            const double sv = load[(size_t)jj * cap + u] - sh[t];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) part[c][t] += (w * Bv[c]) * sv;
+          }
+        }
+      }
+      // tree reduction across the LANES lanes of each group
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int t = 0; t < NJG; ++t) {
+          double v = part[c][t];
+#pragma unroll
+          for (int d = LANES / 2; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+          run[c][t] += v;
+        }
+    }
+    if (gl == 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int t = 0; t < NJG; ++t) {
+          const int jj = grp * NJG + t;
+          if (jj < NJ) acc[(size_t)i * A::NOUT + c * NJ + jj] = run[c][t];
+        }
+    }
+  }
+}
+
+// Per pair: the disk term of the grid's outer radius and the add into the
+// pair's table row.
+template <int P, int KC>
+__global__ void __launch_bounds__(128)
+k_finish(int np, int64_t lo, int64_t n_src, const double* __restrict__ obs,
+         const SrcPrep* __restrict__ prep, const int* __restrict__ st_src,
+         const int* __restrict__ pair_st, const int* __restrict__ pair_oc,
+         const double* __restrict__ foot, const double* __restrict__ acc, double mu, double lam,
+         double* __restrict__ T) {
+  using A = AccumShape<P, KC>;
+  constexpr int K = n_nodes(P), NJ = A::NJ;
+  constexpr int NR = row_of(KC);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int s = st_src[pair_st[i]];
+  const SrcPrep& sp = prep[s];
+  const int oc = pair_oc[i];
+  FoldPair fp;
+  pair_geom(obs, lo, oc, sp, fp);
+  double br[FOLD_MAX_BREAKS];
+  double R1 = 0.0;
+  if (fold_breaks(fp.rho_s, fp.zeta, sp.r_f, sp.eps, sp.diam, br, &R1) < 0) return;
+  const Material m = make_material(mu, lam);
+  const double* a = acc + (size_t)i * A::NOUT;
+  const double* sh = foot + (size_t)i * NJ;
+  double* row = T + (((int64_t)oc * n_src + s) * K) * NR;
+  if constexpr (KC == KD_HE) {
+    double srr, szz;
+    disk_stress(R1, fp.zeta, m.nu_f, &srr, &szz);
+    const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    for (int k = 0; k < K; ++k)
+      for (int mm = 0; mm < 3; ++mm) {
+        double Hb[3][3];
+        for (int c = 0; c < 6; ++c) {
+          const double v = a[c * NJ + 3 * k + mm];
+          Hb[ia[c]][ib[c]] = v;
+          Hb[ib[c]][ia[c]] = v;
+        }
+        const double shv = sh[3 * k + mm];
+        Hb[0][0] += shv * srr;
+        Hb[1][1] += shv * srr;
+        Hb[2][2] += shv * szz;
+        for (int aa = 0; aa < 3; ++aa)
+          for (int b = 0; b < 3; ++b) row[k * NR + 9 * aa + 3 * b + mm] += Hb[aa][b];
+      }
+  } else {
+    const double uz = disk_disp_z(R1, fp.zeta, m.mu, m.nu_f);
+    for (int k = 0; k < K; ++k)
+      for (int mm = 0; mm < 3; ++mm)
+        for (int ii = 0; ii < 3; ++ii)
+          row[k * NR + 3 * ii + mm] += a[ii * NJ + 3 * k + mm] +
+                                       (ii == 2 ? sh[3 * k + mm] * uz : 0.0);
+  }
+}
+
+__global__ void k_zero(double* __restrict__ a, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] = 0.0;
+}
+
+__global__ void k_census_pairs(const Hdr* __restrict__ hdr, unsigned long long* __restrict__ census,
+                               int np) {
+  census[MHS_CENSUS_PAIRS] += (unsigned long long)np;
+  census[MHS_CENSUS_PANELS] += (unsigned long long)hdr->q_batch;
+}
+
+}  // namespace fold_waves
+
+namespace fold_waves {
+
+// Bytes of the fold region's parts.
+template <int P, int KC, class RF>
+struct Sizes {
+  static constexpr int K = n_nodes(P), NJ = 3 * K;
+  static constexpr int NOUT = AccumShape<P, KC>::NOUT;
+  static constexpr size_t per_src = sizeof(Src<P, RF>);
+  // pair_st, pair_oc (int), pair_poff, pair_noff (scan input and output,
+  // one more entry), foot (NJ), acc (NOUT)
+  static constexpr size_t per_pair = 4 + 4 + 8 + 8 + 8 * NJ + 8 * NOUT;
+  static constexpr size_t per_panel = 8 + 8 + 8;          // ra, rb, first node
+  static constexpr size_t per_node = 8 * 3 + 4 + 1 + 4 + 8 * NJ;
+};
+
+inline size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// The fold of one observer chunk: plan, then batches of band pairs, each
+// in waves of whole panels.  Returns an MHS status code.
+template <int P, int KC, class RF>
+int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_bytes,
+             int64_t lo, int64_t nc, const SrcPrep* prep, const int* cnt, const int* list,
+             double* T, int* status, unsigned long long* census) {
+  using Z = Sizes<P, KC, RF>;
+  constexpr int NJ = Z::NJ;
+  constexpr int NOUT = Z::NOUT;
+  const int64_t n_src = r->n_src;
+  int dev = 0, sms = 0;
+  MHS_CUDA_TRY(cudaGetDevice(&dev));
+  MHS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // fixed part: header and the straddler tables
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    char* p = region + off;
+    off = up256(off + bytes);
+    return p;
+  };
+  Hdr* hdr = (Hdr*)carve(sizeof(Hdr));
+  int* st_rank = (int*)carve(sizeof(int) * n_src);
+  int* st_src = (int*)carve(sizeof(int) * n_src);
+  long long* st_off = (long long*)carve(sizeof(long long) * (n_src + 1));
+  if (off >= region_bytes)
+    return fail(MHS_ERR_WORKSPACE, "fold region of %zu bytes below its fixed part", region_bytes);
+  MHS_CUDA_TRY(cudaMemsetAsync(hdr, 0, sizeof(Hdr), st));
+  k_band_scan<<<1, 1024, 0, st>>>(n_src, prep, cnt, st_rank, st_src, st_off, hdr);
+  Hdr h;
+  MHS_CUDA_TRY(cudaMemcpyAsync(&h, hdr, sizeof(Hdr), cudaMemcpyDeviceToHost, st));
+  MHS_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h.n_pairs == 0) return MHS_OK;
+  std::vector<long long> so((size_t)h.n_st + 1);
+  MHS_CUDA_TRY(cudaMemcpyAsync(so.data(), st_off, sizeof(long long) * so.size(),
+                               cudaMemcpyDeviceToHost, st));
+  MHS_CUDA_TRY(cudaStreamSynchronize(st));
+  // budgets of the variable part
+  const size_t rest = region_bytes - off;
+  const size_t b_src = rest / 10, b_pair = rest * 3 / 20, b_pan = rest * 3 / 20;
+  const size_t b_node = rest - b_src - b_pair - b_pan - 8 * 256;
+  const long long cap_src = (long long)(b_src / Z::per_src);
+  const long long cap_pair = (long long)(b_pair / Z::per_pair) - 2;
+  const long long cap_pan = (long long)(b_pan / Z::per_panel) - 2;
+  const long long cap_node = (long long)(b_node / Z::per_node);
+  if (cap_src < 1 || cap_pair < 1 || cap_pan < 1 || cap_node < 1)
+    return fail(MHS_ERR_WORKSPACE, "fold region of %zu bytes too small for one pair", region_bytes);
+  Src<P, RF>* srcs = (Src<P, RF>*)carve(Z::per_src * cap_src);
+  int* pair_st = (int*)carve(4 * cap_pair);
+  int* pair_oc = (int*)carve(4 * cap_pair);
+  long long* pair_poff = (long long*)carve(8 * (cap_pair + 1));
+  long long* pair_noff = (long long*)carve(8 * (cap_pair + 1));
+  double* foot = (double*)carve(8 * NJ * cap_pair);
+  double* acc = (double*)carve(8 * NOUT * cap_pair);
+  double* pan_ra = (double*)carve(8 * cap_pan);
+  double* pan_rb = (double*)carve(8 * cap_pan);
+  long long* pan_noff = (long long*)carve(8 * (cap_pan + 1));
+  double* npx = (double*)carve(8 * cap_node);
+  double* npy = (double*)carve(8 * cap_node);
+  double* nw = (double*)carve(8 * cap_node);
+  int* npair = (int*)carve(4 * cap_node);
+  unsigned char* ncls = (unsigned char*)carve(cap_node);
+  int* nlist = (int*)carve(4 * cap_node);
+  double* load = (double*)carve(8 * NJ * cap_node);
+  if (off > region_bytes) return fail(MHS_ERR_WORKSPACE, "fold region carve-up overflow");
+  const SurfaceLoadConsts* slcs = &srcs[0].slc;
+  // grid sizes of the grid-stride kernels
+  int occ_far = 1, occ_near = 1, occ_nodes = 1;
+  MHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_far, k_far<P, KC, RF>, 128, 0));
+  MHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_near, k_near<P, KC>, 128, 0));
+  MHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_nodes, k_nodes<P>, 256, 0));
+  const int g_far = sms * (occ_far > 0 ? occ_far : 1) * 4;
+  const int g_near = sms * (occ_near > 0 ? occ_near : 1) * 4;
+  const int g_nodes = sms * (occ_nodes > 0 ? occ_nodes : 1) * 2;
+  const int g_scatter = sms * 8;
+  long long p0 = 0;
+  long long batch = cap_pair;
+  while (p0 < h.n_pairs) {
+    long long p1 = std::min<long long>(h.n_pairs, p0 + batch);
+    // straddlers the batch touches, within the source-data capacity
+    auto strad = [&](long long p) {  // straddle rank of pair p
+      return (long long)(std::upper_bound(so.begin(), so.end(), p) - so.begin()) - 1;
+    };
+    const long long j0 = strad(p0);
+    if (strad(p1 - 1) - j0 + 1 > cap_src) p1 = std::max<long long>(p0 + 1, so[j0 + cap_src]);
+    const int np = (int)(p1 - p0);
+    const long long j1 = strad(p1 - 1) + 1;
+    MHS_CUDA_TRY(cudaMemsetAsync(&hdr->max_panel, 0, sizeof(long long), st));
+    k_pairs<<<(np + 127) / 128, 128, 0, st>>>(p0, np, lo, nc, r->obs, prep, list, st_src, st_off,
+                                              hdr, pair_st, pair_oc, pair_poff, pair_noff, status);
+    k_scan<<<1, 1024, 0, st>>>(pair_poff, np, &hdr->q_batch, nullptr);
+    k_scan<<<1, 1024, 0, st>>>(pair_noff, np, &hdr->n_batch, nullptr);
+    MHS_CUDA_TRY(cudaMemcpyAsync(&h, hdr, sizeof(Hdr), cudaMemcpyDeviceToHost, st));
+    MHS_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h.q_batch > cap_pan) {
+      if (np == 1)
+        return fail(MHS_ERR_WORKSPACE, "one fold pair has %lld panels, above the fold region's "
+                    "%lld", h.q_batch, cap_pan);
+      batch = std::max<long long>(1, np / 2);
+      continue;
+    }
+    if (h.max_panel > cap_node / 2)
+      return fail(MHS_ERR_WORKSPACE, "a fold panel of %lld nodes does not fit the fold "
+                  "region's %lld-node waves", h.max_panel, cap_node);
+    const long long nq = h.q_batch, nn = h.n_batch;
+    k_src<P, KC, RF><<<(unsigned)(j1 - j0), 128, 0, st>>>((int)j0, (int)(j1 - j0), st_src, prep,
+                                                          r->mu, r->lam, srcs);
+    k_panels<<<(np + 1 + 127) / 128, 128, 0, st>>>(np, lo, r->obs, prep, st_src, pair_st, pair_oc,
+                                                   pair_poff, pair_noff, pan_ra, pan_rb, pan_noff);
+    k_foot<P, KC, RF><<<(np + 127) / 128, 128, 0, st>>>(np, (int)j0, lo, r->obs, prep, st_src,
+                                                        pair_st, pair_oc, srcs, foot);
+    k_zero<<<sms * 4, 256, 0, st>>>(acc, (long long)np * NOUT);
+    if (census) k_census_pairs<<<1, 1, 0, st>>>(hdr, census, np);
+    const long long span = cap_node - h.max_panel;
+    const long long waves = (nn + span - 1) / span;
+    for (long long w = 0; w < waves; ++w) {
+      k_wave_begin<<<1, 1, 0, st>>>(w, span, nq, pan_noff, hdr);
+      k_nodes<P><<<g_nodes, 256, 0, st>>>(np, lo, r->obs, prep, st_src, pair_st, pair_oc,
+                                          pair_poff, pan_ra, pan_rb, pan_noff, hdr, npx, npy, nw,
+                                          npair, ncls);
+      k_wave_classes<<<1, 1, 0, st>>>(hdr, census);
+      k_scatter<<<g_scatter, 256, 0, st>>>(hdr, ncls, nlist);
+      k_far<P, KC, RF><<<g_far, 128, 0, st>>>(hdr, nlist, npx, npy, npair, pair_st, (int)j0,
+                                              st_src, prep, srcs, load, cap_node);
+      k_near<P, KC><<<g_near, 128, 0, st>>>(hdr, nlist, npx, npy, npair, pair_st, (int)j0, st_src,
+                                            prep, slcs, (long long)sizeof(Src<P, RF>), load,
+                                            cap_node);
+      k_accum<P, KC><<<(np + 3) / 4 < sms * 16 ? (np + 3) / 4 : sms * 16, 128, 0, st>>>(
+          np, lo, r->obs, prep, st_src, pair_st, pair_oc, pair_poff, pan_noff, hdr, npx, npy, nw,
+          load, cap_node, foot, r->mu, r->lam, acc);
+    }
+    k_finish<P, KC><<<(np + 127) / 128, 128, 0, st>>>(np, lo, n_src, r->obs, prep, st_src,
+                                                      pair_st, pair_oc, foot, acc, r->mu, r->lam, T);
+    MHS_CUDA_TRY(cudaGetLastError());
+    p0 = p1;
+    batch = cap_pair;
+  }
+  return MHS_OK;
+}
+
+}  // namespace fold_waves

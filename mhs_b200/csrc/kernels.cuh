@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <vector>
 
 #include "pipeline.cuh"
 
@@ -366,375 +367,6 @@ k_band(int64_t lo, int64_t n_chunk, const double* __restrict__ obs,
   if (threadIdx.x == 0) cnt[s] = base;
 }
 
-// ---------------------------------------------------------------- k_fold
-// Work census (measurement only): pairs, panels, nodes per class, near
-// edges per form; counted when the kernel is given a non-null pointer.
-
-// Grid nodes are processed in pages of FOLD_PAGE.  Each page is split by
-// surface-load class (closed form, 12 x 12 rule, 8 x 8 rule) and every
-// 32-node batch of one class runs one code path; the edges of a batch of
-// near nodes are sorted again by edge form (closed, small-|u| series,
-// large-|u| series) before their integrals are taken.  The weighted
-// point-load products are then summed in grid order, 32 nodes at a time.
-constexpr int FOLD_PAGE = 128;
-constexpr int FOLD_WARPS = 4;    // band pairs per fold block (one source)
-
-// Packed size of one edge's integrals P[j][0..edge[j]].
-MHS_FI constexpr int edge_pack_size(const Spec& sp) {
-  int o = 0;
-  for (int j = 0; j < MS; ++j) o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
-  return o;
-}
-
-template <int P, int KC>
-struct FoldWarp {
-  static constexpr int K = n_nodes(P);
-  static constexpr int NC = KC == KD_HE ? 6 : 3;
-  static constexpr int NJ = 3 * K;
-  static constexpr int NP = edge_pack_size(SurfaceSpec<P>::spec);
-  double px[FOLD_PAGE], py[FOLD_PAGE], wt[FOLD_PAGE];
-  double sS[FOLD_PAGE][NJ + 1];      // load minus the load at the foot
-  union {
-    struct {
-      double eu[96][3];              // (ua, ub, rho2) of one near batch's edges (node * 3 + e)
-      double eP[96][NP];             // their packed integrals
-    } edge;
-    double sB[32][NC + 1];           // weighted point-load tensor (after the loads)
-  };
-  unsigned char list[3][FOLD_PAGE];  // page nodes per class
-  unsigned char elist[3][96];        // batch edges per form
-  double brk[FOLD_MAX_BREAKS];
-  double sh_load[NJ];
-  double outv[NC * NJ];
-  double R1;
-  int nbrk;
-};
-
-template <int P, int KC, class RF>
-struct FoldShared {
-  SrcPrep sp;
-  SmemRules<P> rd;       // element (surface load)
-  SurfaceLoadConsts slc; // sigma_zz row of the element's H, per slip component
-  std::conditional_t<std::is_same<RF, float>::value, FloatRules<P>, NoRules> fr;
-  FoldWarp<P, KC> w[FOLD_WARPS];
-};
-
-// Append `val` to `list` for every lane where pred holds, in lane order.
-__device__ __forceinline__ void warp_append(bool pred, int val, unsigned char* list, int& count,
-                                            int lane) {
-  const unsigned mask = __ballot_sync(0xffffffffu, pred);
-  if (pred) list[count + __popc(mask & ((1u << lane) - 1u))] = (unsigned char)val;
-  count += __popc(mask);
-}
-
-// Surface loads of the near nodes list[0..n) of a page into W.sS.
-template <int P, int KC>
-__device__ void fold_near_batch(FoldWarp<P, KC>& W, const Frame& f, const SurfaceLoadConsts& c,
-                                double eps, int n, int lane, unsigned long long* census) {
-  using S = SurfaceSpec<P>;
-  constexpr Spec sp = S::spec;
-  constexpr int K = n_nodes(P);
-  constexpr int NJ = 3 * K;
-  constexpr int NB = sp.b_off[MS] > 0 ? sp.b_off[MS] : 1;
-  for (int b = 0; b < n; b += 32) {
-    const int i = b + lane;
-    const bool active = i < n;
-    const int u = active ? W.list[SL_NEAR][i] : 0;
-    double z = 0.0, X0 = 0.0, X1 = 0.0, h2 = 1.0;
-    double pr[3][2] = {};
-    int cnt[3] = {0, 0, 0};
-    if (active) {
-      const double x[3] = {W.px[u], W.py[u], 0.0};
-      to_plane(f, x, z, X0, X1);
-      h2 = z * z + eps * eps;
-      foot_vertices(f, X0, X1, pr);
-    }
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-      int form = -1;
-      if (active) {
-        const EdgeGeom g = edge_geom_rcp(pr, e, h2);
-        W.edge.eu[3 * lane + e][0] = g.ua;
-        W.edge.eu[3 * lane + e][1] = g.ub;
-        W.edge.eu[3 * lane + e][2] = g.rho2;
-        form = edge_regime_sq(g.ua, g.ub, g.rho2);
-      }
-#pragma unroll
-      for (int r = 0; r < 3; ++r) warp_append(form == r, 3 * lane + e, W.elist[r], cnt[r], lane);
-    }
-    if (census && lane == 0)
-      for (int r = 0; r < 3; ++r)
-        atomicAdd(census + MHS_CENSUS_EDGE_CLOSED + r, (unsigned long long)cnt[r]);
-    __syncwarp();
-    // edge integrals, one form per pass
-#pragma unroll 1
-    for (int r = 0; r < 3; ++r) {
-      for (int q = 0; q < cnt[r]; q += 32) {
-        if (q + lane < cnt[r]) {
-          const int slot = W.elist[r][q + lane];
-          const double ua = W.edge.eu[slot][0], ub = W.edge.eu[slot][1], rho2 = W.edge.eu[slot][2];
-          double Pt[MS][8];
-          if (r == EDGE_CLOSED) edge_closed<S, true>(ua, ub, rho2, Pt);
-          else if (r == EDGE_SMALL) edge_small<S>(ua, ub, sqrt(rho2), Pt);
-          else edge_large<S>(ua, ub, rho2, Pt);
-          int o = 0;
-#pragma unroll
-          for (int j = 0; j < MS; ++j) {
-#pragma unroll
-            for (int k = 0; k <= sp.edge[j]; ++k) W.edge.eP[slot][o + k] = Pt[j][k];
-            o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
-          }
-        }
-      }
-    }
-    __syncwarp();
-    if (active) {
-      double BN1[NB], BN2[NB], BD[MS];
-#pragma unroll
-      for (int t = 0; t < NB; ++t) {
-        BN1[t] = 0.0;
-        BN2[t] = 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < MS; ++j) BD[j] = 0.0;
-#pragma unroll 1
-      for (int e = 0; e < 3; ++e) {
-        const int slot = 3 * lane + e;
-        const EdgeGeom g = edge_geom_rcp(pr, e, h2);   // as in the pass above
-        double Pt[MS][8] = {};
-        int o = 0;
-#pragma unroll
-        for (int j = 0; j < MS; ++j) {
-#pragma unroll
-          for (int k = 0; k <= sp.edge[j]; ++k) Pt[j][k] = W.edge.eP[slot][o + k];
-          o += sp.edge[j] >= 0 ? sp.edge[j] + 1 : 0;
-        }
-        edge_accumulate<S>(g, Pt, BN1, BN2, BD);
-      }
-      MomentTable<S> T;
-      closed_finish_t<S, true>(pr, h2, BN1, BN2, BD, T);
-      double sl[NJ] = {};
-      surface_load_near<P>(f, T, c, z, X0, X1, sl);
-#pragma unroll
-      for (int jj = 0; jj < NJ; ++jj) W.sS[u][jj] = sl[jj] - W.sh_load[jj];
-    }
-    __syncwarp();
-  }
-}
-
-// One warp per band pair.
-template <int P, int KC, class RF>
-__global__ void __launch_bounds__(32 * FOLD_WARPS)
-k_fold(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
-       const SrcPrep* __restrict__ prep, const int* __restrict__ cnt,
-       const int* __restrict__ list, double mu, double lam, double* __restrict__ T,
-       int* __restrict__ status, unsigned long long* __restrict__ census) {
-  constexpr int K = n_nodes(P);
-  constexpr int NR = row_of(KC);
-  constexpr int C = comps_of(KC);
-  constexpr bool WH = KC == KD_HE;
-  constexpr int NC = WH ? 6 : 3;          // point-load components
-  constexpr int NJ = 3 * K;               // load components (node x slip)
-  constexpr int NOUT = NC * NJ;
-  constexpr int PER_LANE = (NOUT + 31) / 32;
-  const int64_t s = blockIdx.x;
-  const int n_band = cnt[s];
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if ((int64_t)blockIdx.y * FOLD_WARPS >= n_band) return;
-  extern __shared__ __align__(16) unsigned char fold_smem[];
-  FoldShared<P, KC, RF>& sh = *reinterpret_cast<FoldShared<P, KC, RF>*>(fold_smem);
-  SrcPrep& sp = sh.sp;
-  SmemRules<P>& rd = sh.rd;
-  FoldWarp<P, KC>& W = sh.w[wid];
-  const Material m = make_material(mu, lam);
-  if (threadIdx.x == 0) sp = prep[s];
-  __syncthreads();
-  rd.build(sp.f, threadIdx.x, 32 * FOLD_WARPS);
-  {
-    static_assert(NLIFT <= 32 * FOLD_WARPS, "one thread per lifted slot");
-    if (threadIdx.x < NLIFT) {
-      double col[3] = {};
-      szz_coefficient(sp.f, sp.eps, m, threadIdx.x, col);
-      for (int j = 0; j < 3; ++j) sh.slc.coef[j][threadIdx.x] = col[j];
-    }
-    if (threadIdx.x == 32) surface_load_ezz(sp.f, sp.eps, m, sh.slc);
-  }
-  __syncthreads();
-  if constexpr (std::is_same<RF, float>::value) {
-    float_rules<P>(rd, sh.fr, threadIdx.x, 32 * FOLD_WARPS);
-    __syncthreads();
-  }
-  const int bi = blockIdx.y * FOLD_WARPS + wid;
-  if (bi >= n_band) return;
-  const int64_t oc = list[s * n_chunk + bi];
-  const int64_t o = lo + oc;
-  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const double eps = sp.eps;
-  double* row = T + ((oc * n_src + s) * K) * NR;
-  const QuadRule r12 = rd.r12(), r8 = rd.r8();
-  static_assert(KC != KD_E, "the eigen-only readout has no Boussinesq term");
-  {
-    const SurfaceLoadConsts& slc = sh.slc;
-    FoldPair fp;
-    fold_pair_setup(x, sp.centre, sp.r_f, eps, fp);
-    if (lane == 0) {
-      double R1;
-      W.nbrk = fold_breaks(fp.rho_s, fp.zeta, sp.r_f, eps, sp.diam, W.brk, &R1);
-      if (census) atomicAdd(census + MHS_CENSUS_PAIRS, 1ull);
-      W.R1 = R1;
-      double sl[NJ] = {};
-      fold_surface_load_fast<P, RF>(sp.f, r12, r8, slc, x[0], x[1], eps, sl);
-      for (int j = 0; j < NJ; ++j) W.sh_load[j] = sl[j];
-    }
-    __syncwarp();
-    const int nb = W.nbrk;
-    if (nb < 0) {
-      if (lane == 0) atomic_status(status, MHS_DEV_FOLD_GRID_OVERFLOW);
-      return;
-    }
-    fp.R1 = W.R1;
-    const double* gx6 = d_glx + gl_offset(cst::FOLD_N_RADIAL);
-    const double* gw6 = d_glw + gl_offset(cst::FOLD_N_RADIAL);
-    const double* gx4 = d_glx + gl_offset(cst::FOLD_N_ANGULAR);
-    const double* gw4 = d_glw + gl_offset(cst::FOLD_N_ANGULAR);
-    double acc[PER_LANE];
-#pragma unroll
-    for (int i = 0; i < PER_LANE; ++i) acc[i] = 0.0;
-    for (int pi = 0; pi + 1 < nb; ++pi) {
-      const double ra = W.brk[pi], rb = W.brk[pi + 1];
-      if (rb - ra < 1e-9 * eps) continue;
-      AngRule A;
-      fold_panel_rule(fp, ra, rb, A);
-      if (A.n < 0) {  // uniform across the warp: every lane built the same rule
-        if (lane == 0) atomic_status(status, MHS_DEV_FOLD_GRID_OVERFLOW);
-        return;
-      }
-      const int npts = cst::FOLD_N_RADIAL * A.n;
-      if (census && lane == 0) atomicAdd(census + MHS_CENSUS_PANELS, 1ull);
-      for (int p0 = 0; p0 < npts; p0 += FOLD_PAGE) {
-        const int np = min(FOLD_PAGE, npts - p0);
-        // nodes of the page and their classes
-        int ncls[3] = {0, 0, 0};
-#pragma unroll
-        for (int r = 0; r < FOLD_PAGE / 32; ++r) {
-          const int u = 32 * r + lane;
-          int cls = -1;
-          if (u < np) {
-            const int t = p0 + u;
-            const int ir = t / A.n, j = t % A.n;
-            const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
-            const double wr = (rb - ra) * (0.5 * gw6[ir]);
-            double th, wt;
-            fold_ang_node(A, gx4, gw4, j, &th, &wt);
-            double sn, cs;
-            sincos(th, &sn, &cs);
-            const double px = fp.xh0 + R * cs, py = fp.xh1 + R * sn;
-            W.px[u] = px;
-            W.py[u] = py;
-            W.wt[u] = wr * wt * R;
-            cls = surface_class(sp.f, px, py, eps);
-          }
-#pragma unroll
-          for (int c = 0; c < 3; ++c) warp_append(cls == c, u, W.list[c], ncls[c], lane);
-        }
-        if (census && lane == 0)
-          for (int c = 0; c < 3; ++c)
-            atomicAdd(census + MHS_CENSUS_NEAR + c, (unsigned long long)ncls[c]);
-        __syncwarp();
-        // far loads
-#pragma unroll 1
-        for (int c = SL_FAR12; c <= SL_FAR8; ++c) {
-          constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
-          const QuadRule& qd = c == SL_FAR8 ? r8 : r12;
-          QuadRuleT<RF> q;
-          if constexpr (std::is_same<RF, float>::value) {
-            const int off = c == SL_FAR8 ? N12 : 0;
-            q = QuadRuleT<float>{qd.nq, sh.fr.e0 + off, sh.fr.e1 + off, sh.fr.wq + off,
-                                 sh.fr.Nq + off * K};
-          } else {
-            q = qd;
-          }
-          for (int b = 0; b < ncls[c]; b += 32) {
-            if (b + lane < ncls[c]) {
-              const int u = W.list[c][b + lane];
-              const double xx[3] = {W.px[u], W.py[u], 0.0};
-              double z, X0, X1;
-              to_plane(sp.f, xx, z, X0, X1);
-              double sl[NJ] = {};
-              surface_load_far<P, RF>(q, slc, z, X0, X1, z * z + eps * eps, sl);
-#pragma unroll
-              for (int jj = 0; jj < NJ; ++jj) W.sS[u][jj] = sl[jj] - W.sh_load[jj];
-            }
-          }
-        }
-        // near loads
-        fold_near_batch<P, KC>(W, sp.f, slc, eps, ncls[SL_NEAR], lane, census);
-        __syncwarp();
-        // weighted point loads and the ordered sum, 32 nodes at a time
-        for (int c0 = 0; c0 < np; c0 += 32) {
-          const int u = c0 + lane;
-          if (u < np) {
-            const double px = W.px[u], py = W.py[u], w = W.wt[u];
-            double Bv[NC] = {};
-            if (WH) point_stress6(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.nu_f, Bv);
-            else point_disp3(fp.xh0 - px, fp.xh1 - py, fp.zeta, m.mu, m.nu_f, Bv);
-            for (int c = 0; c < NC; ++c) W.sB[lane][c] = w * Bv[c];
-          }
-          __syncwarp();
-          const int nvalid = min(32, np - c0);
-#pragma unroll
-          for (int i = 0; i < PER_LANE; ++i) {
-            const int oi = lane + 32 * i;
-            if (oi < NOUT) {
-              const int c = oi / NJ, jj = oi % NJ;
-              double a = acc[i];
-              for (int v = 0; v < nvalid; ++v) a += W.sB[v][c] * W.sS[c0 + v][jj];
-              acc[i] = a;
-            }
-          }
-          __syncwarp();
-        }
-      }
-    }
-    // gather the lane partials into the scratch row
-#pragma unroll
-    for (int i = 0; i < PER_LANE; ++i) {
-      const int oi = lane + 32 * i;
-      if (oi < NOUT) W.outv[oi] = acc[i];
-    }
-    __syncwarp();
-    if (lane == 0) {
-      if constexpr (WH) {
-        double srr, szz;
-        disk_stress(fp.R1, fp.zeta, m.nu_f, &srr, &szz);
-        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
-        for (int k = 0; k < K; ++k)
-          for (int mm = 0; mm < 3; ++mm) {
-            double Hb[3][3];
-            for (int c = 0; c < 6; ++c) {
-              const double v = W.outv[c * NJ + 3 * k + mm];
-              Hb[ia[c]][ib[c]] = v;
-              Hb[ib[c]][ia[c]] = v;
-            }
-            const double shv = W.sh_load[3 * k + mm];
-            Hb[0][0] += shv * srr;
-            Hb[1][1] += shv * srr;
-            Hb[2][2] += shv * szz;
-            for (int a = 0; a < 3; ++a)
-              for (int b = 0; b < 3; ++b) row[k * NR + 9 * a + 3 * b + mm] += Hb[a][b];
-          }
-      } else {
-        const double uz = disk_disp_z(fp.R1, fp.zeta, m.mu, m.nu_f);
-        for (int k = 0; k < K; ++k)
-          for (int mm = 0; mm < 3; ++mm)
-            for (int i = 0; i < 3; ++i)
-              row[k * NR + 3 * i + mm] += W.outv[i * NJ + 3 * k + mm] +
-                                          (i == 2 ? W.sh_load[3 * k + mm] * uz : 0.0);
-      }
-    }
-  }
-}
-
 // --------------------------------------------------------- k_fold_mirror
 // The mirror element of every band pair, one thread per pair: its
 // full-space field with the slip signs of the reflection (fold.py:334-350)
@@ -782,6 +414,8 @@ k_fold_mirror(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restri
       for (int i = 0; i < 9; ++i) row[k * NR + i] += Mv[9 * k + i] * mirror_slip_sign(i % 3);
   }
 }
+
+#include "fold_waves.cuh"
 
 // --------------------------------------------------------------- k_final
 struct FinalArgs {
@@ -965,12 +599,9 @@ int run(const mhs_request* r, cudaStream_t st, const Layout& L, unsigned long lo
       StageTimer t(MHS_STAGE_FOLD, st);
       k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
       if constexpr (KC != KD_E) {
-        dim3 gf((unsigned)r->n_src, (unsigned)((nc + FOLD_WARPS - 1) / FOLD_WARPS));
-        const size_t fsm = sizeof(FoldShared<P, KC, RF>);
-        MHS_CUDA_TRY(cudaFuncSetAttribute(k_fold<P, KC, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)fsm));
-        k_fold<P, KC, RF><<<gf, 32 * FOLD_WARPS, fsm, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list,
-                                                        r->mu, r->lam, T, status, census);
+        const int rc = fold_waves::run_fold<P, KC, RF>(r, st, ws + L.fold, L.fold_bytes, lo, nc,
+                                                       prep, cnt, list, T, status, census);
+        if (rc) return rc;
       }
       dim3 gm((unsigned)r->n_src, (unsigned)((nc + TB - 1) / TB));
       k_fold_mirror<P, KC, RF><<<gm, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list, r->mu,

@@ -147,17 +147,23 @@ int run_request(const mhs_request* r, cudaStream_t st, const Layout& L) {
   return fail(MHS_ERR_ARG, "no kernel unit for order %d", r->order);
 }
 
-// Largest observer chunk whose workspace fits `bytes` (plan() is monotone
-// in the chunk); 0 when not even one row fits.
-int64_t fit_chunk(const mhs_request* r, size_t bytes) {
-  if (plan(r, 1).total > bytes) return 0;
+// Layout of the largest observer chunk whose workspace fits `bytes`
+// (plan() is monotone in the chunk), beside the fold region the workspace
+// size affords; chunk 0 when not even one row fits.
+Layout fit_layout(const mhs_request* r, size_t bytes) {
+  const size_t fb = fold_bytes_for(r, bytes);
+  Layout none = plan(r, 1, fb);
+  if (none.total > bytes) {
+    none.chunk = 0;
+    return none;
+  }
   int64_t lo = 1, hi = std::min<int64_t>(r->n_obs, 65535);
   while (lo < hi) {
     const int64_t mid = lo + (hi - lo + 1) / 2;
-    if (plan(r, mid).total <= bytes) lo = mid;
+    if (plan(r, mid, fb).total <= bytes) lo = mid;
     else hi = mid - 1;
   }
-  return lo;
+  return plan(r, lo, fb);
 }
 
 constexpr size_t GOOD_T_BYTES = size_t(2) << 30;
@@ -194,15 +200,15 @@ extern "C" {
 int mhs_workspace_bytes(const mhs_request* req, size_t* min_bytes, size_t* good_bytes) {
   int rc = check_request(req);
   if (rc) return rc;
-  const Layout one = plan(req, 1);
-  const size_t row = plan(req, 2).total - one.total;
+  const size_t fgood = fold_good_bytes(req);
+  const size_t fmin = fgood ? FOLD_MIN_BYTES : 0;
+  const Layout one = plan(req, 1, 0);
+  const size_t row = plan(req, 2, 0).total - one.total;
   int64_t chunk = std::min<int64_t>(req->n_obs, 65535);
-  const Layout all = plan(req, chunk);
-  if (all.total - one.total > GOOD_T_BYTES && row > 0) {
+  if (plan(req, chunk, 0).total - one.total > GOOD_T_BYTES && row > 0)
     chunk = std::max<int64_t>(1, (int64_t)(GOOD_T_BYTES / row));
-  }
-  if (min_bytes) *min_bytes = one.total;
-  if (good_bytes) *good_bytes = plan(req, chunk).total;
+  if (min_bytes) *min_bytes = plan(req, 1, fmin).total;
+  if (good_bytes) *good_bytes = plan(req, chunk, fgood).total;
   return MHS_OK;
 }
 
@@ -212,11 +218,14 @@ int mhs_assemble(const mhs_request* req, void* stream) {
   rc = ensure_device_tables();
   if (rc) return rc;
   // largest chunk the workspace holds
-  const int64_t chunk = req->workspace ? fit_chunk(req, req->workspace_bytes) : 0;
-  if (chunk == 0)
+  const Layout L = fit_layout(req, req->workspace ? req->workspace_bytes : 0);
+  if (L.chunk == 0) {
+    size_t mn = 0;
+    mhs_workspace_bytes(req, &mn, nullptr);
     return fail(MHS_ERR_WORKSPACE, "workspace %zu bytes, need at least %zu", req->workspace_bytes,
-                plan(req, 1).total);
-  return run_request(req, (cudaStream_t)stream, plan(req, chunk));
+                mn);
+  }
+  return run_request(req, (cudaStream_t)stream, L);
 }
 
 int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits) {
@@ -228,17 +237,16 @@ int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits)
   rc = noalloc_scratch(&scratch);
   if (rc) return rc;
   const size_t cap = MHS_NOALLOC_SCRATCH_BYTES;
-  const int64_t chunk = fit_chunk(req, cap);
-  if (chunk == 0)
+  const Layout L = fit_layout(req, cap);
+  if (L.chunk == 0)
     return fail(MHS_ERR_WORKSPACE,
                 "request needs %zu bytes of scratch for one observer row, above the %zu-byte "
                 "array of the allocation-free entry point (MHS_NOALLOC_SCRATCH_BYTES); pass "
                 "fewer sources per call or use mhs_assemble with a caller workspace",
-                plan(req, 1).total, cap);
+                L.total, cap);
   mhs_request r = *req;
   r.workspace = scratch;
   r.workspace_bytes = cap;
-  const Layout L = plan(&r, chunk);
   cudaStream_t st = (cudaStream_t)stream;
   rc = run_request(&r, st, L);
   if (rc || !status_bits) return rc;

@@ -23,6 +23,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "../../include/mhs_b200.h"
 #include "engine_fold.cuh"
 #include "host_prep.h"
@@ -58,13 +60,14 @@ MHS_FI constexpr int row_of(int kc) { return comps_of(kc) + 2; }
 
 inline size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Workspace carve-up for a chunk of `chunk` observers.
+// Workspace carve-up for a chunk of `chunk` observers plus `fold_bytes`
+// for the fold's plan, pair batches and node waves.
 struct Layout {
-  size_t status, coef, prep, G, cnt, list, T, total;
+  size_t status, coef, prep, G, cnt, list, T, fold, fold_bytes, total;
   int64_t chunk;
 };
 
-inline Layout plan(const mhs_request* r, int64_t chunk) {
+inline Layout plan(const mhs_request* r, int64_t chunk, size_t fold_bytes = 0) {
   const int kc = kind_class(r->kind);
   const int K = n_nodes(r->order);
   Layout L;
@@ -77,9 +80,33 @@ inline Layout plan(const mhs_request* r, int64_t chunk) {
   L.cnt = off; off = align_up(off + sizeof(int) * (size_t)r->n_src);
   L.list = off; off = align_up(off + sizeof(int) * (size_t)r->n_src * (size_t)chunk);
   L.T = off; off = align_up(off + sizeof(double) * (size_t)chunk * r->n_src * K * row_of(kc));
+  L.fold = off; off = align_up(off + fold_bytes);
+  L.fold_bytes = fold_bytes;
   L.total = off;
   L.chunk = chunk;
   return L;
+}
+
+// Fold region: none without the fold or for the blob-only readout; else at
+// least FOLD_MIN_BYTES, at most the request's useful size (FOLD_GOOD_BYTES,
+// less for small requests), otherwise half of what the workspace holds
+// beyond one observer row.
+constexpr size_t FOLD_MIN_BYTES = size_t(8) << 20;
+constexpr size_t FOLD_GOOD_BYTES = size_t(2) << 30;
+
+inline size_t fold_good_bytes(const mhs_request* r) {
+  if (!r->fold || kind_class(r->kind) == KD_E) return 0;
+  const double want = 4096.0 * (double)r->n_obs * (double)r->n_src;
+  if (want >= (double)FOLD_GOOD_BYTES) return FOLD_GOOD_BYTES;
+  return std::max<size_t>(FOLD_MIN_BYTES * 8, align_up((size_t)want));
+}
+
+inline size_t fold_bytes_for(const mhs_request* r, size_t workspace_bytes) {
+  const size_t good = fold_good_bytes(r);
+  if (!good) return 0;
+  const size_t row = plan(r, 1, 0).total;
+  const size_t half = workspace_bytes > row ? (workspace_bytes - row) / 2 : 0;
+  return align_up(std::min(good, std::max(FOLD_MIN_BYTES, half)));
 }
 
 // ------------------------------------------- services of the host unit

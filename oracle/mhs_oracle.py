@@ -234,6 +234,9 @@ def _edge_closed(ua, ub, rho2, spec):
 
 
 def _edge_small(ua, ub, rho2, spec):
+    """Small-|u| series (primitives.py:351-399): P[m][k] = rho^(k+1-m)
+    sum_j C(-m/2, j) (yb^pw - ya^pw) / pw, pw = k + 2j + 1, y = u / rho; each
+    power difference is formed once and shared by every (m, k)."""
     rho = np.sqrt(rho2)
     ya, yb = ua / rho, ub / rho
     same = ua * ub > 0.0
@@ -241,20 +244,26 @@ def _edge_small(ua, ub, rho2, spec):
         log_r = np.where(same, np.log1p((ub - ua) / ua), 0.0)
         ratio = np.where(same, ub / ua, np.inf)
     close = same & (np.abs(ratio) < 2.0) & (np.abs(ratio) > 0.5)
+    pwmax = max(km for km in spec.values()) + 2 * (SERIES_TERMS - 1) + 1
+    diff = {}
+    for pw in range(1, pwmax + 1):
+        with np.errstate(over="ignore", invalid="ignore"):
+            diff[pw] = np.where(close, ya ** pw * np.expm1(pw * log_r), yb ** pw - ya ** pw)
     out = {}
     for m, km in spec.items():
         for k in range(km + 1):
             acc = np.zeros_like(ua)
             for j in range(SERIES_TERMS):
                 pw = k + 2 * j + 1
-                with np.errstate(over="ignore", invalid="ignore"):
-                    d = np.where(close, ya ** pw * np.expm1(pw * log_r), yb ** pw - ya ** pw)
-                acc = acc + _binom_half(m, j) * d / pw
+                acc = acc + _binom_half(m, j) * diff[pw] / pw
             out[(m, k)] = rho ** (k + 1 - m) * acc
     return out
 
 
 def _edge_large(ua, ub, rho2, spec):
+    """Large-|u| series (primitives.py:293-349) on one side of the foot:
+    P[m][k] = +-a^s sum_j C(-m/2, j) x^j [t^q / q]_1^(b/a), q = s - 2j; each
+    bracket is formed once per exponent q."""
     neg = ua < 0.0
     a = np.where(neg, -ub, ua)
     b = np.where(neg, -ua, ub)
@@ -262,22 +271,28 @@ def _edge_large(ua, ub, rho2, spec):
     log_r = np.log1p((b - a) / a)
     close = r < 2.0
     x = rho2 / (a * a)
+    xp = [np.ones_like(a)]
+    for _ in range(1, SERIES_TERMS):
+        xp.append(xp[-1] * x)
+    brk = {}
+
+    def bracket(q):
+        if q not in brk:
+            if q == 0:
+                brk[q] = log_r
+            else:
+                with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
+                    brk[q] = np.where(close, np.expm1(q * log_r), r ** q - 1.0) / q
+        return brk[q]
+
     out = {}
     for m, km in spec.items():
         for k in range(km + 1):
-            s = k - m + 1
+            s_ = k - m + 1
             acc = np.zeros_like(a)
-            xj = np.ones_like(a)
             for j in range(SERIES_TERMS):
-                q = s - 2 * j
-                if q == 0:
-                    t = log_r
-                else:
-                    with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
-                        t = np.where(close, np.expm1(q * log_r), r ** q - 1.0) / q
-                acc = acc + _binom_half(m, j) * xj * t
-                xj = xj * x
-            val = a ** s * acc
+                acc = acc + _binom_half(m, j) * xp[j] * bracket(s_ - 2 * j)
+            val = a ** s_ * acc
             out[(m, k)] = np.where(neg, -val, val) if k % 2 else val
     return out
 
@@ -406,9 +421,27 @@ def weighted_tables(f, x, eps, P, need0):
             xi0 = eta[None, :, 0] - X0[sel][:, None]
             xi1 = eta[None, :, 1] - X1[sel][:, None]
             R2 = xi0 * xi0 + xi1 * xi1 + h2[sel][:, None]
+            # in-plane monomials (weights folded in) from power tables, and
+            # R^-n from one reciprocal square root and a ladder in R^-2, in
+            # the order of mhs/fullspace/moments.py:456-498
+            dmax = max(need0.values())
+            p0, p1 = _pow_table(xi0, max(dmax, 1)), _pow_table(xi1, max(dmax, 1))
             inv = 1.0 / np.sqrt(R2)
+            inv2 = inv * inv
+            rn, cur = {}, inv
+            for n in range(1, max(need0) + 1, 2):
+                rn[n] = cur
+                cur = cur * inv2
             for (n, a, b) in W:
-                W[(n, a, b)][sel] = (wq[None, :] * xi0 ** a * xi1 ** b * inv ** n) @ Nq
+                if a and b:
+                    mono = wq[None, :] * p0[a] * p1[b]
+                elif a:
+                    mono = wq[None, :] * p0[a]
+                elif b:
+                    mono = wq[None, :] * p1[b]
+                else:
+                    mono = np.broadcast_to(wq[None, :], R2.shape)
+                W[(n, a, b)][sel] = (mono * rn[n]) @ Nq
     return W, z
 
 
@@ -585,9 +618,40 @@ def _tri_distance(x, t):
     return out
 
 
-def image_q(x, tri, P, mu, lam, eps, want):
-    """Q-family by per-observer Gauss quadrature (kernels/image.py:211-432)."""
+@functools.lru_cache(maxsize=8)
+def _q_dense(nu):
+    """Monomial keys (a, b, c, n, q) of the Q-family records and, per
+    readout, the (slots, monomials) matrix of record coefficients summed by
+    (slot, monomial) -- each record adds one number to one output slot
+    (kernels/image.py:257-297)."""
     t = _table()
+    monos = sorted({tuple(e) for e in t["q_dg_exp"]} | {tuple(e) for e in t["q_ddg_exp"]})
+    midx = {m: i for i, m in enumerate(monos)}
+    mats = {}
+    for key, nix in (("q_dg", 3), ("q_ddg", 4)):
+        coefs = _coef_by_record(t[f"{key}_terms"], len(t[f"{key}_idx"]), 0.0, nu, False)
+        C = np.zeros((3 ** nix, len(monos)))
+        for r, (ix, ex) in enumerate(zip(t[f"{key}_idx"], t[f"{key}_exp"])):
+            slot = 0
+            for i in ix:
+                slot = slot * 3 + int(i)
+            C[slot, midx[tuple(ex)]] += coefs[r]
+        mats[key] = C
+    return monos, mats
+
+
+def _pow_table(v, kmax):
+    """[1, v, v^2, ..., v^kmax] by repeated multiplication."""
+    out = [None, v]
+    for _ in range(2, kmax + 1):
+        out.append(out[-1] * v)
+    return out
+
+
+def image_q(x, tri, P, mu, lam, eps, want):
+    """Q-family by per-observer Gauss quadrature (kernels/image.py:211-432):
+    observers grouped by their Gauss order, monomials formed from power
+    tables, one dense contraction of the records per group."""
     tri = np.asarray(tri, float)
     nu = lam / (2.0 * (lam + mu))
     scale = 2.0 * (lam + mu) / (np.pi * mu * (lam + 2.0 * mu))
@@ -597,8 +661,8 @@ def image_q(x, tri, P, mu, lam, eps, want):
     delta = _tri_distance(x, tri * np.array([1.0, 1.0, -1.0]))
     orders = np.clip(np.ceil(Q_BUDGET_C * f.L / np.sqrt(delta * delta + eps * eps)) + P,
                      Q_MIN, Q_MAX).astype(int)
-    monos = sorted({tuple(e) for e in t["q_dg_exp"]} | {tuple(e) for e in t["q_ddg_exp"]})
-    midx = {m: i for i, m in enumerate(monos)}
+    monos, mats = _q_dense(nu)
+    emax = [max(m[i] for m in monos) for i in range(5)]
     DG = np.zeros((N, K, 27)) if "U" in want else None
     DDG = np.zeros((N, K, 81)) if "H" in want else None
     c0 = shape_poly(f, P, np.zeros(1), np.zeros(1))
@@ -615,20 +679,18 @@ def image_q(x, tri, P, mu, lam, eps, want):
         d2 = xs[:, 1:2] - y[None, :, 1]
         d3 = xs[:, 2:3] + y[None, :, 2]
         r2 = np.sqrt(d1 * d1 + d2 * d2 + d3 * d3 + eps ** 2)
-        ir, iq = 1.0 / r2, 1.0 / (r2 - d3)
-        basis = np.stack([(d1 ** a * d2 ** b * d3 ** c * ir ** n * iq ** q) @ wN
-                          for (a, b, c, n, q) in monos])          # (M, n_sel, K)
-        for key, arr, nix in (("q_dg", DG, 3), ("q_ddg", DDG, 4)):
-            if arr is None:
-                continue
-            coefs = _coef_by_record(t[f"{key}_terms"], len(t[f"{key}_idx"]), 0.0, nu, False)
-            sub = np.zeros((int(sel.sum()), K, 3 ** nix))
-            for r, (ix, ex) in enumerate(zip(t[f"{key}_idx"], t[f"{key}_exp"])):
-                slot = 0
-                for i in ix:
-                    slot = slot * 3 + int(i)
-                sub[:, :, slot] += coefs[r] * basis[midx[tuple(ex)]]
-            arr[sel] = sub * scale
+        pw = [_pow_table(v, e) for v, e in zip((d1, d2, d3, 1.0 / r2, 1.0 / (r2 - d3)), emax)]
+        basis = np.empty((len(monos), xs.shape[0], K))
+        for k, mono in enumerate(monos):
+            term = None
+            for table, e in zip(pw, mono):
+                if e:
+                    term = table[e] if term is None else term * table[e]
+            basis[k] = (np.ones_like(r2) if term is None else term) @ wN
+        for key, arr in (("q_dg", DG), ("q_ddg", DDG)):
+            if arr is not None:
+                flat = np.tensordot(mats[key], basis, axes=([1], [0]))     # (slots, n, K)
+                arr[sel] = np.moveaxis(flat, 0, -1) * scale
     return _contract(None if DG is None else DG.reshape(N, K, 3, 3, 3),
                      None if DDG is None else DDG.reshape(N, K, 3, 3, 3, 3), f.n, mu, lam)
 
