@@ -8,20 +8,30 @@ correlation length 5), 2,400 triangles, eps per triangle 0.3 x its mean
 edge, receivers at the centroids with cutde frames, mu = lam = 30: output
 (2400, 2400, 3, 3) float64.  Synthetic, seeded inputs (there is no dataset).
 
-  value  entries/s with inputs resident on the device (CUDA events)
-  e2e    entries/s through the public API from pinned host inputs, with the
-         host->device copies and the full device->host read of the matrix
-         inside the timed region
-  roofline   the dominant stage (the fold): its algorithmic flops -- per-unit
-         operation counts of the op-counting host build times the device
-         census of its work units in an untimed step -- over its time per
-         launch, against the measured FP64 FMA ceiling
-  cpu_baseline   the numpy oracle (a restatement of mhs's CPU path) on a
-         stratified sample of the same workload, extrapolated
+  value      entries/s with inputs resident on the device (CUDA events)
+  e2e        entries/s through the public API from pinned host inputs, with
+             the host->device copies and the full device->host read of the
+             matrix inside the timed region
+  roofline   the dominant kernel (a part of the fold): its algorithmic flops
+             -- per-unit operation counts of the op-counting host build times
+             the device census of its work units in an untimed step -- over
+             its time per launch, against the measured FP64 FMA ceiling
+  cpu_baseline  the numpy oracle (a restatement of mhs's CPU path, timed
+             within 20 % of mhs itself on the same inputs) on a stratified
+             sample of the same workload, extrapolated
 
-``--impl reference`` times that CPU implementation alone on the host cores.
-``--gpus N`` (under torchrun) runs N independent replicas, one seeded mesh
-per rank (weak scaling, no collective on the data path).
+Further legs (``--legs``): ``mixed`` (the mixed-precision form and its
+error against this run's FP64 matrix), ``e2e``, ``c4`` (the continuous P2
+interaction of the 3-fault network, ~6,000 triangles, FP64 and mixed),
+``serving`` (a seeded Poisson stream through the serving loop at scaled-down
+sizes), ``batch`` (the 64 uneven requests of the batched configuration at
+their stated sizes), ``serve_full`` (the serving stream at its stated sizes,
+bounded by ``--serve-requests``).
+
+``--impl reference`` times the CPU implementation alone on the host cores.
+``--gpus N`` (under torchrun): the rows of ONE matrix are split across the
+ranks by cost-balanced receiver blocks (mhs_b200.parallel), timed as the
+max over ranks; no collective on the data path (strong scaling).
 """
 from __future__ import annotations
 
@@ -42,12 +52,13 @@ sys.path.insert(0, ROOT)
 METRIC = "Green's-fn entries/s"
 UNIT = "entries/s"
 WORKLOAD = "interaction_matrix (3,3), rough surface-reaching fault, 2400 tris, per-tri eps, fold on"
+LEGS = ("main", "mixed", "e2e", "c4", "serving", "batch")
 
-# DRAM bytes (read + write) of one k_fold launch on this workload, from
-# profiles/fold_c2_traffic.md; keyed by (nu, nv, precision).
-FOLD_TRAFFIC_PER_LAUNCH = {(60, 20, "fp64"): 120.4e6 + 1.78e9}
-# Kernels each profiled stage launches (csrc/mhs_b200.cu: run()).
-KERNELS_PER_STAGE = {"prep": 2, "pair": 1, "imageq": 1, "fold": 3, "final": 1}
+#: Wall time of the numpy oracle over mhs itself on the same inputs, timed in
+#: the build container (one core each, BLAS at one thread): config-1
+#: disp_matrix 7.94 s vs 9.62 s; a config-2 block of 10 ordinary sources x 40
+#: receivers 0.31 s vs 0.26 s; one config-2 fold pair 0.26 s vs 0.28 s.
+PORT_OVER_MHS = {"c1_disp_matrix": 0.83, "c2_ordinary_block": 1.20, "c2_fold_pair": 0.92}
 
 
 def parse():
@@ -59,6 +70,9 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--nu", type=int, default=60, help="rectangles along strike")
     ap.add_argument("--nv", type=int, default=20, help="rectangles down dip")
+    ap.add_argument("--legs", default=",".join(LEGS),
+                    help=f"comma list of {LEGS + ('serve_full',)}")
+    ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
@@ -81,6 +95,7 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.p = None
+        self.out = ""
 
     def __enter__(self):
         try:
@@ -122,13 +137,23 @@ class Clocks:
 
 
 # --------------------------------------------------------- CPU baseline
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def _oracle_rows(args):
     """Oracle interaction of sources `srcs` at receivers `recs` (worker)."""
     import numpy as _np
     sys.path.insert(0, ROOT)
     from oracle import mhs_oracle as O
     tris, eps, mu, lam, recs, srcs = args
-    K = O.self_interaction  # noqa: F841  (module warm-up)
     pts = O.collocation_points(tris)
     fr = O.slip_frame(tris)
     t = time.perf_counter()
@@ -137,10 +162,21 @@ def _oracle_rows(args):
     return time.perf_counter() - t
 
 
-def cpu_baseline(tris, eps, mu, lam, seconds: float, seed: int = 1):
+def _one_thread_blas():
+    os.environ.update({k: "1" for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                        "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS")})
+    try:
+        from threadpoolctl import threadpool_limits
+        threadpool_limits(1)
+    except ImportError:
+        pass
+
+
+def cpu_baseline(tris, eps, mu, lam, seconds: float, seed: int = 1, fold_pairs: int = 256):
     """Stratified sample of the workload through the numpy oracle on all
-    host cores (spawned pool): fold pairs (straddling source, band receiver)
-    and ordinary pairs timed separately, extrapolated to the full matrix."""
+    host cores (spawned pool, BLAS at one thread per worker): ordinary pairs
+    and fold pairs (straddling source, band receiver) timed separately,
+    extrapolated to the full matrix."""
     import multiprocessing as mp
     sys.path.insert(0, ROOT)
     from oracle import mhs_oracle as O
@@ -148,185 +184,115 @@ def cpu_baseline(tris, eps, mu, lam, seconds: float, seed: int = 1):
     pts = O.collocation_points(tris)
     strad = [s for s in range(n) if O.straddles(tris[s], eps[s])]
     band_of = {s: O.band(pts, tris[s], eps[s]) for s in strad}
-    n_fold = sum(len(b) for b in band_of.values())
+    all_fold = [(s, int(r)) for s in strad for r in band_of[s]]
+    n_fold = len(all_fold)
     n_reg = n * n - n_fold
     rng = np.random.default_rng(seed)
     cores = max(1, min(os.cpu_count() or 1, 64))
+    saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                            "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS")}
+    _one_thread_blas()   # inherited by the spawned workers
     ctx = mp.get_context("spawn")
-    jobs_reg, jobs_fold = [], []
-    # ordinary pairs: sources paired with receivers outside their band
+    jobs_reg = []
     for s in rng.choice(n, size=min(n, 4 * cores), replace=False):
         excl = set(band_of.get(int(s), []))
         recs = [r for r in rng.choice(n, size=min(n, 48), replace=False) if r not in excl]
         if recs:
             jobs_reg.append((tris, eps, mu, lam, np.array(recs, dtype=np.int64),
                              np.array([s], dtype=np.int64)))
-    for s in rng.choice(strad, size=min(len(strad), 2 * cores), replace=False):
-        b = band_of[int(s)]
-        if len(b):
-            jobs_fold.append((tris, eps, mu, lam, rng.choice(b, size=1), np.array([s])))
+    pick = rng.choice(n_fold, size=min(n_fold, fold_pairs), replace=False) if n_fold else []
+    jobs_fold = [(tris, eps, mu, lam, np.array([all_fold[i][1]]), np.array([all_fold[i][0]]))
+                 for i in pick]
     t_start = time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        pool.map(_oracle_rows, jobs_reg[:cores])  # warm the workers
-        t0 = time.perf_counter()
-        pool.map(_oracle_rows, jobs_reg)
-        t_reg = (time.perf_counter() - t0) / sum(len(j[4]) for j in jobs_reg)
-        t0 = time.perf_counter()
-        pool.map(_oracle_rows, jobs_fold)
-        t_fold = (time.perf_counter() - t0) / max(1, len(jobs_fold))
+    try:
+        with ctx.Pool(cores, initializer=_one_thread_blas) as pool:
+            pool.map(_oracle_rows, jobs_reg[:cores])  # warm the workers
+            t0 = time.perf_counter()
+            pool.map(_oracle_rows, jobs_reg)
+            t_reg = (time.perf_counter() - t0) / sum(len(j[4]) for j in jobs_reg)
+            t0 = time.perf_counter()
+            if jobs_fold:
+                pool.map(_oracle_rows, jobs_fold, chunksize=1)
+            t_fold = (time.perf_counter() - t0) / max(1, len(jobs_fold))
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
     total = n_reg * t_reg + n_fold * t_fold
     entries = n * n * 9
     return {"value": entries / total, "unit": UNIT, "cores": cores, "kind": "port",
+            "cpu_model": _cpu_model(), "blas_threads_per_worker": 1,
+            "port_time_over_mhs": PORT_OVER_MHS,
             "sample": (f"numpy oracle, {sum(len(j[4]) for j in jobs_reg)} ordinary pairs and "
-                       f"{len(jobs_fold)} fold pairs timed on a {cores}-process pool, "
-                       f"extrapolated to {n_reg} ordinary + {n_fold} fold pairs"),
+                       f"{len(jobs_fold)} fold pairs (stratified, seeded) timed on a "
+                       f"{cores}-process pool, extrapolated to {n_reg} ordinary + {n_fold} fold "
+                       f"pairs"),
             "seconds": time.perf_counter() - t_start}
 
 
-# ----------------------------------------------------------- our arm
-# Serving stream: seeded Poisson arrivals of uneven requests (the BASELINE
-# serving config's distributions with the sizes scaled down so the stream
-# takes seconds): kind uniform in {disp, stress, traction, interaction},
-# triangles log-uniform in [100, 2000], observers log-uniform in [100, 5000],
-# order uniform in {0, 1, 2}, eps per triangle 0.3 x its mean edge.
-SERVE = {"requests": 48, "rate_per_s": 20.0, "tris": (100, 2000), "obs": (100, 5000)}
+# ------------------------------------------------------------ our arm
+def _sync_max(torch, dev, world, x):
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
 
 
-def _serve_requests(torch, dev, seed):
-    import mhs_b200 as mhs
-    from mhs_b200 import synthetic
-    rng = np.random.default_rng(seed)
-    out = []
-    for i in range(SERVE["requests"]):
-        nt = int(np.exp(rng.uniform(*np.log(SERVE["tris"]))))
-        no = int(np.exp(rng.uniform(*np.log(SERVE["obs"]))))
-        nv = max(1, int(round(np.sqrt(nt / 6.0))))
-        nu = max(1, int(round(nt / (2 * nv))))
-        L, W = 2.0 * nu, 2.0 * nv
-        tris = synthetic.planar_fault(rng.uniform(0, 180), rng.uniform(15, 90), L, W,
-                                      -rng.uniform(0, 5), nu, nv)
-        edges = np.linalg.norm(tris - np.roll(tris, 1, axis=1), axis=2).mean(axis=1)
-        eps = torch.as_tensor(0.3 * edges, device=dev)
-        ext = 1.5 * max(L, W)
-        obs = np.column_stack([rng.uniform(-ext, ext, no), rng.uniform(-ext, ext, no),
-                               -rng.uniform(0, ext, no)])
-        t = torch.as_tensor(tris, device=dev)
-        o = torch.as_tensor(obs, device=dev)
-        mat = mhs.Material(30.0, float(rng.uniform(20, 40)))
-        order = int(rng.integers(0, 3))
-        kind = int(rng.integers(0, 4))
-        if kind == 0:
-            r = (mhs.disp_matrix, (o, t, mat, eps), {"order": order})
-        elif kind == 1:
-            r = (mhs.stress_matrix, (o, t, mat, eps), {"order": order})
-        elif kind == 2:
-            nrm = torch.as_tensor(rng.standard_normal((no, 3)), device=dev)
-            r = (mhs.traction_matrix, (o, nrm, t, mat, eps), {"order": order})
-        else:
-            r = (mhs.interaction_matrix, (t, mat, eps), {"order": order})
-        out.append((r, float(rng.exponential(1.0 / SERVE["rate_per_s"]))))
-    return out
-
-
-def serve_stream(dev, precision, seed):
-    """Latency percentiles and throughput of the seeded stream through the
-    serving loop (requests overlap on the device)."""
-    import torch
-    from mhs_b200 import serve
-    reqs = _serve_requests(torch, dev, seed)
+def timed(torch, dev, world, fn, steps, flush):
+    """Device time of `steps` calls (CUDA events on the current stream, L2
+    flushed before each), max over ranks."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
     torch.cuda.synchronize()
-    with serve.Server(dev, slots=8) as srv:
-        futs = []
-        t_next = time.perf_counter()
-        for (fn, args, kw), gap in reqs:
-            t_next += gap
-            delay = t_next - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            futs.append(srv.submit(fn, *args, precision=precision, **kw))
-        for f in futs:
-            f.result()
-        st = srv.stats()
-        st["peak_in_flight"] = srv.peak_in_flight
-    return st
-
-
-# Batched uneven assembly: 64 seeded requests (the batched config's
-# distributions: kind uniform in {disp, stress, traction}, order uniform in
-# {0, 1, 2}, dip in [15, 90] degrees, top depth in [0, 5], lam in [20, 40],
-# eps 0.1; sizes scaled down -- triangles log-uniform in [50, 1000],
-# observers in [100, 4000] -- so the batch takes seconds), all submitted at
-# once to the serving loop, which overlaps them on the device.
-BATCH = {"requests": 64, "tris": (50, 1000), "obs": (100, 4000)}
-
-
-def _batch_requests(torch, dev, seed):
-    import mhs_b200 as mhs
-    from mhs_b200 import synthetic
-    rng = np.random.default_rng(seed)
-    out = []
-    for i in range(BATCH["requests"]):
-        nt = int(np.exp(rng.uniform(*np.log(BATCH["tris"]))))
-        no = int(np.exp(rng.uniform(*np.log(BATCH["obs"]))))
-        nv = max(1, int(round(np.sqrt(nt / 6.0))))
-        nu = max(1, int(round(nt / (2 * nv))))
-        L, W = 2.0 * nu, 2.0 * nv
-        tris = synthetic.planar_fault(0.0, rng.uniform(15, 90), L, W, -rng.uniform(0, 5), nu, nv)
-        ext = 1.5 * max(L, W)
-        obs = np.column_stack([rng.uniform(-ext, ext, no), rng.uniform(-ext, ext, no),
-                               -rng.uniform(0, ext, no)])
-        t = torch.as_tensor(tris, device=dev)
-        o = torch.as_tensor(obs, device=dev)
-        mat = mhs.Material(30.0, float(rng.uniform(20, 40)))
-        order = int(rng.integers(0, 3))
-        kind = int(rng.integers(0, 3))
-        if kind == 0:
-            out.append((mhs.disp_matrix, (o, t, mat, 0.1), {"order": order}))
-        elif kind == 1:
-            out.append((mhs.stress_matrix, (o, t, mat, 0.1), {"order": order}))
-        else:
-            v = rng.standard_normal((no, 3))
-            nrm = torch.as_tensor(v / np.linalg.norm(v, axis=1, keepdims=True), device=dev)
-            out.append((mhs.traction_matrix, (o, nrm, t, mat, 0.1), {"order": order}))
-    return out
-
-
-def batch_run(dev, precision, seed):
-    """Makespan and entries/s of the seeded batch, all requests submitted at
-    once (device time from the first submit to the last result)."""
-    import torch
-    from mhs_b200 import serve
-    reqs = _batch_requests(torch, dev, seed)
+    if world > 1:
+        torch.distributed.barrier()
+    for i in range(steps):
+        flush.fill_(i & 0xFF)
+        ev[i][0].record()
+        fn()
+        ev[i][1].record()
     torch.cuda.synchronize()
-    with serve.Server(dev, slots=16) as srv:
-        t0 = time.perf_counter()
-        futs = [srv.submit(fn, *args, precision=precision, **kw) for fn, args, kw in reqs]
-        for f in futs:
-            f.result()
-        t1 = time.perf_counter()
-        st = srv.stats()
-    return {"makespan_s": t1 - t0, "entries": st["entries"],
-            "entries_per_s": st["entries"] / (t1 - t0), "p50_ms": st["p50_ms"],
-            "p99_ms": st["p99_ms"], "peak_in_flight": srv.peak_in_flight}
+    if world > 1:
+        torch.distributed.barrier()
+    return _sync_max(torch, dev, world, sum(a.elapsed_time(b) for a, b in ev))
 
 
-def run_ours(a, rank, world):
+# Algorithmic flops per fold part, from the census and the op-counting build.
+def _fold_parts_flops(census, u):
+    near_units = (census["near"] * u["near"]["flop"] +
+                  census["edge_closed"] * u["edge_closed"]["flop"] +
+                  census["edge_small"] * u["edge_small"]["flop"] +
+                  census["edge_large"] * u["edge_large"]["flop"])
+    far_units = census["far12"] * u["far12"]["flop"] + census["far8"] * u["far8"]["flop"]
+    return {"fold_near": near_units, "fold_far": far_units}
+
+
+def run_ours(a, rank, world, legs):
     import torch
     import mhs_b200 as mhs
-    from mhs_b200 import _native
+    from mhs_b200 import _native, parallel
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    tris, eps, mu, lam = workload(rank, a.nu, a.nv)
+    tris, eps, mu, lam = workload(0, a.nu, a.nv)
     n = tris.shape[0]
     mat = mhs.Material(mu, lam)
     t_dev = torch.as_tensor(tris, device=dev)
     e_dev = torch.as_tensor(eps, device=dev)
-    out = torch.empty((n, n, 3, 3), dtype=torch.float64, device=dev)
+    # rows of this rank (all of them at N = 1)
+    if world > 1:
+        costs = parallel.row_costs(mhs.collocation_points(tris), tris, eps)
+        lo, hi = parallel.row_blocks(costs, world)[rank]
+    else:
+        lo, hi = 0, n
+    rows = None if world == 1 else (lo, hi)
+    out = torch.empty((hi - lo, n, 3, 3), dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def step():
-        return mhs.interaction_matrix(t_dev, mat, e_dev, out=out, precision=a.precision)
+    def step(precision=a.precision):
+        return mhs.interaction_matrix(t_dev, mat, e_dev, out=out, precision=precision, rows=rows)
 
     for _ in range(a.warmup):
         step()
@@ -336,153 +302,297 @@ def run_ours(a, rank, world):
     step()
     census = _native.census_read()
     _native.census(False)
-    if world > 1:
-        torch.distributed.barrier()
     _native.profile(True)
     _native.profile_read()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(a.steps)]
-    torch.cuda.synchronize()
+    _native.kernel_count()
     with Clocks(dev.index) as clk:
-        for i in range(a.steps):
-            flush.fill_(i & 0xFF)          # evict L2 between steps (untimed)
-            ev[i][0].record()
-            step()
-            ev[i][1].record()
-        torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+        ms = timed(torch, dev, world, step, a.steps, flush)
+    launches = _native.kernel_count() // max(1, a.steps)
     stages = _native.profile_read()
     _native.profile(False)
-    ms = sum(s.elapsed_time(e) for s, e in ev)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms = float(ms_t.item())
     entries = n * n * 9
-    value = world * entries * a.steps / (ms * 1e-3)
+    value = entries * a.steps / (ms * 1e-3)
+    stage_ms = {k: v[0] / a.steps for k, v in stages.items()}
 
-    # the mixed form beside the FP64 one, same protocol; its error is the
-    # relmax of its matrix against this run's FP64 matrix
-    mixed = None
-    if a.precision == "fp64":
+    # roofline of the dominant kernel: the fold's near or far loads (or a
+    # whole stage when the fold is absent), algorithmic flops over its time
+    from mhs_b200 import flops as _flops
+    peak = _native.fp_peak(fp64=True)
+    fl = _flops.fold_flops(census, order=0, want_h=True, mu=mu, lam=lam,
+                           eps=float(np.mean(eps)))
+    parts = _fold_parts_flops(census, fl["per_unit"])
+    per_kernel = {}
+    for k, f in parts.items():
+        t = stage_ms.get(k, 0.0)
+        if t > 0:
+            per_kernel[k] = {"ms_per_step": t, "flop_per_step": f,
+                             "achieved_tflops": f / (t * 1e-3) / 1e12,
+                             "frac_of_measured_fp64": f / (t * 1e-3) / 1e12 / peak}
+    top = max(per_kernel, key=lambda k: per_kernel[k]["ms_per_step"]) if per_kernel else None
+    fold_ms = stage_ms.get("fold", 0.0)
+    roof = {"bound": "fp64", "kernel": top, "unit": "TFLOP/s", "peak": peak,
+            "achieved": per_kernel[top]["achieved_tflops"] if top else None,
+            "frac": per_kernel[top]["frac_of_measured_fp64"] if top else None,
+            "traffic": None,
+            "peak_source": "measured FP64 FMA ceiling of this device (mhs_fp_peak, this run); "
+                           "of measured",
+            "fold_stage": {"ms_per_step": fold_ms, "flop_per_step": fl["flop"],
+                           "achieved_tflops": fl["flop"] / (fold_ms * 1e-3) / 1e12 if fold_ms else None,
+                           "frac": fl["flop"] / (fold_ms * 1e-3) / 1e12 / peak if fold_ms else None},
+            "kernels": per_kernel,
+            "algorithmic": {"flop_fold": fl["flop"], "div": fl["div"], "sqrt": fl["sqrt"],
+                            "special": fl["special"], "census": census,
+                            "counting": "op-counting host build of the engine "
+                                        "(mhs_b200/csrc/opcount.cpp): add/sub/mul 1 flop, fma 2; "
+                                        "div, sqrt, library calls apart"},
+            "stage_ms_per_step": stage_ms}
+
+    line = {"metric": METRIC, "value": value,
+            "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "weak" if world == 1 else "strong", "vs_baseline": None,
+            "dtype": "f64" if a.precision == "fp64" else "f64+f32",
+            "data": "synthetic (seeded rough fault mesh)",
+            "config": {"workload": WORKLOAD, "n_tri": n, "entries_per_step": entries,
+                       "precision": a.precision, "global_batch": 1,
+                       "l2": "L2 flushed between steps (256 MiB write); output 415 MB per step",
+                       "parallelism": f"row blocks x{world}" if world > 1 else "single GPU"},
+            "roofline": roof, "clocks": clk.summary(), "gpu_launches": launches}
+    if world > 1:
+        # every rank assembled its own row block of the one matrix; value is
+        # the whole matrix over the slowest rank's time
+        line["config"]["rows_of_rank0"] = [lo, hi]
+
+    if "mixed" in legs and a.precision == "fp64":
         ref = out.clone()
-
-        def step_mixed():
-            return mhs.interaction_matrix(t_dev, mat, e_dev, out=out, precision="mixed")
-
         for _ in range(max(1, a.warmup)):
-            step_mixed()
+            step("mixed")
+        _native.profile(True)
+        _native.profile_read()
+        ms_m = timed(torch, dev, world, lambda: step("mixed"), a.steps, flush)
+        stages_m = _native.profile_read()
+        _native.profile(False)
+        err = _sync_max(torch, dev, world,
+                        float(((out - ref).abs().max() / ref.abs().max()).item()))
+        vm = entries * a.steps / (ms_m * 1e-3)
+        line["mixed"] = {"value": vm, "unit": UNIT, "ms_per_step": ms_m / a.steps,
+                         "speedup_vs_fp64": vm / line["value"],
+                         "relmax_vs_fp64": err,
+                         "dtype": "f64+f32 (far-field quadrature bulk in f32)",
+                         "stage_ms_per_step": {k: v[0] / a.steps for k, v in stages_m.items()}}
+        del ref
+
+    if "e2e" in legs:
+        # pinned host inputs, H2D inside, this rank's rows read back
+        h_tris = torch.as_tensor(tris).pin_memory()
+        h_eps = torch.as_tensor(eps).pin_memory()
+        h_out = torch.empty(tuple(out.shape), dtype=torch.float64).pin_memory()
+        e2e_steps = max(1, min(a.steps, 3))
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(e2e_steps):
+            td = h_tris.to(dev, non_blocking=True)
+            ed = h_eps.to(dev, non_blocking=True)
+            r = mhs.interaction_matrix(td, mat, ed, out=out, precision=a.precision, rows=rows)
+            h_out.copy_(r, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = _sync_max(torch, dev, world, e0.elapsed_time(e1))
+        line["e2e"] = {"value": entries * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+                       "h2d_bytes_per_step": int(tris.nbytes + eps.nbytes),
+                       "d2h_bytes_per_step": int(out.numel() * 8)}
+    del out
+    torch.cuda.empty_cache()
+
+    if world == 1:
+        if "c4" in legs:
+            line["c4"] = c4_leg(torch, dev, flush)
+        if "serving" in legs:
+            line["serving"] = {"stream": dict(SERVE, note="sizes scaled down from the serving "
+                                              "config; arrivals Poisson, seeded; latency = submit "
+                                              "to result ready on the device, host clock"),
+                               "fp64": serve_stream(dev, "fp64", 100),
+                               "mixed": serve_stream(dev, "mixed", 100)}
+        if "batch" in legs:
+            line["batch"] = {"config": {"requests": 64, "tris": [50, 5000], "obs": [100, 20000],
+                                        "note": "the batched configuration at its stated sizes "
+                                                "(synthetic.batched_requests) through "
+                                                "mhs_b200.batch: one group of launches per class "
+                                                "and sub-batch"},
+                             "fp64": batch_run(dev, "fp64", 0),
+                             "mixed": batch_run(dev, "mixed", 0)}
+        if "serve_full" in legs:
+            line["serve_full"] = serve_full(dev, a.serve_requests)
+    return line, tris, eps, mu, lam
+
+
+# ------------------------------------------------------------ config 4
+def c4_leg(torch, dev, flush):
+    """Continuous P2 interaction of the 3-fault network, source = (strike,
+    dip), FP64 and mixed: one untimed and one timed step each."""
+    import mhs_b200 as mhs
+    from mhs_b200 import _native, synthetic
+    c = synthetic.config4()
+    sn = mhs.shared_nodes(c["tris"], groups=c["groups"])
+    mat = mhs.Material(c["mu"], c["lam"])
+    t = torch.as_tensor(c["tris"], device=dev)
+    out = torch.empty((sn.n, sn.n, 3, 2), dtype=torch.float64, device=dev)
+    res = {"workload": "interaction_matrix order=2 continuous, 3-fault network, source=(strike,dip)",
+           "n_tri": int(c["tris"].shape[0]), "n_nodes": int(sn.n),
+           "entries_per_step": int(out.numel())}
+    ref = None
+    for prec in ("fp64", "mixed"):
+        def step():
+            return mhs.interaction_matrix(t, mat, c["eps"], order=2, layout="continuous", shared=sn,
+                                          source=("strike", "dip"), out=out, precision=prec)
+        step()
         _native.profile(True)
         _native.profile_read()
-        evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(a.steps)]
-        for i in range(a.steps):
-            flush.fill_(i & 0xFF)
-            evm[i][0].record()
-            step_mixed()
-            evm[i][1].record()
-        torch.cuda.synchronize()
-        stages_m = _native.profile_read()
+        ms = timed(torch, dev, 1, step, 1, flush)
+        st = _native.profile_read()
         _native.profile(False)
-        ms_m = sum(x.elapsed_time(y) for x, y in evm)
-        ms_mt = torch.tensor([ms_m], dtype=torch.float64, device=dev)
-        err = float(((out - ref).abs().max() / ref.abs().max()).item())
-        err_t = torch.tensor([err], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(ms_mt, op=torch.distributed.ReduceOp.MAX)
-            torch.distributed.all_reduce(err_t, op=torch.distributed.ReduceOp.MAX)
-        ms_m = float(ms_mt.item())
-        vm = world * entries * a.steps / (ms_m * 1e-3)
-        mixed = {"value": vm, "unit": UNIT, "ms_per_step": ms_m / a.steps,
-                 "speedup_vs_fp64": vm / value, "relmax_vs_fp64": float(err_t.item()),
-                 "dtype": "f64+f32 (far-field quadrature bulk in f32)",
-                 "stage_ms_per_step": {k: v[0] / a.steps for k, v in stages_m.items()}}
-        del ref
+        res[prec] = {"value": out.numel() / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                     "stage_ms_per_step": {k: v[0] for k, v in st.items() if v[1]}}
+        if prec == "fp64":
+            ref = out.clone()
+        else:
+            res[prec]["relmax_vs_fp64"] = float(((out - ref).abs().max() / ref.abs().max()).item())
+            res[prec]["speedup_vs_fp64"] = res["fp64"]["ms_per_step"] / ms
+    del out, ref
+    torch.cuda.empty_cache()
+    return res
 
-    # end to end: pinned host inputs, H2D inside, full matrix read back
-    h_tris = torch.as_tensor(tris).pin_memory()
-    h_eps = torch.as_tensor(eps).pin_memory()
-    h_out = torch.empty((n, n, 3, 3), dtype=torch.float64).pin_memory()
-    e2e_steps = max(1, min(a.steps, 3))
+
+# ------------------------------------------------------------ serving
+# Scaled-down serving stream: seeded Poisson arrivals of uneven requests
+# (the serving configuration's distributions with the sizes scaled down so
+# the stream takes seconds): kind uniform in {disp, stress, traction,
+# interaction}, triangles log-uniform in [100, 2000], observers log-uniform
+# in [100, 5000], order uniform in {0, 1, 2}, eps per triangle 0.3 x edge.
+SERVE = {"requests": 48, "rate_per_s": 20.0, "tris": (100, 2000), "obs": (100, 5000)}
+
+
+def _submit_args(torch, dev, r, precision):
+    import mhs_b200 as mhs
+    t = torch.as_tensor(r["tris"], device=dev)
+    mat = mhs.Material(r["mu"], r["lam"])
+    eps = torch.as_tensor(np.broadcast_to(np.asarray(r["eps"], float), (t.shape[0],)).copy(),
+                          device=dev)
+    kw = {"order": r["order"], "precision": precision}
+    if r["kind"] == "interaction":
+        if "receiver" in r:
+            kw.update(receiver=r["receiver"], source=r["source"])
+        return mhs.interaction_matrix, (t, mat, eps), kw
+    o = torch.as_tensor(r["obs"], device=dev)
+    if r["kind"] == "disp":
+        return mhs.disp_matrix, (o, t, mat, eps), kw
+    if r["kind"] == "stress":
+        return mhs.stress_matrix, (o, t, mat, eps), kw
+    nrm = torch.as_tensor(r["normals"], device=dev)
+    return mhs.traction_matrix, (o, nrm, t, mat, eps), kw
+
+
+def _stream(dev, precision, reqs, slots, budget=None):
+    import torch
+    from mhs_b200 import serve
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    refused = 0
+    with serve.Server(dev, slots=slots, budget_bytes=budget) as srv:
+        futs = []
+        t0 = time.perf_counter()
+        for r in reqs:
+            delay = t0 + r["arrival_s"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            fn, args, kw = _submit_args(torch, dev, r, precision)
+            try:
+                futs.append(srv.submit(fn, *args, **kw))
+            except MemoryError:
+                refused += 1
+        for f in futs:
+            f.result()
+        t1 = time.perf_counter()
+        st = srv.stats()
+        st["peak_in_flight"] = srv.peak_in_flight
+    st["refused"] = refused
+    st["wall_s"] = t1 - t0
+    return st
+
+
+def serve_stream(dev, precision, seed):
+    """Latency percentiles and throughput of the scaled-down stream."""
+    from mhs_b200 import synthetic
+    reqs = synthetic.serving_requests(SERVE["requests"], seed=seed, rate_per_s=SERVE["rate_per_s"],
+                                      tri_range=SERVE["tris"], obs_range=SERVE["obs"],
+                                      strike_strike=())
+    return _stream(dev, precision, reqs, slots=8)
+
+
+def serve_full(dev, n_requests):
+    """The serving stream at its stated sizes (100-20k triangles, 100-50k
+    observers, strike/strike interactions at n = 10k and 20k), bounded to
+    `n_requests` arrivals at 20/s; admission by output bytes against a
+    150 GB budget (requests above it are refused and counted)."""
+    from mhs_b200 import synthetic
+    reqs = synthetic.serving_requests(n_requests, seed=5)
+    out = {"requests_offered": n_requests, "rate_per_s": 20.0, "budget_bytes": 150e9,
+           "sizes": {"tris": [100, 20000], "obs": [100, 50000], "strike_strike": [10000, 20000]}}
+    for prec in ("fp64", "mixed"):
+        out[prec] = _stream(dev, prec, reqs, slots=8, budget=int(150e9))
+    return out
+
+
+def batch_run(dev, precision, seed, budget=50e9):
+    """The batched configuration's 64 requests at their stated sizes through
+    mhs_b200.batch: packed into sub-batches of at most `budget` output and
+    scratch bytes (batch.split), each queued as one group of launches per class; a request
+    whose one-pass scratch is above the batch limit runs alone through its
+    public function.  Device time from the first submission to the last
+    completion (staging and planning apart), and the wall time of it all."""
+    import torch
+    from mhs_b200 import batch, synthetic
+    reqs = synthetic.batched_requests(64, seed=seed)
+    calls = [_submit_args(torch, dev, r, precision) for r in reqs]
+    groups, big = batch.split(calls, budget)
+    rest = [i for g in groups for i in g]
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(e2e_steps):
-        td = h_tris.to(dev, non_blocking=True)
-        ed = h_eps.to(dev, non_blocking=True)
-        r = mhs.interaction_matrix(td, mat, ed, out=out, precision=a.precision)
-        h_out.copy_(r, non_blocking=True)
-    e1.record()
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_ms = float(e2e_t.item())
-    e2e_val = world * entries * e2e_steps / (e2e_ms * 1e-3)
-
-    # serving: the seeded Poisson stream through the request loop, FP64 and mixed
-    serving = {"stream": dict(SERVE, note="sizes scaled down from the serving config; "
-                                        "arrivals Poisson, seeded; latency = submit to "
-                                        "result ready on the device, host clock"),
-               "fp64": serve_stream(dev, "fp64", 100 + rank),
-               "mixed": serve_stream(dev, "mixed", 100 + rank)}
-
-    batch = {"config": dict(BATCH, note="sizes scaled down from the batched config; all "
-                                        "submitted at once to the serving loop (stream overlap)"),
-             "fp64": batch_run(dev, "fp64", 200 + rank),
-             "mixed": batch_run(dev, "mixed", 200 + rank)}
-
-    # roofline of the dominant stage (the fold): algorithmic flops of the
-    # census'd work units over the stage's time per launch
-    top = max(stages, key=lambda s: stages[s][0])
-    top_ms, top_n = stages[top]
-    peak = _native.fp_peak(fp64=True)
-    achieved, fl = None, None
-    if top == "fold":
-        from mhs_b200 import flops as _flops
-        fl = _flops.fold_flops(census, order=0, want_h=True, mu=mu, lam=lam,
-                               eps=float(np.mean(eps)))
-        achieved = fl["flop"] / (top_ms / max(top_n, 1) * 1e-3) / 1e12
-    roof = {"bound": "fp64", "kernel": top, "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
-            "traffic": FOLD_TRAFFIC_PER_LAUNCH.get((a.nu, a.nv, a.precision)) if top == "fold" else None,
-            "peak_source": "measured FP64 FMA ceiling (mhs_fp_peak, this run)",
-            "algorithmic": None if fl is None else {
-                "flop_per_launch": fl["flop"], "div": fl["div"], "sqrt": fl["sqrt"],
-                "special": fl["special"], "census": census,
-                "counting": "op-counting host build of the engine (mhs_b200/csrc/opcount.cpp): "
-                            "add/sub/mul 1 flop, fma 2; div, sqrt, library calls apart"},
-            "stage_ms_per_step": {k: v[0] / a.steps for k, v in stages.items()},
-            "stage_launches_per_step": {k: v[1] / a.steps for k, v in stages.items()}}
-
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f64+f32",
-            "data": "synthetic (seeded rough fault mesh per rank)",
-            "config": {"workload": WORKLOAD, "n_tri": n, "entries_per_step": entries,
-                       "precision": a.precision, "global_batch": world,
-                       "l2": "L2 flushed between steps (256 MiB write); output 415 MB per step",
-                       "parallelism": f"replicas x{world}"},
-            "e2e": {"value": e2e_val, "unit": UNIT,
-                    "h2d_bytes_per_step": int(tris.nbytes + eps.nbytes),
-                    "d2h_bytes_per_step": int(entries * 8)},
-            "roofline": roof, "mixed": mixed, "serving": serving, "batch": batch,
-            "clocks": clk.summary(),
-            "gpu_launches": int(sum(v[1] * KERNELS_PER_STAGE[k] for k, v in stages.items()))}
-    return line, tris, eps, mu, lam
+    dev_ms, entries = 0.0, 0
+    for g in groups:
+        bt = batch.Batch([calls[i] for i in g], dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bt.run()
+        e1.record()
+        bt.wait()
+        dev_ms += e0.elapsed_time(e1)
+        entries += bt.entries
+        bt.close()
+        del bt
+    for i in big:
+        fn, args, kw = calls[i]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn(*args, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        dev_ms += e0.elapsed_time(e1)
+        entries += out.numel()
+        del out
+    torch.cuda.empty_cache()
+    wall = time.perf_counter() - t0
+    return {"device_s": dev_ms * 1e-3, "wall_s": wall, "entries": int(entries),
+            "entries_per_s": entries / (dev_ms * 1e-3), "sub_batches": len(groups),
+            "requests_batched": len(rest), "requests_alone": len(big)}
 
 
 def main():
     a = parse()
+    legs = set(x.strip() for x in a.legs.split(",") if x.strip())
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if a.impl == "reference":
@@ -491,7 +601,8 @@ def main():
         tris, eps, mu, lam = workload(0, a.nu, a.nv)
         vals = []
         for i in range(a.warmup + a.steps):
-            r = cpu_baseline(tris, eps, mu, lam, a.cpu_seconds, seed=100 + i)
+            r = cpu_baseline(tris, eps, mu, lam, a.cpu_seconds, seed=100 + i,
+                             fold_pairs=64 if i < a.warmup else 256)
             if i >= a.warmup:
                 vals.append(r)
         v = statistics.median(x["value"] for x in vals)
@@ -511,7 +622,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line, tris, eps, mu, lam = run_ours(a, rank, world)
+    line, tris, eps, mu, lam = run_ours(a, rank, world, legs)
     if rank == 0:
         if world == 1 and not a.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(tris, eps, mu, lam, a.cpu_seconds)

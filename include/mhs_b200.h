@@ -76,6 +76,14 @@ typedef struct mhs_request {
   void* out;                 /* output, C-contiguous, zero not required */
   void* workspace;
   size_t workspace_bytes;
+  /* Apply mode (slip != NULL): out receives the matrix times a slip vector,
+   * y[o][c] = sum over columns and slip components of M[o][c][col][s]
+   * slip[col][s], and the matrix itself is never stored.  slip is (n_dof,
+   * n_s) with n_s = 3 (Cartesian slip) or n_b (INTERACTION); out is (n_obs,
+   * C) with C = 3 (DISP, TRACTION), 9 (the stress-like kinds, [a][b]) or n_a
+   * (INTERACTION).  This is the product a cycle or cascade model reads
+   * (studies/active_fractal/kernel.py:1-30 keeps the whole K for it). */
+  const double* slip;
 } mhs_request;
 
 /* Bytes of workspace a request needs: *min_bytes for one observer row per
@@ -122,6 +130,65 @@ int mhs_assemble(const mhs_request* req, void* stream);
 #define MHS_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int mhs_assemble_noalloc(const mhs_request* req, void* stream, int* status_bits);
 
+/* ------------------------------------------------------------- batches
+ * A batch: n requests queued as one group of launches per (order, readout
+ * class, precision).  Each stage -- image coefficients, per-source data, the
+ * two pair kernels, the output stage -- runs once over every request of the
+ * group, its blocks finding their request by a prefix of block counts; the
+ * fold of a request with fold = 1 runs per request between the pair kernels
+ * and the output stage.  Every request runs in one pass over all its
+ * observers (a request whose one-pass scratch would exceed 8 GiB is refused;
+ * run it alone with mhs_assemble).  Apply-mode requests (slip != NULL) are
+ * grouped apart from matrix requests.
+ *   mhs_batch_pass_bytes  one request's one-pass scratch and the batch
+ *                         limit (host only), to split a list of requests
+ *                         into batches and requests to assemble alone
+ *   mhs_batch_create      checks and plans the requests (host only; their
+ *                         workspace fields are ignored; the array is copied)
+ *   mhs_batch_workspace_bytes   bytes of the one device arena of the batch
+ *   mhs_batch_bind        places each request's scratch and the launch
+ *                         descriptors in the arena (copies queued on stream)
+ *   mhs_submit_batch      queues the batch's kernels on stream.  With no
+ *                         request at fold = 1 it queues kernels only, so it
+ *                         can be captured into a CUDA graph and replayed
+ *                         (a request whose sources all lie deeper than
+ *                         FOLD_SOURCE_DEPTH_EPS eps gives the same result at
+ *                         fold = 0); a request at fold = 1 makes the call
+ *                         synchronise the stream to read its fold plan.
+ *   mhs_poll              *done = 1 once the last submission has completed,
+ *                         and then *status_bits = the OR of the requests'
+ *                         device status bits
+ *   mhs_batch_destroy
+ * Inputs and outputs stay the caller's device buffers; a replay reads them
+ * as they are at the time.  No counterpart in mhs, which has no launch to
+ * amortise (mhs/chunking.py:3-6) and batches only by processes
+ * (mhs/parallel.py:132-221). */
+typedef struct mhs_batch mhs_batch;
+int mhs_batch_pass_bytes(const mhs_request* req, size_t* bytes, size_t* limit);
+int mhs_batch_create(const mhs_request* reqs, int n, mhs_batch** batch);
+int mhs_batch_workspace_bytes(const mhs_batch* batch, size_t* bytes);
+int mhs_batch_bind(mhs_batch* batch, void* workspace, size_t bytes, void* stream);
+int mhs_submit_batch(mhs_batch* batch, void* stream);
+int mhs_poll(mhs_batch* batch, int* done, int* status_bits);
+int mhs_batch_destroy(mhs_batch* batch);
+
+/* Launch shapes of one (order, readout class, precision) on the current
+ * device: threads per block of the two pair kernels (observer tile, 32 to
+ * 128) and of the output stage (column tile, 32 to 128), and the grid
+ * multipliers of the fold's far- and near-load kernels (blocks per SM at
+ * full occupancy x the multiplier, 1 to 16).  None of them changes a
+ * result: each thread's arithmetic is the same under every shape.
+ * mhs_autotune times the sample request (its workspace included) under each
+ * candidate shape -- pair and output tiles 64 or 128, multipliers 2, 4 or
+ * 8 -- keeps the fastest for the sample's class, returns it and its time.
+ * No counterpart in mhs. */
+typedef struct mhs_tune {
+  int pair_tb, final_tb, far_mult, near_mult;
+} mhs_tune;
+int mhs_autotune(const mhs_request* sample, void* stream, mhs_tune* chosen, double* best_ms);
+int mhs_set_tune(const mhs_request* like, const mhs_tune* tune);
+int mhs_get_tune(const mhs_request* like, mhs_tune* tune);
+
 /* Synchronise `stream` and return the device status bits of the last
  * request that used `workspace` (0 = clean), clearing them.  workspace =
  * NULL reads the status of the last mhs_assemble_noalloc call on the
@@ -158,10 +225,20 @@ enum mhs_stage {
   MHS_STAGE_IMAGEQ = 2,  /* image Q-family */
   MHS_STAGE_FOLD = 3,    /* band lists + folded image */
   MHS_STAGE_FINAL = 4,   /* eigenstress, contraction, layout stores */
-  MHS_N_STAGES = 5
+  /* parts of the fold stage (their time is inside MHS_STAGE_FOLD's) */
+  MHS_STAGE_FOLD_PLAN = 5,   /* band scan, pair and panel plan, foot loads */
+  MHS_STAGE_FOLD_NODES = 6,  /* polar-grid nodes and their class lists */
+  MHS_STAGE_FOLD_FAR = 7,    /* far-field surface loads (12 x 12, 8 x 8 rules) */
+  MHS_STAGE_FOLD_NEAR = 8,   /* near-field surface loads (closed form) */
+  MHS_STAGE_FOLD_ACCUM = 9,  /* point-load products, panel sums, disk term */
+  MHS_N_STAGES = 10
 };
 int mhs_profile_enable(int on);
 int mhs_profile_read(double* ms, int* launches);
+
+/* Kernels this library queued (all devices, all threads) since the last
+ * call; the count is returned and reset.  No counterpart in mhs. */
+int mhs_kernel_count(unsigned long long* n);
 
 /* Fold work census (measurement).  While enabled, the fold kernel counts its
  * work units into device counters: band pairs, radial panels, polar-grid

@@ -15,12 +15,16 @@ from .materials import Material
 from .matrices import (
     collocation_points,
     disp_matrix,
+    disp_matvec,
     eigenstress_matrix,
     elastic_strain_matrix,
     interaction_matrix,
+    interaction_matvec,
     stress_matrix,
+    stress_matvec,
     total_stress_matrix,
     traction_matrix,
+    traction_matvec,
 )
 from .shared import SharedNodes, shared_nodes
 
@@ -34,6 +38,10 @@ __all__ = [
     "eigenstress_matrix",
     "elastic_strain_matrix",
     "collocation_points",
+    "interaction_matvec",
+    "disp_matvec",
+    "stress_matvec",
+    "traction_matvec",
     "shared_nodes",
     "SharedNodes",
     "chunking",

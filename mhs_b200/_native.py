@@ -46,14 +46,24 @@ class Request(ctypes.Structure):
         ("out", ctypes.c_void_p),
         ("workspace", ctypes.c_void_p),
         ("workspace_bytes", ctypes.c_size_t),
+        ("slip", ctypes.c_void_p),
     ]
+
+
+class Tune(ctypes.Structure):
+    """Mirror of ``struct mhs_tune``."""
+
+    _fields_ = [("pair_tb", ctypes.c_int), ("final_tb", ctypes.c_int),
+                ("far_mult", ctypes.c_int), ("near_mult", ctypes.c_int)]
 
 
 #: Symbols the header declares; a test checks the library exports each.
 EXPORTS = ("mhs_workspace_bytes", "mhs_assemble", "mhs_read_status", "mhs_column_plan",
            "mhs_last_error", "mhs_version", "mhs_profile_enable", "mhs_profile_read",
            "mhs_fp_peak", "mhs_debug_terms", "mhs_assemble_noalloc", "mhs_census_enable",
-           "mhs_census_read")
+           "mhs_census_read", "mhs_kernel_count", "mhs_batch_create", "mhs_batch_workspace_bytes",
+           "mhs_batch_bind", "mhs_submit_batch", "mhs_poll", "mhs_batch_destroy", "mhs_autotune",
+           "mhs_set_tune", "mhs_get_tune", "mhs_batch_pass_bytes")
 
 _lib = None
 
@@ -99,11 +109,30 @@ def load() -> ctypes.CDLL:
     lib.mhs_census_enable.restype = ctypes.c_int
     lib.mhs_census_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)]
     lib.mhs_census_read.restype = ctypes.c_int
+    lib.mhs_kernel_count.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.mhs_kernel_count.restype = ctypes.c_int
+    V = ctypes.c_void_p
+    lib.mhs_batch_create.argtypes = [R, ctypes.c_int, ctypes.POINTER(V)]
+    lib.mhs_batch_workspace_bytes.argtypes = [V, ctypes.POINTER(ctypes.c_size_t)]
+    lib.mhs_batch_bind.argtypes = [V, V, ctypes.c_size_t, V]
+    lib.mhs_submit_batch.argtypes = [V, V]
+    lib.mhs_poll.argtypes = [V, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    lib.mhs_batch_destroy.argtypes = [V]
+    lib.mhs_batch_pass_bytes.argtypes = [R, ctypes.POINTER(ctypes.c_size_t),
+                                         ctypes.POINTER(ctypes.c_size_t)]
+    lib.mhs_autotune.argtypes = [R, V, ctypes.POINTER(Tune), ctypes.POINTER(ctypes.c_double)]
+    lib.mhs_set_tune.argtypes = [R, ctypes.POINTER(Tune)]
+    lib.mhs_get_tune.argtypes = [R, ctypes.POINTER(Tune)]
+    for f in ("mhs_batch_create", "mhs_batch_workspace_bytes", "mhs_batch_bind", "mhs_submit_batch",
+              "mhs_poll", "mhs_batch_destroy", "mhs_autotune", "mhs_set_tune", "mhs_get_tune",
+              "mhs_batch_pass_bytes"):
+        getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
 
 
-STAGES = ("prep", "pair", "imageq", "fold", "final")
+STAGES = ("prep", "pair", "imageq", "fold", "final", "fold_plan", "fold_nodes", "fold_far",
+          "fold_near", "fold_accum")
 
 
 def profile(on: bool) -> None:
@@ -131,6 +160,13 @@ def census_read() -> dict:
     c = (ctypes.c_ulonglong * len(CENSUS))()
     check(load().mhs_census_read(c))
     return {k: int(c[i]) for i, k in enumerate(CENSUS)}
+
+
+def kernel_count() -> int:
+    """Kernels the library queued since the last call (the count resets)."""
+    n = ctypes.c_ulonglong()
+    check(load().mhs_kernel_count(ctypes.byref(n)))
+    return int(n.value)
 
 
 def fp_peak(fp64: bool = True, iters: int = 1 << 16, stream=None) -> float:

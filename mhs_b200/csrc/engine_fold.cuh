@@ -113,6 +113,47 @@ MHS_HD void point_stress6(double dx, double dy, double zeta, double nu, double* 
   S[5] = t_rz * ey;
 }
 
+// point_stress6 with the radii from reciprocal square roots and one
+// division (rounding-level differences): the fold's accumulation kernel.
+MHS_HD void point_stress6_rcp(double dx, double dy, double zeta, double nu, double* S) {
+  const double r2 = dx * dx + dy * dy;
+  const double q = r2 + zeta * zeta;
+  const double irho = rsqrt_r(q);
+  const double rho = q * irho;
+  const double irho2 = irho * irho;
+  const double irho3 = irho2 * irho;
+  const double irho5 = irho3 * irho2;
+  const double a = irho / (rho + zeta);
+  const double c = 1.0 - 2.0 * nu;
+  const double zr3 = zeta * irho3;
+  const double s_th = c * (-a + zr3);
+  const double s_r_th = 2.0 * c * a - 3.0 * zeta * r2 * irho5 - c * zr3;
+  const double ir = r2 > 0.0 ? rsqrt_r(r2) : 0.0;
+  const double r = r2 * ir;
+  const double ex = dx * ir, ey = dy * ir;
+  const double pref = 1.0 / (2.0 * cst::PI);
+  S[0] = pref * (s_th + s_r_th * ex * ex);
+  S[1] = pref * (s_th + s_r_th * ey * ey);
+  S[2] = -pref * 3.0 * (zeta * zeta * zeta) * irho5;
+  S[3] = pref * s_r_th * ex * ey;
+  const double t_rz = pref * 3.0 * r * zeta * zeta * irho5;
+  S[4] = t_rz * ex;
+  S[5] = t_rz * ey;
+}
+
+// point_disp3 with the radius from a reciprocal square root.
+MHS_HD void point_disp3_rcp(double dx, double dy, double zeta, double mu, double nu, double* u) {
+  const double q = dx * dx + dy * dy + zeta * zeta;
+  const double irho = rsqrt_r(q);
+  const double rho = q * irho;
+  const double irho3 = irho * irho * irho;
+  const double pref = 1.0 / (4.0 * cst::PI * mu);
+  const double ur = pref * (zeta * irho3 - (1.0 - 2.0 * nu) * (irho / (rho + zeta)));
+  u[0] = ur * dx;
+  u[1] = ur * dy;
+  u[2] = -pref * (2.0 * (1.0 - nu) * irho + zeta * zeta * irho3);
+}
+
 MHS_HD void point_disp3(double dx, double dy, double zeta, double mu, double nu, double* u) {
   const double r2 = dx * dx + dy * dy;
   const double rho = sqrt(r2 + zeta * zeta);

@@ -203,7 +203,7 @@ MHS_HD void szz_coefficient(const Frame& f, double eps, const Material& m, int l
 template <int P, int WANT, class R_FAR = double, class Q = QuadRule>
 MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
                         const double* x, double eps, const Material& m,
-                        double* U, double* H, double* E) {
+                        double* U, double* H, double* E, double near_l = cst::D_STAR) {
   using S = DirectSpec<P, WANT>;
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
@@ -214,7 +214,9 @@ MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
   to_plane(f, x, z, X0, X1);
   const double h2 = z * z + eps * eps;
   const double e4 = 15.0 * (eps * eps) * (eps * eps) / (8.0 * cst::PI);
-  if (D <= cst::D_STAR * f.L) {
+  // closed form within D_STAR element lengths (near_l < D_STAR: the mixed
+  // form's narrower closed-form zone, the far rule beyond it)
+  if (D <= cst::D_STAR * f.L && D <= near_l * f.L) {
     MomentTable<S> T;
     closed_moments<S>(f, X0, X1, h2, T);
     double c[K][ntri(P)];
@@ -355,10 +357,11 @@ MHS_HD void contract_ddg(const double* DDG, const double* nrm, const Material& m
 // The closed-form R-family on the reflected element (mhs/kernels/image.py:
 // 435-497): weighted tables of the image frame, Cartesian monomial moments
 // D1^a D2^b D3^c / R2^n from the basis products G, then the generated records.
-template <int P, int WANT, class R_FAR = double>
+template <int P, int WANT, class R_FAR = double, class Q = QuadRule>
 MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
-                         const QuadRule& r12, const QuadRule& r8, const double* x, double eps,
-                         const Material& m, const ImageCoef& ic, double* U, double* H) {
+                         const Q& r12, const Q& r8, const double* x, double eps,
+                         const Material& m, const ImageCoef& ic, double* U, double* H,
+                         double near_l = cst::D_STAR) {
   using S = SpecImg<P>;
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
@@ -373,14 +376,14 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
   zpow[0] = 1.0;
   for (int i = 1; i <= G_RMAX; ++i) zpow[i] = zpow[i - 1] * zp;
   double Wall[K * NW] = {};
-  if (D <= cst::D_STAR * fi.L) {
+  if (D <= cst::D_STAR * fi.L && D <= near_l * fi.L) {
     MomentTable<S> T;
     closed_moments<S>(fi, X0, X1, h2, T);
     double c[K][ntri(P)];
     shape_coeffs<P>(fi, X0, X1, c);
     for (int k = 0; k < K; ++k) weight_closed<S, P>(T, c, k, Wall + k * NW);
   } else {
-    const QuadRule& q = (D > cst::D_STAR_DISTANT * fi.L) ? r8 : r12;
+    const Q& q = (D > cst::D_STAR_DISTANT * fi.L) ? r8 : r12;
     weight_far<S, P, R_FAR>(q, X0, X1, h2, Wall);
   }
 #pragma unroll 1

@@ -31,6 +31,7 @@
 namespace fold_waves {
 
 constexpr int NCLS = 12;          // 10 near signatures, far 12 x 12, far 8 x 8
+
 constexpr int CLS_FAR12 = 10;
 constexpr int CLS_FAR8 = 11;
 
@@ -338,86 +339,125 @@ __device__ __forceinline__ int panel_pair(const long long* pair_poff, int np, lo
   return a;
 }
 
-// Nodes of the wave's panels: position, weight, pair, class.  One block per
-// panel (grid-stride over the wave's panels).
+// Nodes of the wave's panels: position, weight, pair, class.  One warp per
+// panel (grid-stride over the wave's panels): each lane takes angular nodes
+// j (one sincos each) and writes the panel's six radial nodes at j, in the
+// grid's order ir * n_ang + j.
 template <int P>
 __global__ void __launch_bounds__(256)
-k_nodes(int np, int64_t lo, const double* __restrict__ obs, const SrcPrep* __restrict__ prep,
-        const int* __restrict__ st_src, const int* __restrict__ pair_st,
-        const int* __restrict__ pair_oc, const long long* __restrict__ pair_poff,
-        const double* __restrict__ pan_ra, const double* __restrict__ pan_rb,
-        const long long* __restrict__ pan_noff, Hdr* __restrict__ hdr,
-        double* __restrict__ npx, double* __restrict__ npy, double* __restrict__ nw,
-        int* __restrict__ npair, unsigned char* __restrict__ ncls) {
-  __shared__ AngRule A;
-  __shared__ FoldPair fp;
-  __shared__ int s_pair;
-  __shared__ int s_cnt[NCLS];
+k_nodes(double near_l, int np, int64_t lo, const double* __restrict__ obs,
+        const SrcPrep* __restrict__ prep, const int* __restrict__ st_src,
+        const int* __restrict__ pair_st, const int* __restrict__ pair_oc,
+        const long long* __restrict__ pair_poff, const double* __restrict__ pan_ra,
+        const double* __restrict__ pan_rb, const long long* __restrict__ pan_noff,
+        const Hdr* __restrict__ hdr, double* __restrict__ npx, double* __restrict__ npy,
+        double* __restrict__ nw, int* __restrict__ npair, unsigned char* __restrict__ ncls) {
+  constexpr int NR = cst::FOLD_N_RADIAL;
+  __shared__ AngRule sA[8];
+  __shared__ FoldPair sfp[8];
+  __shared__ int spair[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const long long q0 = hdr->wave_q0, q1 = hdr->wave_q1, n0 = hdr->wave_n0;
-  const double* gx6 = d_glx + gl_offset(cst::FOLD_N_RADIAL);
-  const double* gw6 = d_glw + gl_offset(cst::FOLD_N_RADIAL);
+  const double* gx6 = d_glx + gl_offset(NR);
+  const double* gw6 = d_glw + gl_offset(NR);
   const double* gx4 = d_glx + gl_offset(cst::FOLD_N_ANGULAR);
   const double* gw4 = d_glw + gl_offset(cst::FOLD_N_ANGULAR);
-  for (long long q = q0 + blockIdx.x; q < q1; q += gridDim.x) {
-    if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
-    if (threadIdx.x == 0) {
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long q = q0 + (long long)blockIdx.x * (blockDim.x >> 5) + wid; q < q1; q += nwarps) {
+    if (lane == 0) {
       const int i = panel_pair(pair_poff, np, q);
       const SrcPrep& sp = prep[st_src[pair_st[i]]];
       FoldPair f;
       pair_geom(obs, lo, pair_oc[i], sp, f);
-      fold_panel_rule(f, pan_ra[q], pan_rb[q], A);
-      fp = f;
-      s_pair = i;
+      fold_panel_rule(f, pan_ra[q], pan_rb[q], sA[wid]);
+      sfp[wid] = f;
+      spair[wid] = i;
     }
-    __syncthreads();
-    const int i = s_pair;
+    __syncwarp();
+    const AngRule& A = sA[wid];
+    const FoldPair& fp = sfp[wid];
+    const int i = spair[wid];
     const SrcPrep& sp = prep[st_src[pair_st[i]]];
     const double ra = pan_ra[q], rb = pan_rb[q];
-    const int na = A.n;
-    const long long npts = (long long)cst::FOLD_N_RADIAL * (na > 0 ? na : 0);
+    const int na = A.n > 0 ? A.n : 0;
     const long long base = pan_noff[q] - n0;
-    for (long long t = threadIdx.x; t < npts; t += blockDim.x) {
-      const int ir = (int)(t / na), jn = (int)(t % na);
-      const double R = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
-      const double wr = (rb - ra) * (0.5 * gw6[ir]);
+    double R[NR], wr[NR];
+#pragma unroll
+    for (int ir = 0; ir < NR; ++ir) {
+      R[ir] = ra + (rb - ra) * (0.5 * (gx6[ir] + 1.0));
+      wr[ir] = (rb - ra) * (0.5 * gw6[ir]);
+    }
+    for (int jn = lane; jn < na; jn += 32) {
       double th, wt;
       fold_ang_node(A, gx4, gw4, jn, &th, &wt);
       double sn, cs;
       sincos(th, &sn, &cs);
-      const double px = fp.xh0 + R * cs, py = fp.xh1 + R * sn;
-      int cls = surface_class(sp.f, px, py, sp.eps);
-      if (cls == SL_NEAR) {
-        const double xx[3] = {px, py, 0.0};
-        double z, X0, X1;
-        to_plane(sp.f, xx, z, X0, X1);
-        const double h2 = z * z + sp.eps * sp.eps;
-        double pr[3][2];
-        foot_vertices(sp.f, X0, X1, pr);
-        int ns = 0, nl = 0;
 #pragma unroll
-        for (int e = 0; e < 3; ++e) {
-          const EdgeGeom g = edge_geom_rcp(pr, e, h2);
-          const int form = edge_regime_sq(g.ua, g.ub, g.rho2);
-          ns += form == EDGE_SMALL;
-          nl += form == EDGE_LARGE;
+      for (int ir = 0; ir < NR; ++ir) {
+        const double px = fp.xh0 + R[ir] * cs, py = fp.xh1 + R[ir] * sn;
+        int cls = surface_class(sp.f, px, py, sp.eps);
+        if (cls == SL_NEAR && near_l < cst::D_STAR) {
+          // the mixed form: closed form only within near_l element lengths
+          const double d0 = px - sp.f.c[0], d1 = py - sp.f.c[1], d2 = 0.0 - sp.f.c[2];
+          const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + sp.eps * sp.eps);
+          if (D > near_l * sp.f.L) cls = SL_FAR12;
         }
-        cls = near_sig(ns, nl);
-      } else {
-        cls = cls == SL_FAR8 ? CLS_FAR8 : CLS_FAR12;
+        if (cls == SL_NEAR) {
+          const double xx[3] = {px, py, 0.0};
+          double z, X0, X1;
+          to_plane(sp.f, xx, z, X0, X1);
+          const double h2 = z * z + sp.eps * sp.eps;
+          double pr[3][2];
+          foot_vertices(sp.f, X0, X1, pr);
+          int ns = 0, nl = 0;
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+            const EdgeGeom g = edge_geom_rcp(pr, e, h2);
+            const int form = edge_regime_sq(g.ua, g.ub, g.rho2);
+            ns += form == EDGE_SMALL;
+            nl += form == EDGE_LARGE;
+          }
+          cls = near_sig(ns, nl);
+        } else {
+          cls = cls == SL_FAR8 ? CLS_FAR8 : CLS_FAR12;
+        }
+        const long long u = base + (long long)ir * na + jn;
+        npx[u] = px;
+        npy[u] = py;
+        nw[u] = wr[ir] * wt * R[ir];
+        npair[u] = i;
+        ncls[u] = (unsigned char)cls;
       }
-      const long long u = base + t;
-      npx[u] = px;
-      npy[u] = py;
-      nw[u] = wr * wt * R;
-      npair[u] = i;
-      ncls[u] = (unsigned char)cls;
-      atomicAdd(&s_cnt[cls], 1);
     }
-    __syncthreads();
-    if (threadIdx.x < NCLS && s_cnt[threadIdx.x])
-      atomicAdd(&hdr->cls_count[threadIdx.x], s_cnt[threadIdx.x]);
-    __syncthreads();
+    __syncwarp();
   }
+}
+
+// Class counts of the wave's nodes (block-aggregated: one global add per
+// class per block tile).
+constexpr int SCAT_PER_THREAD = 4;
+
+__global__ void __launch_bounds__(256)
+k_count(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls) {
+  __shared__ int s_cnt[NCLS];
+  const long long n = hdr->wave_nodes;
+  const long long tile = (long long)blockDim.x * SCAT_PER_THREAD;
+  if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (long long t0 = (long long)blockIdx.x * tile; t0 < n; t0 += (long long)gridDim.x * tile) {
+#pragma unroll
+    for (int k = 0; k < SCAT_PER_THREAD; ++k) {
+      const long long u = t0 + (long long)k * blockDim.x + threadIdx.x;
+      const int cls = u < n ? ncls[u] : -1;
+#pragma unroll 1
+      for (int c = 0; c < NCLS; ++c) {
+        const unsigned m = __ballot_sync(0xffffffffu, cls == c);
+        if (m && (threadIdx.x & 31) == 0) atomicAdd(&s_cnt[c], __popc(m));
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < NCLS && s_cnt[threadIdx.x]) atomicAdd(&hdr->cls_count[threadIdx.x], s_cnt[threadIdx.x]);
 }
 
 // Class offsets of the wave (and the census of its nodes and near edges).
@@ -446,29 +486,77 @@ __global__ void k_wave_classes(Hdr* __restrict__ hdr, unsigned long long* __rest
   }
 }
 
-// Node indices into their class lists (one thread per node; warp-aggregated
-// appends).
+// Node indices into their class lists: per block tile of
+// SCAT_PER_THREAD x blockDim nodes, the warps' class counts are combined in
+// shared memory and each class takes one global add per tile.
 __global__ void __launch_bounds__(256)
 k_scatter(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls, int* __restrict__ nlist) {
+  constexpr int WMAX = 8;
+  __shared__ int w_cnt[SCAT_PER_THREAD][WMAX][NCLS];
+  __shared__ int b_base[NCLS];
   const long long n = hdr->wave_nodes;
-  const int lane = threadIdx.x & 31;
-  for (long long u0 = (long long)blockIdx.x * blockDim.x; u0 < n; u0 += (long long)gridDim.x * blockDim.x) {
-    const long long u = u0 + threadIdx.x;
-    const int cls = u < n ? ncls[u] : -1;
-#pragma unroll 1
-    for (int c = 0; c < NCLS; ++c) {
-      const unsigned m = __ballot_sync(0xffffffffu, cls == c);
-      if (!m) continue;
-      const int leader = __ffs(m) - 1;
-      int base = 0;
-      if (lane == leader) base = atomicAdd(&hdr->cls_fill[c], __popc(m));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (cls == c) nlist[hdr->cls_off[c] + base + __popc(m & ((1u << lane) - 1u))] = (int)u;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long tile = (long long)blockDim.x * SCAT_PER_THREAD;
+  for (long long t0 = (long long)blockIdx.x * tile; t0 < n; t0 += (long long)gridDim.x * tile) {
+    int cls[SCAT_PER_THREAD];
+    unsigned mk[SCAT_PER_THREAD];
+#pragma unroll
+    for (int k = 0; k < SCAT_PER_THREAD; ++k) {
+      const long long u = t0 + (long long)k * blockDim.x + threadIdx.x;
+      cls[k] = u < n ? ncls[u] : -1;
+      mk[k] = 0;
     }
+    // per warp, per sub-tile: count of each class, and this lane's mask
+#pragma unroll
+    for (int k = 0; k < SCAT_PER_THREAD; ++k)
+#pragma unroll 1
+      for (int c = 0; c < NCLS; ++c) {
+        const unsigned m = __ballot_sync(0xffffffffu, cls[k] == c);
+        if (cls[k] == c) mk[k] = m;
+        if (lane == 0) w_cnt[k][wid][c] = __popc(m);
+      }
+    __syncthreads();
+    if (threadIdx.x < NCLS) {
+      const int c = threadIdx.x;
+      int tot = 0;
+      for (int k = 0; k < SCAT_PER_THREAD; ++k)
+        for (int w = 0; w < nw; ++w) tot += w_cnt[k][w][c];
+      b_base[c] = tot ? atomicAdd(&hdr->cls_fill[c], tot) : 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SCAT_PER_THREAD; ++k) {
+      const int c = cls[k];
+      if (c >= 0) {
+        int off = b_base[c];
+        for (int kk = 0; kk < k; ++kk)
+          for (int w = 0; w < nw; ++w) off += w_cnt[kk][w][c];
+        for (int w = 0; w < wid; ++w) off += w_cnt[k][w][c];
+        off += __popc(mk[k] & ((1u << lane) - 1u));
+        const long long u = t0 + (long long)k * blockDim.x + threadIdx.x;
+        nlist[hdr->cls_off[c] + off] = (int)u;
+      }
+    }
+    __syncthreads();
   }
 }
 
-// Far loads: one thread per node of the far lists.
+// Far loads: one thread per node of the far lists (two consecutive list
+// entries per thread at constant slip, sharing each rule node's loads when
+// they belong to the same source and rule).
+template <int P, int KC, class RF>
+__device__ __forceinline__ QuadRuleT<RF> far_rule(const Src<P, RF>& d, bool r8) {
+  constexpr int K = n_nodes(P), N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
+  constexpr int N8 = cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
+  const int off = r8 ? N12 : 0;
+  if constexpr (std::is_same<RF, float>::value)
+    return QuadRuleT<float>{r8 ? N8 : N12, d.fr.e0 + off, d.fr.e1 + off, d.fr.wq + off,
+                            d.fr.Nq + off * K};
+  else
+    return QuadRuleT<double>{r8 ? N8 : N12, d.rd.e0 + off, d.rd.e1 + off, d.rd.wq + off,
+                             d.rd.Nq + off * K};
+}
+
 template <int P, int KC, class RF>
 __global__ void __launch_bounds__(128)
 k_far(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* __restrict__ npx,
@@ -476,32 +564,68 @@ k_far(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* 
       const int* __restrict__ pair_st, int j0, const int* __restrict__ st_src,
       const SrcPrep* __restrict__ prep, const Src<P, RF>* __restrict__ srcs,
       double* __restrict__ load, long long cap) {
+  using S = SurfaceSpec<P>;
+  constexpr Spec spc = S::spec;
+  constexpr int NW = spc.w_off[NS];
   constexpr int K = n_nodes(P);
   constexpr int NJ = 3 * K;
-  constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
+  constexpr int STEP = 1;   // one node per thread (two-node blocking measured slower)
   const long long a = hdr->cls_off[CLS_FAR12], b = hdr->cls_off[CLS_FAR8 + 1];
-  for (long long e = a + (long long)blockIdx.x * blockDim.x + threadIdx.x; e < b;
-       e += (long long)gridDim.x * blockDim.x) {
+  const long long r8_from = hdr->cls_off[CLS_FAR8];
+  for (long long e = a + STEP * ((long long)blockIdx.x * blockDim.x + threadIdx.x); e < b;
+       e += (long long)STEP * gridDim.x * blockDim.x) {
     const int u = nlist[e];
     const int j = pair_st[npair[u]];
     const SrcPrep& sp = prep[st_src[j]];
     const Src<P, RF>& d = srcs[j - j0];
-    const bool r8 = e >= hdr->cls_off[CLS_FAR8];
+    const bool r8 = e >= r8_from;
     const double xx[3] = {npx[u], npy[u], 0.0};
     double z, X0, X1;
     to_plane(sp.f, xx, z, X0, X1);
-    double sl[NJ] = {};
-    if constexpr (std::is_same<RF, float>::value) {
-      const int off = r8 ? N12 : 0;
-      const QuadRuleT<float> q{r8 ? cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT : N12,
-                               d.fr.e0 + off, d.fr.e1 + off, d.fr.wq + off, d.fr.Nq + off * K};
-      surface_load_far<P, RF>(q, d.slc, z, X0, X1, z * z + sp.eps * sp.eps, sl);
-    } else {
-      surface_load_far<P, RF>(r8 ? d.rd.r8() : d.rd.r12(), d.slc, z, X0, X1,
-                              z * z + sp.eps * sp.eps, sl);
-    }
+    const double h2 = z * z + sp.eps * sp.eps;
+    if constexpr (STEP == 2) {
+      // the entry after this one, when it shares source and rule
+      int u2 = -1;
+      if (e + 1 < b && ((e + 1 >= r8_from) == r8)) {
+        const int v = nlist[e + 1];
+        if (pair_st[npair[v]] == j) u2 = v;
+      }
+      double sa[NJ] = {}, sb[NJ] = {};
+      if (u2 >= 0) {
+        const double xy[3] = {npx[u2], npy[u2], 0.0};
+        double z2, Y0, Y1;
+        to_plane(sp.f, xy, z2, Y0, Y1);
+        double Wa[NW], Wb[NW];
+        weight_far2<S, RF>(far_rule<P, KC, RF>(d, r8), X0, X1, h2, Y0, Y1,
+                           z2 * z2 + sp.eps * sp.eps, Wa, Wb);
+        surface_load_node<S>(d.slc, Wa, z, sa);
+        surface_load_node<S>(d.slc, Wb, z2, sb);
 #pragma unroll
-    for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sl[jj];
+        for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u2] = sb[jj];
+      } else {
+        surface_load_far<P, RF>(far_rule<P, KC, RF>(d, r8), d.slc, z, X0, X1, h2, sa);
+        if (e + 1 < b) {  // the next entry on its own
+          const int v = nlist[e + 1];
+          const int jv = pair_st[npair[v]];
+          const SrcPrep& spv = prep[st_src[jv]];
+          const Src<P, RF>& dv = srcs[jv - j0];
+          const double xy[3] = {npx[v], npy[v], 0.0};
+          double z2, Y0, Y1;
+          to_plane(spv.f, xy, z2, Y0, Y1);
+          surface_load_far<P, RF>(far_rule<P, KC, RF>(dv, e + 1 >= r8_from), dv.slc, z2, Y0, Y1,
+                                  z2 * z2 + spv.eps * spv.eps, sb);
+#pragma unroll
+          for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + v] = sb[jj];
+        }
+      }
+#pragma unroll
+      for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sa[jj];
+    } else {
+      double sl[NJ] = {};
+      surface_load_far<P, RF>(far_rule<P, KC, RF>(d, r8), d.slc, z, X0, X1, h2, sl);
+#pragma unroll
+      for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sl[jj];
+    }
   }
 }
 
@@ -590,106 +714,102 @@ k_near(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double*
   }
 }
 
-// Accumulation of the wave: one warp per pair with panels in the wave,
-// panel by panel in grid order.  The lanes form G groups; group g holds the
-// load components jj in [g * NJG, (g + 1) * NJG) of all NC point-load
-// components and strides over the panel's nodes; each panel's partial sums
-// are reduced across the group in a fixed tree and added, in panel order,
-// to the pair's running sums acc[pair][c * NJ + jj].
+// Accumulation: per panel, the weighted point-load products of its nodes
+// summed by one warp (lanes in G groups; group g holds the load components
+// jj in [g * NJG, (g + 1) * NJG) of all NC point-load components and
+// strides over the panel's nodes; each group's partials are reduced in a
+// fixed butterfly order) into part[q][c * NJ + jj]; then, per pair, the
+// panel sums added in grid order (k_pair_sum).  Neither order depends on
+// how panels were grouped into waves.
 template <int P, int KC>
 struct AccumShape {
   static constexpr int K = n_nodes(P);
   static constexpr int NJ = 3 * K;
   static constexpr int NC = KC == KD_HE ? 6 : 3;
-  static constexpr int G = NJ * NC > 60 ? 2 : 1;    // lane groups
+  static constexpr int NOUT = NC * NJ;
+  static constexpr int G = NOUT <= 27 ? 1 : (NOUT <= 54 ? 2 : 4);   // lane groups
   static constexpr int NJG = (NJ + G - 1) / G;
   static constexpr int LANES = 32 / G;
-  static constexpr int NOUT = NC * NJ;
 };
 
+constexpr int ACCUM_WARPS = 4;
+
 template <int P, int KC>
-__global__ void __launch_bounds__(128)
-k_accum(int np, int64_t lo, const double* __restrict__ obs, const SrcPrep* __restrict__ prep,
-        const int* __restrict__ st_src, const int* __restrict__ pair_st,
-        const int* __restrict__ pair_oc, const long long* __restrict__ pair_poff,
-        const long long* __restrict__ pan_noff, const Hdr* __restrict__ hdr,
-        const double* __restrict__ npx, const double* __restrict__ npy,
-        const double* __restrict__ nw, const double* __restrict__ load, long long cap,
-        const double* __restrict__ foot, double mu, double lam, double* __restrict__ acc) {
+__global__ void __launch_bounds__(32 * ACCUM_WARPS)
+k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restrict__ pair_oc,
+        const long long* __restrict__ pair_poff, const long long* __restrict__ pan_noff,
+        const Hdr* __restrict__ hdr, const double* __restrict__ npx,
+        const double* __restrict__ npy, const double* __restrict__ nw,
+        const double* __restrict__ load, long long cap, const double* __restrict__ foot,
+        double mu, double lam, double* __restrict__ part) {
   using A = AccumShape<P, KC>;
-  constexpr int NJ = A::NJ, NC = A::NC, NJG = A::NJG, LANES = A::LANES;
+  constexpr int NJ = A::NJ, NC = A::NC, NJG = A::NJG, LANES = A::LANES, NOUT = A::NOUT;
   const Material m = make_material(mu, lam);
   const long long q0 = hdr->wave_q0, q1 = hdr->wave_q1, n0 = hdr->wave_n0;
-  if (q1 <= q0) return;
-  const int pa = panel_pair(pair_poff, np, q0), pb = panel_pair(pair_poff, np, q1 - 1);
-  const int lane = threadIdx.x & 31, grp = lane / LANES, gl = lane % LANES;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = pa + warp; i <= pb; i += nwarps) {
-    const SrcPrep& sp = prep[st_src[pair_st[i]]];
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / LANES, gl = lane % LANES;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long q = q0 + warp; q < q1; q += nwarps) {
+    const int i = panel_pair(pair_poff, np, q);
     const int64_t o = lo + pair_oc[i];
     const double xh0 = obs[3 * o], xh1 = obs[3 * o + 1];
     const double zeta = -obs[3 * o + 2] > 0.0 ? -obs[3 * o + 2] : 0.0;
-    (void)sp;
     double sh[NJG];
 #pragma unroll
     for (int t = 0; t < NJG; ++t) {
       const int jj = grp * NJG + t;
       sh[t] = jj < NJ ? foot[(size_t)i * NJ + jj] : 0.0;
     }
-    double run[NC][NJG];
+    double pt[NC][NJG];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int t = 0; t < NJG; ++t) pt[c][t] = 0.0;
+    const long long ua = pan_noff[q] - n0, ub = pan_noff[q + 1] - n0;
+#pragma unroll 2
+    for (long long u = ua + gl; u < ub; u += LANES) {
+      const double px = npx[u], py = npy[u], w = nw[u];
+      double Bv[NC];
+      if constexpr (KC == KD_HE) point_stress6_rcp(xh0 - px, xh1 - py, zeta, m.nu_f, Bv);
+      else point_disp3_rcp(xh0 - px, xh1 - py, zeta, m.mu, m.nu_f, Bv);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) Bv[c] *= w;
+#pragma unroll
+      for (int t = 0; t < NJG; ++t) {
+        const int jj = grp * NJG + t;
+        if (jj < NJ) {
+          const double sv = load[(size_t)jj * cap + u] - sh[t];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) pt[c][t] += Bv[c] * sv;
+        }
+      }
+    }
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
       for (int t = 0; t < NJG; ++t) {
+        double v = pt[c][t];
+#pragma unroll
+        for (int d = LANES / 2; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
         const int jj = grp * NJG + t;
-        run[c][t] = jj < NJ ? acc[(size_t)i * A::NOUT + c * NJ + jj] : 0.0;
+        if (gl == 0 && jj < NJ) part[(size_t)q * NOUT + c * NJ + jj] = v;
       }
-    const long long qa = pair_poff[i] > q0 ? pair_poff[i] : q0;
-    const long long qb = pair_poff[i + 1] < q1 ? pair_poff[i + 1] : q1;
-    for (long long q = qa; q < qb; ++q) {
-      double part[NC][NJG];
-#pragma unroll
-      for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int t = 0; t < NJG; ++t) part[c][t] = 0.0;
-      const long long ua = pan_noff[q] - n0, ub = pan_noff[q + 1] - n0;
-      for (long long u = ua + gl; u < ub; u += LANES) {
-        const double px = npx[u], py = npy[u], w = nw[u];
-        double Bv[NC];
-        if constexpr (KC == KD_HE) point_stress6(xh0 - px, xh1 - py, zeta, m.nu_f, Bv);
-        else point_disp3(xh0 - px, xh1 - py, zeta, m.mu, m.nu_f, Bv);
-#pragma unroll
-        for (int t = 0; t < NJG; ++t) {
-          const int jj = grp * NJG + t;
-          if (jj < NJ) {
-            const double sv = load[(size_t)jj * cap + u] - sh[t];
-#pragma unroll
-            for (int c = 0; c < NC; ++c) part[c][t] += (w * Bv[c]) * sv;
-          }
-        }
-      }
-      // tree reduction across the LANES lanes of each group
-#pragma unroll
-      for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int t = 0; t < NJG; ++t) {
-          double v = part[c][t];
-#pragma unroll
-          for (int d = LANES / 2; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
-          run[c][t] += v;
-        }
-    }
-    if (gl == 0) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int t = 0; t < NJG; ++t) {
-          const int jj = grp * NJG + t;
-          if (jj < NJ) acc[(size_t)i * A::NOUT + c * NJ + jj] = run[c][t];
-        }
-    }
   }
+}
+
+// Per pair and output component: the pair's panel sums in grid order.
+template <int P, int KC>
+__global__ void __launch_bounds__(128)
+k_pair_sum(int np, const long long* __restrict__ pair_poff, const double* __restrict__ part,
+           double* __restrict__ acc) {
+  constexpr int NOUT = AccumShape<P, KC>::NOUT;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)np * NOUT) return;
+  const int i = (int)(t / NOUT), k = (int)(t % NOUT);
+  double a = 0.0;
+  for (long long q = pair_poff[i]; q < pair_poff[i + 1]; ++q) a += part[(size_t)q * NOUT + k];
+  acc[(size_t)i * NOUT + k] = a;
 }
 
 // Per pair: the disk term of the grid's outer radius and the add into the
@@ -772,7 +892,7 @@ struct Sizes {
   // pair_st, pair_oc (int), pair_poff, pair_noff (scan input and output,
   // one more entry), foot (NJ), acc (NOUT)
   static constexpr size_t per_pair = 4 + 4 + 8 + 8 + 8 * NJ + 8 * NOUT;
-  static constexpr size_t per_panel = 8 + 8 + 8;          // ra, rb, first node
+  static constexpr size_t per_panel = 8 + 8 + 8 + 8 * NOUT;   // ra, rb, first node, sums
   static constexpr size_t per_node = 8 * 3 + 4 + 1 + 4 + 8 * NJ;
 };
 
@@ -783,7 +903,7 @@ inline size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 template <int P, int KC, class RF>
 int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_bytes,
              int64_t lo, int64_t nc, const SrcPrep* prep, const int* cnt, const int* list,
-             double* T, int* status, unsigned long long* census) {
+             double* T, int* status, unsigned long long* census, const Tune& tune) {
   using Z = Sizes<P, KC, RF>;
   constexpr int NJ = Z::NJ;
   constexpr int NOUT = Z::NOUT;
@@ -805,7 +925,11 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
   if (off >= region_bytes)
     return fail(MHS_ERR_WORKSPACE, "fold region of %zu bytes below its fixed part", region_bytes);
   MHS_CUDA_TRY(cudaMemsetAsync(hdr, 0, sizeof(Hdr), st));
-  k_band_scan<<<1, 1024, 0, st>>>(n_src, prep, cnt, st_rank, st_src, st_off, hdr);
+  {
+    StageTimer t(MHS_STAGE_FOLD_PLAN, st);
+    k_band_scan<<<1, 1024, 0, st>>>(n_src, prep, cnt, st_rank, st_src, st_off, hdr);
+    count_kernels(1);
+  }
   Hdr h;
   MHS_CUDA_TRY(cudaMemcpyAsync(&h, hdr, sizeof(Hdr), cudaMemcpyDeviceToHost, st));
   MHS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -834,6 +958,7 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
   double* pan_ra = (double*)carve(8 * cap_pan);
   double* pan_rb = (double*)carve(8 * cap_pan);
   long long* pan_noff = (long long*)carve(8 * (cap_pan + 1));
+  double* pan_sum = (double*)carve(8 * NOUT * cap_pan);
   double* npx = (double*)carve(8 * cap_node);
   double* npy = (double*)carve(8 * cap_node);
   double* nw = (double*)carve(8 * cap_node);
@@ -848,10 +973,13 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
   MHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_far, k_far<P, KC, RF>, 128, 0));
   MHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_near, k_near<P, KC>, 128, 0));
   MHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_nodes, k_nodes<P>, 256, 0));
-  const int g_far = sms * (occ_far > 0 ? occ_far : 1) * 4;
-  const int g_near = sms * (occ_near > 0 ? occ_near : 1) * 4;
+  const int g_far = sms * (occ_far > 0 ? occ_far : 1) * tune.far_mult;
+  const int g_near = sms * (occ_near > 0 ? occ_near : 1) * tune.near_mult;
   const int g_nodes = sms * (occ_nodes > 0 ? occ_nodes : 1) * 2;
   const int g_scatter = sms * 8;
+  // closed-form near field out to D_STAR element lengths in both forms (a
+  // near node's FP64 closed form costs less than the float 12 x 12 rule)
+  const double near_l = cst::D_STAR;
   long long p0 = 0;
   long long batch = cap_pair;
   while (p0 < h.n_pairs) {
@@ -865,10 +993,14 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
     const int np = (int)(p1 - p0);
     const long long j1 = strad(p1 - 1) + 1;
     MHS_CUDA_TRY(cudaMemsetAsync(&hdr->max_panel, 0, sizeof(long long), st));
-    k_pairs<<<(np + 127) / 128, 128, 0, st>>>(p0, np, lo, nc, r->obs, prep, list, st_src, st_off,
-                                              hdr, pair_st, pair_oc, pair_poff, pair_noff, status);
-    k_scan<<<1, 1024, 0, st>>>(pair_poff, np, &hdr->q_batch, nullptr);
-    k_scan<<<1, 1024, 0, st>>>(pair_noff, np, &hdr->n_batch, nullptr);
+    {
+      StageTimer t(MHS_STAGE_FOLD_PLAN, st);
+      k_pairs<<<(np + 127) / 128, 128, 0, st>>>(p0, np, lo, nc, r->obs, prep, list, st_src, st_off,
+                                                hdr, pair_st, pair_oc, pair_poff, pair_noff, status);
+      k_scan<<<1, 1024, 0, st>>>(pair_poff, np, &hdr->q_batch, nullptr);
+      k_scan<<<1, 1024, 0, st>>>(pair_noff, np, &hdr->n_batch, nullptr);
+      count_kernels(3);
+    }
     MHS_CUDA_TRY(cudaMemcpyAsync(&h, hdr, sizeof(Hdr), cudaMemcpyDeviceToHost, st));
     MHS_CUDA_TRY(cudaStreamSynchronize(st));
     if (h.q_batch > cap_pan) {
@@ -882,34 +1014,67 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
       return fail(MHS_ERR_WORKSPACE, "a fold panel of %lld nodes does not fit the fold "
                   "region's %lld-node waves", h.max_panel, cap_node);
     const long long nq = h.q_batch, nn = h.n_batch;
-    k_src<P, KC, RF><<<(unsigned)(j1 - j0), 128, 0, st>>>((int)j0, (int)(j1 - j0), st_src, prep,
-                                                          r->mu, r->lam, srcs);
-    k_panels<<<(np + 1 + 127) / 128, 128, 0, st>>>(np, lo, r->obs, prep, st_src, pair_st, pair_oc,
-                                                   pair_poff, pair_noff, pan_ra, pan_rb, pan_noff);
-    k_foot<P, KC, RF><<<(np + 127) / 128, 128, 0, st>>>(np, (int)j0, lo, r->obs, prep, st_src,
-                                                        pair_st, pair_oc, srcs, foot);
-    k_zero<<<sms * 4, 256, 0, st>>>(acc, (long long)np * NOUT);
-    if (census) k_census_pairs<<<1, 1, 0, st>>>(hdr, census, np);
+    {
+      StageTimer t(MHS_STAGE_FOLD_PLAN, st);
+      k_src<P, KC, RF><<<(unsigned)(j1 - j0), 128, 0, st>>>((int)j0, (int)(j1 - j0), st_src, prep,
+                                                            r->mu, r->lam, srcs);
+      k_panels<<<(np + 1 + 127) / 128, 128, 0, st>>>(np, lo, r->obs, prep, st_src, pair_st,
+                                                     pair_oc, pair_poff, pair_noff, pan_ra, pan_rb,
+                                                     pan_noff);
+      k_foot<P, KC, RF><<<(np + 127) / 128, 128, 0, st>>>(np, (int)j0, lo, r->obs, prep, st_src,
+                                                          pair_st, pair_oc, srcs, foot);
+      count_kernels(3);
+      if (census) {
+        k_census_pairs<<<1, 1, 0, st>>>(hdr, census, np);
+        count_kernels(1);
+      }
+    }
     const long long span = cap_node - h.max_panel;
     const long long waves = (nn + span - 1) / span;
     for (long long w = 0; w < waves; ++w) {
-      k_wave_begin<<<1, 1, 0, st>>>(w, span, nq, pan_noff, hdr);
-      k_nodes<P><<<g_nodes, 256, 0, st>>>(np, lo, r->obs, prep, st_src, pair_st, pair_oc,
-                                          pair_poff, pan_ra, pan_rb, pan_noff, hdr, npx, npy, nw,
-                                          npair, ncls);
-      k_wave_classes<<<1, 1, 0, st>>>(hdr, census);
-      k_scatter<<<g_scatter, 256, 0, st>>>(hdr, ncls, nlist);
-      k_far<P, KC, RF><<<g_far, 128, 0, st>>>(hdr, nlist, npx, npy, npair, pair_st, (int)j0,
-                                              st_src, prep, srcs, load, cap_node);
-      k_near<P, KC><<<g_near, 128, 0, st>>>(hdr, nlist, npx, npy, npair, pair_st, (int)j0, st_src,
-                                            prep, slcs, (long long)sizeof(Src<P, RF>), load,
-                                            cap_node);
-      k_accum<P, KC><<<(np + 3) / 4 < sms * 16 ? (np + 3) / 4 : sms * 16, 128, 0, st>>>(
-          np, lo, r->obs, prep, st_src, pair_st, pair_oc, pair_poff, pan_noff, hdr, npx, npy, nw,
-          load, cap_node, foot, r->mu, r->lam, acc);
+      {
+        StageTimer t(MHS_STAGE_FOLD_NODES, st);
+        k_wave_begin<<<1, 1, 0, st>>>(w, span, nq, pan_noff, hdr);
+        k_nodes<P><<<g_nodes, 256, 0, st>>>(near_l, np, lo, r->obs, prep, st_src, pair_st,
+                                            pair_oc, pair_poff, pan_ra, pan_rb, pan_noff, hdr, npx,
+                                            npy, nw, npair, ncls);
+        k_count<<<g_scatter, 256, 0, st>>>(hdr, ncls);
+        k_wave_classes<<<1, 1, 0, st>>>(hdr, census);
+        k_scatter<<<g_scatter, 256, 0, st>>>(hdr, ncls, nlist);
+        count_kernels(5);
+      }
+      {
+        StageTimer t(MHS_STAGE_FOLD_FAR, st);
+        k_far<P, KC, RF><<<g_far, 128, 0, st>>>(hdr, nlist, npx, npy, npair, pair_st, (int)j0,
+                                                st_src, prep, srcs, load, cap_node);
+        count_kernels(1);
+      }
+      {
+        StageTimer t(MHS_STAGE_FOLD_NEAR, st);
+        k_near<P, KC><<<g_near, 128, 0, st>>>(hdr, nlist, npx, npy, npair, pair_st, (int)j0,
+                                              st_src, prep, slcs, (long long)sizeof(Src<P, RF>),
+                                              load, cap_node);
+        count_kernels(1);
+      }
+      {
+        StageTimer t(MHS_STAGE_FOLD_ACCUM, st);
+        k_accum<P, KC><<<sms * 16, 32 * ACCUM_WARPS, 0, st>>>(np, lo, r->obs, pair_oc, pair_poff,
+                                                             pan_noff, hdr, npx, npy, nw, load,
+                                                             cap_node, foot, r->mu, r->lam,
+                                                             pan_sum);
+        count_kernels(1);
+      }
     }
-    k_finish<P, KC><<<(np + 127) / 128, 128, 0, st>>>(np, lo, n_src, r->obs, prep, st_src,
-                                                      pair_st, pair_oc, foot, acc, r->mu, r->lam, T);
+    {
+      StageTimer t(MHS_STAGE_FOLD_ACCUM, st);
+      const long long nt = (long long)np * NOUT;
+      k_pair_sum<P, KC><<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(np, pair_poff, pan_sum, acc);
+      count_kernels(1);
+      k_finish<P, KC><<<(np + 127) / 128, 128, 0, st>>>(np, lo, n_src, r->obs, prep, st_src,
+                                                        pair_st, pair_oc, foot, acc, r->mu, r->lam,
+                                                        T);
+      count_kernels(1);
+    }
     MHS_CUDA_TRY(cudaGetLastError());
     p0 = p1;
     batch = cap_pair;

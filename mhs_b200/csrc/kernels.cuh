@@ -78,6 +78,22 @@ __device__ void float_rules(const SmemRules<P>& rd, FloatRules<P>& fr, int tid, 
   }
   for (int t = tid; t < N * K; t += nthr) fr.Nq[t] = (float)rd.Nq[t];
 }
+// Float rules built directly (nodes formed in double, then rounded).
+template <int P>
+__device__ void build_float_rules(const Frame& f, FloatRules<P>& fr, int tid, int nthr) {
+  constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N, K = n_nodes(P);
+  for (int t = tid; t < FloatRules<P>::N; t += nthr) {
+    const int n = t < N12 ? cst::FAR_GAUSS_N : cst::FAR_GAUSS_N_DISTANT;
+    const int q = t < N12 ? t : t - N12;
+    double e0, e1, wq, Nq[K];
+    rule_node<P>(f, n, q, e0, e1, wq, Nq);
+    fr.e0[t] = (float)e0;
+    fr.e1[t] = (float)e1;
+    fr.wq[t] = (float)wq;
+    for (int k = 0; k < K; ++k) fr.Nq[t * K + k] = (float)Nq[k];
+  }
+}
+
 template <int P>
 __device__ QuadRuleT<float> float_r12(const FloatRules<P>& fr) {
   return QuadRuleT<float>{cst::FAR_GAUSS_N * cst::FAR_GAUSS_N, fr.e0, fr.e1, fr.wq, fr.Nq};
@@ -90,11 +106,11 @@ __device__ QuadRuleT<float> float_r8(const FloatRules<P>& fr) {
 }
 
 // ---------------------------------------------------------------- k_coef
-__global__ void k_coef(double mu, double lam, double* out) {
+// Record coefficients t of one material (t < MHS_Q_NDDG covers every table).
+__device__ __forceinline__ void coef_entry(double mu, double lam, double* out, int t) {
   const Material m = make_material(mu, lam);
   const double nu = m.nu_i, s = m.scale_c;
   const double nup[3] = {1.0, nu, nu * nu};
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double* r_dg = out;
   double* r_ddg = r_dg + 3 * MHS_R_NDG;
   double* q_dg = r_ddg + 3 * MHS_R_NDDG;
@@ -123,12 +139,32 @@ __global__ void k_coef(double mu, double lam, double* out) {
   }
 }
 
+// Per-pass image coefficients (and the pass's status word cleared).
+__global__ void k_coef(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq) {
+  const int r = find_req(off, nreq, blockIdx.x);
+  const ReqDesc& d = D[r];
+  const long long b = blockIdx.x - off[r];
+  if (b == 0 && threadIdx.x == 0) *d.status = 0;
+  coef_entry(d.fa.mu, d.fa.lam, d.coef, (int)(b * blockDim.x + threadIdx.x));
+}
+
+// The same for one material (diagnostics).
+__global__ void k_coef1(double mu, double lam, double* out) {
+  coef_entry(mu, lam, out, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ---------------------------------------------------------------- k_prep
-__global__ void k_prep(int64_t n_src, const double* __restrict__ tris,
-                       const double* __restrict__ eps, int fold, int want_g,
-                       SrcPrep* __restrict__ prep, double* __restrict__ G) {
-  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (s >= n_src) return;
+__global__ void k_prep(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq,
+                       int want_g) {
+  const int r = find_req(off, nreq, blockIdx.x);
+  const ReqDesc& d = D[r];
+  const int64_t s = (blockIdx.x - off[r]) * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= d.fa.n_src) return;
+  const double* __restrict__ tris = d.tris;
+  const double* __restrict__ eps = d.eps;
+  const int fold = d.fold;
+  SrcPrep* __restrict__ prep = d.prep;
+  double* __restrict__ G = d.G;
   SrcPrep p;
   const double* t = tris + 9 * s;
   double ti[9];
@@ -150,32 +186,45 @@ __global__ void k_prep(int64_t n_src, const double* __restrict__ tris,
 // mixed form).
 template <int P, int KC, class RF>
 __global__ void __launch_bounds__(TB)
-k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
-       const SrcPrep* __restrict__ prep, const double* __restrict__ Gall,
-       const double* __restrict__ coef, double mu, double lam, double* __restrict__ T) {
+k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq,
+       double near_l_mixed) {
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);
   constexpr bool IMG = KC != KD_E;
-  const int64_t s = blockIdx.x;
-  __shared__ SrcPrep sp;
-  __shared__ SmemRules<P> rd;
-  __shared__ SmemRules<IMG ? P : 0> ri;
-  __shared__ double sG[IMG ? G_SIZE : 1];
+  const int r = find_req(off, nreq, blockIdx.x);
+  const ReqDesc& d = D[r];
+  const int64_t lo = d.fa.lo, n_chunk = d.fa.n_chunk, n_src = d.fa.n_src;
+  const long long local = blockIdx.x - off[r];
+  const int64_t s = local % n_src, tile = local / n_src;
+  const double* __restrict__ obs = d.obs;
+  const SrcPrep* __restrict__ prep = d.prep;
+  const double* __restrict__ Gall = d.G;
+  const double* __restrict__ coef = d.coef;
+  const double mu = d.fa.mu, lam = d.fa.lam;
+  double* __restrict__ T = d.T;
   constexpr bool F32 = std::is_same<RF, float>::value;
+  // far rules of the element and of its reflection: double, or float only
+  // in the mixed form (whose far field runs in float)
+  __shared__ SrcPrep sp;
+  __shared__ std::conditional_t<F32, NoRules, SmemRules<P>> rd;
+  __shared__ std::conditional_t<F32 || !IMG, NoRules, SmemRules<IMG ? P : 0>> ri;
+  __shared__ double sG[IMG ? G_SIZE : 1];
   __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rdf;
+  __shared__ std::conditional_t<F32 && IMG, FloatRules<IMG ? P : 0>, NoRules> rif;
   if (threadIdx.x == 0) sp = prep[s];
   __syncthreads();
-  rd.build(sp.f, threadIdx.x, TB);
-  if (IMG) {
-    ri.build(sp.fi, threadIdx.x, TB);
-    for (int i = threadIdx.x; i < G_SIZE; i += TB) sG[i] = Gall[s * G_SIZE + i];
-  }
-  __syncthreads();
   if constexpr (F32) {
-    float_rules<P>(rd, rdf, threadIdx.x, TB);
-    __syncthreads();
+    build_float_rules<P>(sp.f, rdf, threadIdx.x, blockDim.x);
+    if constexpr (IMG) build_float_rules<P>(sp.fi, rif, threadIdx.x, blockDim.x);
+  } else {
+    rd.build(sp.f, threadIdx.x, blockDim.x);
+    if constexpr (IMG) ri.build(sp.fi, threadIdx.x, blockDim.x);
   }
-  const int64_t oc = blockIdx.y * (int64_t)TB + threadIdx.x;
+  if (IMG)
+    for (int i = threadIdx.x; i < G_SIZE; i += blockDim.x) sG[i] = Gall[s * G_SIZE + i];
+  __syncthreads();
+  const double near_l = F32 ? near_l_mixed : cst::D_STAR;
+  const int64_t oc = tile * (int64_t)blockDim.x + threadIdx.x;
   if (oc >= n_chunk) return;
   const int64_t o = lo + oc;
   const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
@@ -184,7 +233,7 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
   double* row = T + ((oc * n_src + s) * K) * NR;
   if constexpr (KC == KD_E) {
     double E[K] = {};
-    if constexpr (F32) direct_eval<P, W_E, RF>(sp.f, float_r12<P>(rdf), float_r8<P>(rdf), x, eps, m, nullptr, nullptr, E);
+    if constexpr (F32) direct_eval<P, W_E, RF>(sp.f, float_r12<P>(rdf), float_r8<P>(rdf), x, eps, m, nullptr, nullptr, E, near_l);
     else direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
     for (int k = 0; k < K; ++k) {
       row[k * NR + 0] = E[k];
@@ -197,9 +246,9 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     if constexpr (F32) {
       const QuadRuleT<float> f12 = float_r12<P>(rdf), f8 = float_r8<P>(rdf);
       if constexpr (KC == KD_DISP)
-        direct_eval<P, W_U, RF>(sp.f, f12, f8, x, eps, m, A, nullptr, nullptr);
+        direct_eval<P, W_U, RF>(sp.f, f12, f8, x, eps, m, A, nullptr, nullptr, near_l);
       else
-        direct_eval<P, W_H | W_E, RF>(sp.f, f12, f8, x, eps, m, nullptr, A, E);
+        direct_eval<P, W_H | W_E, RF>(sp.f, f12, f8, x, eps, m, nullptr, A, E, near_l);
     } else {
       if constexpr (KC == KD_DISP)
         direct_eval<P, W_U, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
@@ -210,10 +259,18 @@ k_pair(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ ob
     if (!band) {
       double B[K * C] = {};
       const ImageCoef ic = image_coef_view(coef);
-      if constexpr (KC == KD_DISP)
-        image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
-      else
-        image_r_eval<P, W_H>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, nullptr, B);
+      if constexpr (F32) {
+        const QuadRuleT<float> i12 = float_r12<P>(rif), i8 = float_r8<P>(rif);
+        if constexpr (KC == KD_DISP)
+          image_r_eval<P, W_U, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, B, nullptr, near_l);
+        else
+          image_r_eval<P, W_H, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, nullptr, B, near_l);
+      } else {
+        if constexpr (KC == KD_DISP)
+          image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
+        else
+          image_r_eval<P, W_H>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, nullptr, B);
+      }
       for (int i = 0; i < K * C; ++i) A[i] += B[i];
     }
     for (int k = 0; k < K; ++k) {
@@ -266,13 +323,20 @@ struct QRuleFly {
 // element from the image triangle -- sum their points in float.
 template <int P, int KC, class RF>
 __global__ void __launch_bounds__(TB)
-k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ obs,
-         const SrcPrep* __restrict__ prep, const double* __restrict__ coef, double mu, double lam,
-         double* __restrict__ T) {
+k_imageq(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq) {
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);
   constexpr int C = comps_of(KC);
-  const int64_t s = blockIdx.x;
+  const int r = find_req(off, nreq, blockIdx.x);
+  const ReqDesc& d = D[r];
+  const int64_t lo = d.fa.lo, n_chunk = d.fa.n_chunk, n_src = d.fa.n_src;
+  const long long local = blockIdx.x - off[r];
+  const int64_t s = local % n_src, tile = local / n_src;
+  const double* __restrict__ obs = d.obs;
+  const SrcPrep* __restrict__ prep = d.prep;
+  const double* __restrict__ coef = d.coef;
+  const double mu = d.fa.mu, lam = d.fa.lam;
+  double* __restrict__ T = d.T;
   __shared__ SrcPrep sp;
   __shared__ double qy[QFLOOR * QFLOOR * 3];
   __shared__ double qw[QFLOOR * QFLOOR * K];
@@ -283,15 +347,15 @@ k_imageq(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restrict__ 
   __syncthreads();
   {
     QRuleFly<P> fly{&sp.f, QFLOOR};
-    for (int t = threadIdx.x; t < QFLOOR * QFLOOR; t += TB) fly.node(t, qy + 3 * t, qw + K * t);
+    for (int t = threadIdx.x; t < QFLOOR * QFLOOR; t += blockDim.x) fly.node(t, qy + 3 * t, qw + K * t);
   }
   __syncthreads();
   if constexpr (F32) {
-    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * 3; t += TB) qyf[t] = (float)qy[t];
-    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * K; t += TB) qwf[t] = (float)qw[t];
+    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * 3; t += blockDim.x) qyf[t] = (float)qy[t];
+    for (int t = threadIdx.x; t < QFLOOR * QFLOOR * K; t += blockDim.x) qwf[t] = (float)qw[t];
     __syncthreads();
   }
-  const int64_t oc = blockIdx.y * (int64_t)TB + threadIdx.x;
+  const int64_t oc = tile * (int64_t)blockDim.x + threadIdx.x;
   if (oc >= n_chunk) return;
   const int64_t o = lo + oc;
   const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
@@ -418,17 +482,6 @@ k_fold_mirror(int64_t lo, int64_t n_chunk, int64_t n_src, const double* __restri
 #include "fold_waves.cuh"
 
 // --------------------------------------------------------------- k_final
-struct FinalArgs {
-  int kind, subtract, out_f32, n_a, n_b;
-  int64_t lo, n_chunk, n_src, n_obs, n_dof;
-  const double* normals;
-  const double* rec_basis;
-  const double* src_basis;
-  const int32_t* col_ptr;
-  const int32_t* col_ent;
-  double mu, lam;
-  void* out;
-};
 
 // Eigenstress C:sym(slip (x) n) of one row: phi C(n) + phi_m C(n_m) sign.
 __device__ __forceinline__ double eig_comp(const SrcPrep& p, double phi, double phim, double mu,
@@ -512,24 +565,21 @@ __device__ void row_values(const FinalArgs& a, const SrcPrep& p, const double* r
   }
 }
 
-template <int P, int KC, class OUT, bool CONT>
-__global__ void __launch_bounds__(TB)
-k_final(FinalArgs a, const SrcPrep* __restrict__ prep, const double* __restrict__ T) {
+__device__ __forceinline__ void store_any(void* out, int64_t i, double v, int f32) {
+  if (f32) reinterpret_cast<float*>(out)[i] = (float)v;
+  else reinterpret_cast<double*>(out)[i] = v;
+}
+
+// Values of output column `col` of observer row `o` of one pass: the
+// element's scratch row (discontinuous) or the ordered gather of its shared
+// column (continuous).
+template <int P, int KC>
+__device__ __forceinline__ void column_values(const FinalArgs& a, const SrcPrep* __restrict__ prep,
+                                              const double* __restrict__ T, int64_t oc, int64_t o,
+                                              int64_t col, double* v, int nv) {
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);
-  const int64_t col = blockIdx.x * (int64_t)TB + threadIdx.x;
-  const int64_t oc = blockIdx.y;
-  if (col >= a.n_dof) return;
-  const int64_t o = a.lo + oc;
-  int nv;
-  switch (a.kind) {
-    case MHS_DISP:
-    case MHS_TRACTION: nv = 9; break;
-    case MHS_INTERACTION: nv = a.n_a * a.n_b; break;
-    default: nv = 27;
-  }
-  double v[27];
-  if (!CONT) {
+  if (!a.col_ptr) {
     const int64_t s = col / K;
     const double* row = T + (oc * a.n_src * K + col) * NR;
     row_values<KC>(a, prep[s], row, o, s, v, nv);
@@ -544,100 +594,255 @@ k_final(FinalArgs a, const SrcPrep* __restrict__ prep, const double* __restrict_
       for (int i = 0; i < nv; ++i) v[i] += w[i];
     }
   }
+}
+
+// Output stage of every pass: the store of each (observer, column) value in
+// the caller's layout, or -- in apply mode -- the matrix times the slip
+// vector, y[o][c] = sum over columns and slip components of M[o][c][col][s]
+// slip[col][s], without storing M (one block per observer row; each thread
+// takes a stride of columns and the block's sums are reduced in a fixed
+// tree order).  blockDim is a power of two.
+template <int P, int KC>
+__global__ void __launch_bounds__(TB)
+k_out(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq) {
+  const int r = find_req(off, nreq, blockIdx.x);
+  const ReqDesc& d = D[r];
+  const FinalArgs& a = d.fa;
+  const SrcPrep* __restrict__ prep = d.prep;
+  const double* __restrict__ T = d.T;
+  const long long local = blockIdx.x - off[r];
+  int nv, ns;
+  switch (a.kind) {
+    case MHS_DISP:
+    case MHS_TRACTION: nv = 9; ns = 3; break;
+    case MHS_INTERACTION: nv = a.n_a * a.n_b; ns = a.n_b; break;
+    default: nv = 27; ns = 3;
+  }
+  if (a.slip) {
+    const int64_t oc = local;
+    const int64_t o = a.lo + oc;
+    const int nc = nv / ns;
+    double y[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) y[c] = 0.0;
+    for (int64_t col = threadIdx.x; col < a.n_dof; col += blockDim.x) {
+      double v[27];
+      column_values<P, KC>(a, prep, T, oc, o, col, v, nv);
+      const double* sl = a.slip + col * ns;
+      for (int c = 0; c < nc; ++c) {
+        double acc = 0.0;
+        for (int m = 0; m < ns; ++m) acc += v[c * ns + m] * sl[m];
+        y[c] += acc;
+      }
+    }
+    __shared__ double red[TB][9];
+    for (int c = 0; c < 9; ++c) red[threadIdx.x][c] = y[c];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h >= 1; h >>= 1) {
+      if (threadIdx.x < h)
+        for (int c = 0; c < 9; ++c) red[threadIdx.x][c] += red[threadIdx.x + h][c];
+      __syncthreads();
+    }
+    if (threadIdx.x < nc) store_any(a.out, o * nc + threadIdx.x, red[0][threadIdx.x], a.out_f32);
+    return;
+  }
+  const long long ctiles = (a.n_dof + blockDim.x - 1) / blockDim.x;
+  const int64_t col = (local % ctiles) * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t oc = local / ctiles;
+  if (col >= a.n_dof) return;
+  const int64_t o = a.lo + oc;
+  double v[27];
+  column_values<P, KC>(a, prep, T, oc, o, col, v, nv);
   // store in the caller's layout
   switch (a.kind) {
     case MHS_DISP:
     case MHS_TRACTION:  // (N, 3, n_dof, 3)
       for (int i = 0; i < 3; ++i)
         for (int m = 0; m < 3; ++m)
-          store<OUT>(a.out, ((o * 3 + i) * a.n_dof + col) * 3 + m, v[3 * i + m]);
+          store_any(a.out, ((o * 3 + i) * a.n_dof + col) * 3 + m, v[3 * i + m], a.out_f32);
       break;
     case MHS_INTERACTION:  // (N, n_dof, n_a, n_b)
-      for (int i = 0; i < nv; ++i) store<OUT>(a.out, (o * a.n_dof + col) * nv + i, v[i]);
+      for (int i = 0; i < nv; ++i) store_any(a.out, (o * a.n_dof + col) * nv + i, v[i], a.out_f32);
       break;
     default:  // (N, 3, 3, n_dof, 3)
       for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j)
           for (int m = 0; m < 3; ++m)
-            store<OUT>(a.out, (((o * 3 + i) * 3 + j) * a.n_dof + col) * 3 + m, v[9 * i + 3 * j + m]);
+            store_any(a.out, (((o * 3 + i) * 3 + j) * a.n_dof + col) * 3 + m, v[9 * i + 3 * j + m],
+                      a.out_f32);
   }
 }
 
+// One pass of one request: its observer chunk [lo, lo + nc) on its own
+// workspace; `first` marks the request's first pass (coefficients and
+// per-source data are formed once).
+struct Pass {
+  const mhs_request* r;
+  const Layout* L;
+  int64_t lo, nc;
+  bool first;
+};
 
-template <int P, int KC, class RF>
-int run(const mhs_request* r, cudaStream_t st, const Layout& L, unsigned long long* census) {
-  char* ws = (char*)r->workspace;
-  int* status = (int*)(ws + L.status);
-  double* coef = (double*)(ws + L.coef);
-  SrcPrep* prep = (SrcPrep*)(ws + L.prep);
-  double* G = (double*)(ws + L.G);
-  int* cnt = (int*)(ws + L.cnt);
-  int* list = (int*)(ws + L.list);
-  double* T = (double*)(ws + L.T);
+template <int P, int KC>
+void fill_desc(const Pass& p, ReqDesc& d) {
   constexpr int K = n_nodes(P);
-  MHS_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
-  {
-    StageTimer t(MHS_STAGE_PREP, st);
-    k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(r->mu, r->lam, coef);
-    k_prep<<<(unsigned)((r->n_src + 127) / 128), 128, 0, st>>>(r->n_src, r->tris, r->eps, r->fold,
-                                                                KC != KD_E, prep, G);
-  }
+  const mhs_request* r = p.r;
+  char* ws = (char*)r->workspace;
   const bool cont = r->ids != nullptr;
-  const int64_t n_dof = cont ? r->n_cols : r->n_src * K;
-  for (int64_t lo = 0; lo < r->n_obs; lo += L.chunk) {
-    const int64_t nc = std::min<int64_t>(L.chunk, r->n_obs - lo);
-    dim3 g((unsigned)r->n_src, (unsigned)((nc + TB - 1) / TB));
-    {
-      StageTimer t(MHS_STAGE_PAIR, st);
-      k_pair<P, KC, RF><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, G, coef, r->mu, r->lam, T);
-    }
+  FinalArgs& a = d.fa;
+  a.kind = r->kind;
+  a.subtract = r->subtract_eigenstress;
+  a.out_f32 = r->out_f32;
+  a.n_a = r->n_a;
+  a.n_b = r->n_b;
+  a.lo = p.lo;
+  a.n_chunk = p.nc;
+  a.n_src = r->n_src;
+  a.n_obs = r->n_obs;
+  a.n_dof = cont ? r->n_cols : r->n_src * K;
+  a.normals = r->normals;
+  a.rec_basis = r->rec_basis;
+  a.src_basis = r->src_basis;
+  a.col_ptr = cont ? r->col_ptr : nullptr;
+  a.col_ent = cont ? r->col_ent : nullptr;
+  a.mu = r->mu;
+  a.lam = r->lam;
+  a.out = r->out;
+  a.slip = r->slip;
+  d.obs = r->obs;
+  d.tris = r->tris;
+  d.eps = r->eps;
+  d.prep = (SrcPrep*)(ws + p.L->prep);
+  d.G = (double*)(ws + p.L->G);
+  d.coef = (double*)(ws + p.L->coef);
+  d.T = (double*)(ws + p.L->T);
+  d.status = (int*)(ws + p.L->status);
+  d.fold = r->fold;
+  d.pad = 0;
+}
+
+// Descriptors and stage block prefixes of n passes (host image of the
+// device block at desc_bytes(n)).
+template <int P, int KC>
+void build_descs(const Pass* ps, int n, const Tune& tune, std::vector<char>& host) {
+  host.assign(desc_bytes(n), 0);
+  ReqDesc* hd = (ReqDesc*)host.data();
+  long long* off = (long long*)(host.data() + align_up(sizeof(ReqDesc) * (size_t)n));
+  for (int i = 0; i < n; ++i) fill_desc<P, KC>(ps[i], hd[i]);
+  for (int j = 0; j < N_OFF; ++j) off[j * (n + 1)] = 0;
+  for (int i = 0; i < n; ++i) {
+    const FinalArgs& a = hd[i].fa;
+    const long long b[N_OFF] = {
+        ps[i].first ? (MHS_Q_NDDG + 255) / 256 : 0,
+        ps[i].first ? (a.n_src + 127) / 128 : 0,
+        a.n_src * ((a.n_chunk + tune.pair_tb - 1) / tune.pair_tb),
+        a.slip ? a.n_chunk : ((a.n_dof + tune.final_tb - 1) / tune.final_tb) * a.n_chunk};
+    for (int j = 0; j < N_OFF; ++j) off[j * (n + 1) + i + 1] = off[j * (n + 1) + i] + b[j];
+  }
+}
+
+// The stages of n passes of this unit, each stage in one launch over all of
+// them; the fold runs per pass between the pair stages and the output.  The
+// descriptors live at desc (device); upload = 0 when they are there already.
+template <int P, int KC, class RF>
+int run_passes(const Pass* ps, int n, void* desc, bool upload, cudaStream_t st,
+               unsigned long long* census, const Tune& tune) {
+  std::vector<char> host;
+  build_descs<P, KC>(ps, n, tune, host);
+  const long long* hoff = (const long long*)(host.data() + align_up(sizeof(ReqDesc) * (size_t)n));
+  if (upload)
+    MHS_CUDA_TRY(cudaMemcpyAsync(desc, host.data(), host.size(), cudaMemcpyHostToDevice, st));
+  const ReqDesc* D = (const ReqDesc*)desc;
+  const long long* off = (const long long*)((const char*)desc + align_up(sizeof(ReqDesc) * (size_t)n));
+  auto total = [&](int j) { return hoff[j * (n + 1) + n]; };
+  auto offs = [&](int j) { return off + j * (n + 1); };
+  if (total(OFF_COEF) > 0) {
+    StageTimer t(MHS_STAGE_PREP, st);
+    k_coef<<<(unsigned)total(OFF_COEF), 256, 0, st>>>(D, offs(OFF_COEF), n);
+    k_prep<<<(unsigned)total(OFF_PREP), 128, 0, st>>>(D, offs(OFF_PREP), n, KC != KD_E);
+    count_kernels(2);
+  }
+  {
+    StageTimer t(MHS_STAGE_PAIR, st);
+    k_pair<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(D, offs(OFF_PAIR), n,
+                                                                          MIXED_NEAR_L);
+    count_kernels(1);
+  }
+  if constexpr (KC != KD_E) {
+    StageTimer t(MHS_STAGE_IMAGEQ, st);
+    k_imageq<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(D, offs(OFF_PAIR), n);
+    count_kernels(1);
+  }
+  for (int i = 0; i < n; ++i) {
+    const mhs_request* r = ps[i].r;
+    if (!r->fold) continue;
+    const Layout& L = *ps[i].L;
+    char* ws = (char*)r->workspace;
+    int* status = (int*)(ws + L.status);
+    SrcPrep* prep = (SrcPrep*)(ws + L.prep);
+    int* cnt = (int*)(ws + L.cnt);
+    int* list = (int*)(ws + L.list);
+    double* T = (double*)(ws + L.T);
+    const int64_t lo = ps[i].lo, nc = ps[i].nc;
+    StageTimer t(MHS_STAGE_FOLD, st);
+    k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
+    count_kernels(1);
     if constexpr (KC != KD_E) {
-      StageTimer t(MHS_STAGE_IMAGEQ, st);
-      k_imageq<P, KC, RF><<<g, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, coef, r->mu, r->lam, T);
+      const int rc = fold_waves::run_fold<P, KC, RF>(r, st, ws + L.fold, L.fold_bytes, lo, nc, prep,
+                                                     cnt, list, T, status, census, tune);
+      if (rc) return rc;
     }
-    if (r->fold) {
-      StageTimer t(MHS_STAGE_FOLD, st);
-      k_band<<<(unsigned)r->n_src, 256, 0, st>>>(lo, nc, r->obs, prep, cnt, list);
-      if constexpr (KC != KD_E) {
-        const int rc = fold_waves::run_fold<P, KC, RF>(r, st, ws + L.fold, L.fold_bytes, lo, nc,
-                                                       prep, cnt, list, T, status, census);
-        if (rc) return rc;
-      }
-      dim3 gm((unsigned)r->n_src, (unsigned)((nc + TB - 1) / TB));
-      k_fold_mirror<P, KC, RF><<<gm, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list, r->mu,
-                                              r->lam, T);
-    }
-    StageTimer tfin(MHS_STAGE_FINAL, st);
-    FinalArgs a;
-    a.kind = r->kind;
-    a.subtract = r->subtract_eigenstress;
-    a.out_f32 = r->out_f32;
-    a.n_a = r->n_a;
-    a.n_b = r->n_b;
-    a.lo = lo;
-    a.n_chunk = nc;
-    a.n_src = r->n_src;
-    a.n_obs = r->n_obs;
-    a.n_dof = n_dof;
-    a.normals = r->normals;
-    a.rec_basis = r->rec_basis;
-    a.src_basis = r->src_basis;
-    a.col_ptr = r->col_ptr;
-    a.col_ent = r->col_ent;
-    a.mu = r->mu;
-    a.lam = r->lam;
-    a.out = r->out;
-    dim3 gfin((unsigned)((n_dof + TB - 1) / TB), (unsigned)nc);
-    if (r->out_f32) {
-      if (cont) k_final<P, KC, float, true><<<gfin, TB, 0, st>>>(a, prep, T);
-      else k_final<P, KC, float, false><<<gfin, TB, 0, st>>>(a, prep, T);
-    } else {
-      if (cont) k_final<P, KC, double, true><<<gfin, TB, 0, st>>>(a, prep, T);
-      else k_final<P, KC, double, false><<<gfin, TB, 0, st>>>(a, prep, T);
-    }
+    dim3 gm((unsigned)r->n_src, (unsigned)((nc + TB - 1) / TB));
+    k_fold_mirror<P, KC, RF><<<gm, TB, 0, st>>>(lo, nc, r->n_src, r->obs, prep, cnt, list, r->mu,
+                                                r->lam, T);
+    count_kernels(1);
+  }
+  {
+    StageTimer t(MHS_STAGE_FINAL, st);
+    const bool apply = n > 0 && ps[0].r->slip;
+    k_out<P, KC><<<(unsigned)total(OFF_FINAL), apply ? TB : tune.final_tb, 0, st>>>(
+        D, offs(OFF_FINAL), n);
+    count_kernels(1);
   }
   MHS_CUDA_TRY(cudaGetLastError());
   return MHS_OK;
+}
+
+// One request on its workspace: its observer chunks one pass after another.
+template <int P, int KC, class RF>
+int run(const mhs_request* r, cudaStream_t st, const Layout& L, unsigned long long* census,
+        const Tune& tune) {
+  void* desc = (char*)r->workspace + L.desc;
+  for (int64_t lo = 0; lo < r->n_obs; lo += L.chunk) {
+    const Pass p{r, &L, lo, std::min<int64_t>(L.chunk, r->n_obs - lo), lo == 0};
+    const int rc = run_passes<P, KC, RF>(&p, 1, desc, true, st, census, tune);
+    if (rc) return rc;
+  }
+  return MHS_OK;
+}
+
+// A batch of requests of this unit, each in one pass.  Requests in apply
+// mode and the rest must not be mixed (the output stage's block size).
+// upload: 1 copies the descriptors to desc and launches, 0 launches with
+// the descriptors already there (a batch bound before stream capture), 2
+// only copies them.
+template <int P, int KC, class RF>
+int run_batch(const mhs_request* const* rs, const Layout* L, int n, void* desc, int upload,
+              cudaStream_t st, unsigned long long* census, const Tune& tune) {
+  std::vector<Pass> ps((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    if (L[i].chunk < rs[i]->n_obs) return fail(MHS_ERR_WORKSPACE, "batched request %d needs one pass", i);
+    if ((rs[i]->slip != nullptr) != (rs[0]->slip != nullptr))
+      return fail(MHS_ERR_ARG, "a batch mixes apply-mode and matrix requests");
+    ps[i] = Pass{rs[i], &L[i], 0, rs[i]->n_obs, true};
+  }
+  if (upload == 2) {
+    std::vector<char> host;
+    build_descs<P, KC>(ps.data(), n, tune, host);
+    MHS_CUDA_TRY(cudaMemcpyAsync(desc, host.data(), host.size(), cudaMemcpyHostToDevice, st));
+    return MHS_OK;
+  }
+  return run_passes<P, KC, RF>(ps.data(), n, desc, upload == 1, st, census, tune);
 }
 
 // ---------------------------------------------------- per-term diagnostics
@@ -710,7 +915,7 @@ __global__ void k_terms(int term, int n, const double* __restrict__ obs,
 template <int P>
 int debug_terms(int term, int want_u, int n, const double* obs, const double* tri, double mu,
                 double lam, double eps, double* coef, double* out, cudaStream_t st) {
-  k_coef<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(mu, lam, coef);
+  k_coef1<<<(MHS_Q_NDDG + 255) / 256, 256, 0, st>>>(mu, lam, coef);
   const int nb = (n + 63) / 64;
   if (want_u) k_terms<P, W_U><<<nb, 64, 0, st>>>(term, n, obs, tri, mu, lam, eps, coef, out);
   else k_terms<P, W_H><<<nb, 64, 0, st>>>(term, n, obs, tri, mu, lam, eps, coef, out);

@@ -10,7 +10,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "host_prep.h"
@@ -43,6 +46,9 @@ std::mutex g_prof_mu;
 std::vector<ProfRec> g_prof;
 int g_prof_on = 0;
 
+std::atomic<unsigned long long> g_kernels{0};
+void count_kernels(int n) { g_kernels.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+
 bool prof_enabled() { return __atomic_load_n(&g_prof_on, __ATOMIC_RELAXED) != 0; }
 
 void prof_record(int stage, cudaEvent_t a, cudaEvent_t b) {
@@ -62,8 +68,10 @@ struct UnitEntry {
   int P, KC, RF;
   UnitInit init;
   UnitRun run;
+  UnitBatch batch;
 };
-#define MHS_UNIT_ENTRY(P, KC, RF) {P, KC, RF, unit_init_##P##_##KC##_##RF, unit_run_##P##_##KC##_##RF},
+#define MHS_UNIT_ENTRY(P, KC, RF) \
+  {P, KC, RF, unit_init_##P##_##KC##_##RF, unit_run_##P##_##KC##_##RF, unit_batch_##P##_##KC##_##RF},
 const UnitEntry g_units[] = {MHS_UNIT_LIST(MHS_UNIT_ENTRY)};
 #undef MHS_UNIT_ENTRY
 const UnitInit g_terms_init[3] = {unit_init_terms_0, unit_init_terms_1, unit_init_terms_2};
@@ -136,15 +144,54 @@ __device__ unsigned long long g_census[MHS_CENSUS_N];
 std::atomic<int> g_census_on{0};
 
 // Queue the request on the unit of its (order, readout, precision).
-int run_request(const mhs_request* r, cudaStream_t st, const Layout& L) {
+// Unit of a request: its (order, readout class, precision).
+const UnitEntry* unit_of(const mhs_request* r) {
   const int kc = kind_class(r->kind);
   const int rf = r->precision == MHS_MIXED ? 1 : 0;
-  unsigned long long* census = nullptr;
-  if (g_census_on.load(std::memory_order_relaxed))
-    CUDA_TRY(cudaGetSymbolAddress((void**)&census, g_census));
   for (const UnitEntry& u : g_units)
-    if (u.P == r->order && u.KC == kc && u.RF == rf) return u.run(r, st, L, census);
-  return fail(MHS_ERR_ARG, "no kernel unit for order %d", r->order);
+    if (u.P == r->order && u.KC == kc && u.RF == rf) return &u;
+  return nullptr;
+}
+
+// ------------------------------------------------------ launch shapes
+// Per device and unit, the launch shapes in use: defaults until the
+// autotuner (mhs_autotune) or the caller (mhs_set_tune) sets them.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, Tune> g_tune;
+
+int tune_for(const mhs_request* r, Tune* t) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find({dev, r->order, kind_class(r->kind), r->precision});
+  *t = it == g_tune.end() ? Tune{} : it->second;
+  return MHS_OK;
+}
+
+int set_tune(const mhs_request* r, const Tune& t) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[{dev, r->order, kind_class(r->kind), r->precision}] = t;
+  return MHS_OK;
+}
+
+unsigned long long* census_ptr() {
+  unsigned long long* census = nullptr;
+  if (g_census_on.load(std::memory_order_relaxed) &&
+      cudaGetSymbolAddress((void**)&census, g_census) != cudaSuccess)
+    census = nullptr;
+  return census;
+}
+
+// Queue the request on the unit of its (order, readout, precision).
+int run_request(const mhs_request* r, cudaStream_t st, const Layout& L) {
+  const UnitEntry* u = unit_of(r);
+  if (!u) return fail(MHS_ERR_ARG, "no kernel unit for order %d", r->order);
+  Tune t;
+  const int rc = tune_for(r, &t);
+  if (rc) return rc;
+  return u->run(r, st, L, census_ptr(), t);
 }
 
 // Layout of the largest observer chunk whose workspace fits `bytes`
@@ -193,7 +240,26 @@ int noalloc_scratch(void** out) {
   return MHS_OK;
 }
 
+// ------------------------------------------------------------ batches
+constexpr size_t BATCH_PASS_MAX = size_t(8) << 30;
+
 }  // namespace
+
+struct mhs_batch {
+  struct Group {
+    const UnitEntry* unit;
+    std::vector<int> idx;       // requests of the group
+    size_t desc_off;            // its descriptors in the arena
+  };
+  std::vector<mhs_request> reqs;
+  std::vector<Layout> L;
+  std::vector<size_t> ws_off;
+  std::vector<Group> groups;
+  size_t bytes = 0;
+  char* arena = nullptr;
+  cudaEvent_t done = nullptr;
+  bool submitted = false;
+};
 
 extern "C" {
 
@@ -370,6 +436,212 @@ int mhs_fp_peak(int fp64, int iters, double* tflops, void* stream) {
   cudaEventDestroy(b);
   const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
   if (tflops) *tflops = flops / (ms * 1e-3) / 1e12;
+  return MHS_OK;
+}
+
+int mhs_batch_pass_bytes(const mhs_request* r, size_t* bytes, size_t* limit) {
+  if (!r || !bytes) return fail(MHS_ERR_ARG, "batch: null");
+  mhs_request q = *r;
+  q.workspace = nullptr;
+  q.workspace_bytes = 0;
+  int rc = check_request(&q);
+  if (rc) return rc;
+  *bytes = plan(&q, q.n_obs, fold_good_bytes(&q)).total;
+  if (limit) *limit = BATCH_PASS_MAX;
+  return MHS_OK;
+}
+
+int mhs_batch_create(const mhs_request* reqs, int n, mhs_batch** out) {
+  if (!out || !reqs || n < 1) return fail(MHS_ERR_ARG, "batch: empty or null");
+  std::unique_ptr<mhs_batch> b(new mhs_batch);
+  b->reqs.assign(reqs, reqs + n);
+  size_t off = 0;
+  for (int i = 0; i < n; ++i) {
+    mhs_request& r = b->reqs[i];
+    r.workspace = nullptr;
+    r.workspace_bytes = 0;
+    int rc = check_request(&r);
+    if (rc) {
+      char msg[512];
+      snprintf(msg, sizeof(msg), "%s", mhs_last_error());
+      return fail(rc, "batch request %d: %s", i, msg);
+    }
+    const Layout L = plan(&r, r.n_obs, fold_good_bytes(&r));
+    if (L.total > BATCH_PASS_MAX)
+      return fail(MHS_ERR_WORKSPACE, "batch request %d needs %zu bytes of scratch for one pass, "
+                  "above the batch limit of %zu; assemble it alone", i, L.total, BATCH_PASS_MAX);
+    b->L.push_back(L);
+    b->ws_off.push_back(off);
+    off = align_up(off + L.total);
+    const UnitEntry* u = unit_of(&r);
+    if (!u) return fail(MHS_ERR_ARG, "batch request %d: no kernel unit", i);
+    bool placed = false;
+    for (auto& g : b->groups)
+      if (g.unit == u && (b->reqs[g.idx[0]].slip != nullptr) == (r.slip != nullptr)) {
+        g.idx.push_back(i);
+        placed = true;
+        break;
+      }
+    if (!placed) b->groups.push_back({u, {i}, 0});
+  }
+  for (auto& g : b->groups) {
+    g.desc_off = off;
+    off = align_up(off + desc_bytes((int)g.idx.size()));
+  }
+  b->bytes = off;
+  *out = b.release();
+  return MHS_OK;
+}
+
+int mhs_batch_workspace_bytes(const mhs_batch* b, size_t* bytes) {
+  if (!b || !bytes) return fail(MHS_ERR_ARG, "batch: null");
+  *bytes = b->bytes;
+  return MHS_OK;
+}
+
+int mhs_batch_bind(mhs_batch* b, void* workspace, size_t bytes, void* stream) {
+  if (!b || !workspace) return fail(MHS_ERR_ARG, "batch: null");
+  if (bytes < b->bytes)
+    return fail(MHS_ERR_WORKSPACE, "batch workspace %zu bytes, need %zu", bytes, b->bytes);
+  int rc = ensure_device_tables();
+  if (rc) return rc;
+  b->arena = (char*)workspace;
+  for (size_t i = 0; i < b->reqs.size(); ++i) {
+    b->reqs[i].workspace = b->arena + b->ws_off[i];
+    b->reqs[i].workspace_bytes = b->L[i].total;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  for (auto& g : b->groups) {
+    std::vector<const mhs_request*> rp;
+    std::vector<Layout> lp;
+    for (int i : g.idx) {
+      rp.push_back(&b->reqs[i]);
+      lp.push_back(b->L[i]);
+    }
+    Tune t;
+    rc = tune_for(rp[0], &t);
+    if (rc) return rc;
+    rc = g.unit->batch(rp.data(), lp.data(), (int)rp.size(), b->arena + g.desc_off, 2, st, nullptr,
+                       t);
+    if (rc) return rc;
+  }
+  if (!b->done) CUDA_TRY(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+  return MHS_OK;
+}
+
+int mhs_submit_batch(mhs_batch* b, void* stream) {
+  if (!b || !b->arena) return fail(MHS_ERR_ARG, "batch: not bound to a workspace");
+  cudaStream_t st = (cudaStream_t)stream;
+  for (auto& g : b->groups) {
+    std::vector<const mhs_request*> rp;
+    std::vector<Layout> lp;
+    for (int i : g.idx) {
+      rp.push_back(&b->reqs[i]);
+      lp.push_back(b->L[i]);
+    }
+    Tune t;
+    int rc = tune_for(rp[0], &t);
+    if (rc) return rc;
+    rc = g.unit->batch(rp.data(), lp.data(), (int)rp.size(), b->arena + g.desc_off, 0, st,
+                       census_ptr(), t);
+    if (rc) return rc;
+  }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+  if (cap == cudaStreamCaptureStatusNone) {  // a captured submission is polled by its graph's stream
+    CUDA_TRY(cudaEventRecord(b->done, st));
+    b->submitted = true;
+  }
+  return MHS_OK;
+}
+
+int mhs_poll(mhs_batch* b, int* done, int* status_bits) {
+  if (!b || !done) return fail(MHS_ERR_ARG, "batch: null");
+  *done = 0;
+  if (!b->submitted) return fail(MHS_ERR_ARG, "batch: nothing submitted");
+  const cudaError_t e = cudaEventQuery(b->done);
+  if (e == cudaErrorNotReady) return MHS_OK;
+  if (e != cudaSuccess) return fail(MHS_ERR_CUDA, "batch event: %s", cudaGetErrorString(e));
+  int bits = 0;
+  for (size_t i = 0; i < b->reqs.size(); ++i) {
+    int h = 0;
+    CUDA_TRY(cudaMemcpy(&h, b->arena + b->ws_off[i] + b->L[i].status, sizeof(int),
+                        cudaMemcpyDeviceToHost));
+    bits |= h;
+  }
+  *done = 1;
+  if (status_bits) *status_bits = bits;
+  return MHS_OK;
+}
+
+int mhs_batch_destroy(mhs_batch* b) {
+  if (!b) return MHS_OK;
+  if (b->done) cudaEventDestroy(b->done);
+  delete b;
+  return MHS_OK;
+}
+
+int mhs_set_tune(const mhs_request* like, const mhs_tune* t) {
+  if (!like || !t) return fail(MHS_ERR_ARG, "tune: null");
+  auto ok = [](int v, int lo, int hi) { return v >= lo && v <= hi; };
+  const bool pow2 = t->final_tb > 0 && (t->final_tb & (t->final_tb - 1)) == 0;
+  if (!ok(t->pair_tb, 32, TB) || !ok(t->final_tb, 32, TB) || !pow2 || !ok(t->far_mult, 1, 16) ||
+      !ok(t->near_mult, 1, 16))
+    return fail(MHS_ERR_ARG, "tune out of range");
+  return set_tune(like, Tune{t->pair_tb, t->final_tb, t->far_mult, t->near_mult});
+}
+
+int mhs_get_tune(const mhs_request* like, mhs_tune* t) {
+  if (!like || !t) return fail(MHS_ERR_ARG, "tune: null");
+  Tune v;
+  const int rc = tune_for(like, &v);
+  if (rc) return rc;
+  *t = mhs_tune{v.pair_tb, v.final_tb, v.far_mult, v.near_mult};
+  return MHS_OK;
+}
+
+int mhs_autotune(const mhs_request* sample, void* stream, mhs_tune* chosen, double* best_ms) {
+  int rc = check_request(sample);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  Tune keep;
+  rc = tune_for(sample, &keep);
+  if (rc) return rc;
+  Tune best = keep;
+  double best_t = 1e300;
+  rc = mhs_assemble(sample, stream);   // warm-up at the current shape
+  for (int ptb : {64, 128})
+    for (int ftb : {64, 128})
+      for (int mult : {2, 4, 8}) {
+        if (rc) break;
+        const Tune t{ptb, ftb, mult, mult};
+        set_tune(sample, t);
+        CUDA_TRY(cudaEventRecord(a, st));
+        rc = mhs_assemble(sample, stream);
+        CUDA_TRY(cudaEventRecord(b, st));
+        CUDA_TRY(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+        if (!rc && ms < best_t) {
+          best_t = ms;
+          best = t;
+        }
+      }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  set_tune(sample, rc ? keep : best);
+  if (rc) return rc;
+  if (chosen) *chosen = mhs_tune{best.pair_tb, best.final_tb, best.far_mult, best.near_mult};
+  if (best_ms) *best_ms = best_t;
+  return MHS_OK;
+}
+
+int mhs_kernel_count(unsigned long long* n) {
+  if (!n) return fail(MHS_ERR_ARG, "null count");
+  *n = g_kernels.exchange(0, std::memory_order_relaxed);
   return MHS_OK;
 }
 

@@ -47,6 +47,10 @@ struct SrcPrep {
 };
 
 constexpr int TB = 128;          // threads per block for pair-parallel kernels
+// The mixed form takes the closed-form near field only within this many
+// element lengths (sqrt(|x - c|^2 + eps^2) <= MIXED_NEAR_L * L) and the float
+// 12 x 12 rule beyond, out to D_STAR; the FP64 form uses D_STAR throughout.
+constexpr double MIXED_NEAR_L = 3.0;
 constexpr int QFLOOR = cst::IMAGE_Q_GAUSS_MIN;
 
 enum : int { KD_DISP = 0, KD_HE = 1, KD_E = 2 };   // what the stages compute
@@ -60,10 +64,71 @@ MHS_FI constexpr int row_of(int kc) { return comps_of(kc) + 2; }
 
 inline size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+// ----------------------------------------------------- request descriptors
+// What the output stage needs of one pass (one observer chunk of one
+// request).
+struct FinalArgs {
+  int kind, subtract, out_f32, n_a, n_b;
+  int64_t lo, n_chunk, n_src, n_obs, n_dof;
+  const double* normals;
+  const double* rec_basis;
+  const double* src_basis;
+  const int32_t* col_ptr;
+  const int32_t* col_ent;
+  double mu, lam;
+  void* out;
+  const double* slip;   // apply mode: (n_dof, n_s) slip; out is (n_obs, nv / n_s)
+};
+
+// One pass of one request as the batched stage kernels read it: a group of
+// passes of the same (order, readout, precision) runs each stage in one
+// launch, every block finding its pass by the prefix of block counts.
+struct ReqDesc {
+  FinalArgs fa;
+  const double* obs;
+  const double* tris;
+  const double* eps;
+  SrcPrep* prep;
+  double* G;
+  double* coef;
+  double* T;
+  int* status;
+  int fold, pad;
+};
+
+// Stages' block counts per pass, as exclusive prefixes over the group
+// (n + 1 entries each), following the descriptors in device memory.
+enum : int { OFF_COEF = 0, OFF_PREP = 1, OFF_PAIR = 2, OFF_FINAL = 3, N_OFF = 4 };
+
+MHS_FI int find_req(const long long* off, int n, long long b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+inline size_t desc_bytes(int n) {
+  return align_up(sizeof(ReqDesc) * (size_t)n) + sizeof(long long) * (size_t)N_OFF * (n + 1);
+}
+
+// Launch shapes the autotuner picks per (order, readout, precision) and
+// device: threads per block of the pair kernels (observer tile) and of the
+// output stage (column tile), and the grid multipliers (blocks per SM x
+// this factor) of the fold's grid-stride load kernels.
+struct Tune {
+  int pair_tb = 128;
+  int final_tb = 128;
+  int far_mult = 4;
+  int near_mult = 4;
+};
+
 // Workspace carve-up for a chunk of `chunk` observers plus `fold_bytes`
 // for the fold's plan, pair batches and node waves.
 struct Layout {
-  size_t status, coef, prep, G, cnt, list, T, fold, fold_bytes, total;
+  size_t status, desc, coef, prep, G, cnt, list, T, fold, fold_bytes, total;
   int64_t chunk;
 };
 
@@ -73,6 +138,7 @@ inline Layout plan(const mhs_request* r, int64_t chunk, size_t fold_bytes = 0) {
   Layout L;
   size_t off = 0;
   L.status = off; off = align_up(off + 256);
+  L.desc = off; off = align_up(off + desc_bytes(1));
   L.coef = off; off = align_up(off + sizeof(double) * IMAGE_COEF_SIZE);
   L.prep = off; off = align_up(off + sizeof(SrcPrep) * (size_t)r->n_src);
   L.G = off;
@@ -115,6 +181,8 @@ int fail(int code, const char* fmt, ...);
 // Stage timing: whether it is on, and the record of one stage's events.
 bool prof_enabled();
 void prof_record(int stage, cudaEvent_t a, cudaEvent_t b);
+// Count of kernels queued (mhs_kernel_count).
+void count_kernels(int n);
 
 #define MHS_CUDA_TRY(x)                                                                     \
   do {                                                                                      \
@@ -151,7 +219,13 @@ struct StageTimer {
 // of the fold's work units, or null.
 using UnitInit = int (*)(const double* glx, const double* glw);
 using UnitRun = int (*)(const mhs_request* r, cudaStream_t st, const Layout& L,
-                        unsigned long long* census);
+                        unsigned long long* census, const Tune& tune);
+// A batch: n requests of this unit, request i on its own workspace part with
+// layout L[i] (one pass, all its observers); descriptors at desc (device,
+// desc_bytes(n), already holding what batch_descs wrote when upload = 0).
+using UnitBatch = int (*)(const mhs_request* const* r, const Layout* L, int n, void* desc,
+                          int upload, cudaStream_t st, unsigned long long* census,
+                          const Tune& tune);
 using UnitTerms = int (*)(int term, int want_u, int n, const double* obs, const double* tri,
                           double mu, double lam, double eps, double* coef, double* out,
                           cudaStream_t st);
@@ -164,7 +238,10 @@ using UnitTerms = int (*)(int term, int want_u, int n, const double* obs, const 
 #define MHS_UNIT_DECL(P, KC, RF)                                                     \
   int unit_init_##P##_##KC##_##RF(const double* glx, const double* glw);             \
   int unit_run_##P##_##KC##_##RF(const mhs_request* r, cudaStream_t st, const Layout& L, \
-                                 unsigned long long* census);
+                                 unsigned long long* census, const Tune& tune);      \
+  int unit_batch_##P##_##KC##_##RF(const mhs_request* const* r, const Layout* L, int n,  \
+                                   void* desc, int upload, cudaStream_t st,          \
+                                   unsigned long long* census, const Tune& tune);
 MHS_UNIT_LIST(MHS_UNIT_DECL)
 #undef MHS_UNIT_DECL
 

@@ -40,11 +40,22 @@ int MHS_CAT4(unit_init_, MHS_UNIT_P, MHS_UNIT_KC, MHS_UNIT_RF)(const double* glx
   return copy_tables(glx, glw);
 }
 
+using UnitRF = std::conditional_t<MHS_UNIT_RF == 1, float, double>;
+
 int MHS_CAT4(unit_run_, MHS_UNIT_P, MHS_UNIT_KC, MHS_UNIT_RF)(const mhs_request* r,
                                                               cudaStream_t st, const Layout& L,
-                                                              unsigned long long* census) {
-  using RF = std::conditional_t<MHS_UNIT_RF == 1, float, double>;
-  return run<MHS_UNIT_P, MHS_UNIT_KC, RF>(r, st, L, census);
+                                                              unsigned long long* census,
+                                                              const Tune& tune) {
+  return run<MHS_UNIT_P, MHS_UNIT_KC, UnitRF>(r, st, L, census, tune);
+}
+
+int MHS_CAT4(unit_batch_, MHS_UNIT_P, MHS_UNIT_KC, MHS_UNIT_RF)(const mhs_request* const* r,
+                                                                const Layout* L, int n,
+                                                                void* desc, int upload,
+                                                                cudaStream_t st,
+                                                                unsigned long long* census,
+                                                                const Tune& tune) {
+  return run_batch<MHS_UNIT_P, MHS_UNIT_KC, UnitRF>(r, L, n, desc, upload, st, census, tune);
 }
 
 #endif

@@ -39,6 +39,10 @@ __all__ = [
     "traction_matrix",
     "interaction_matrix",
     "collocation_points",
+    "interaction_matvec",
+    "disp_matvec",
+    "stress_matvec",
+    "traction_matvec",
 ]
 
 COLLOCATION_SHRINK = 0.5
@@ -310,7 +314,7 @@ class Pending:
 
 def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fold,
             subtract=True, normals=None, rec_basis=None, src_basis=None, precision="fp64",
-            like=None):
+            like=None, slip=None):
     """Run one request; returns the output (numpy or torch per the inputs)."""
     torch = _torch()
     lib = _native.load()
@@ -319,7 +323,7 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
     defer = getattr(_defer, "on", False)
     if defer and out is not None:
         raise ValueError("a served request returns its own device tensor: out= does not apply")
-    if out is not None and not _is_torch(out):
+    if out is not None and not _is_torch(out) and slip is None:
         return _launch_streamed(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out,
                                 fold, subtract, normals, rec_basis, src_basis, precision, device)
     # output buffer
@@ -360,6 +364,7 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
     req.src_basis = ptr(src_basis)
     req.n_a = 0 if rec_basis is None else int(np.shape(rec_basis)[1])
     req.n_b = 0 if src_basis is None else int(np.shape(src_basis)[1])
+    req.slip = ptr(slip)
     if ids is not None:
         ids64 = np.ascontiguousarray(ids, dtype=np.int64)
         col_ptr = np.empty(n_dof + 1, dtype=np.int32)
@@ -380,7 +385,13 @@ def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fol
         entries = 1
         for d in out_shape:
             entries *= int(d)
-        return Pending(req, keep, tuple(out_shape), torch.float64, device, good.value, entries)
+        pend = Pending(req, keep, tuple(out_shape), torch.float64, device, good.value, entries)
+        # whether any source reaches the fold depth (host copies: the batch
+        # sets fold = 0 for requests where it changes nothing)
+        depth = -np.asarray(tri, float)[:, :, 2].max(axis=1)
+        pend.straddles = bool(fold) and bool(np.any(depth < defaults.FOLD_SOURCE_DEPTH_EPS *
+                                                    np.asarray(eps_arr, float)))
+        return pend
     with _WS.lock(device):
         ws = _WS.get(device, good.value)
         req.workspace = ctypes.c_void_p(ws.data_ptr())
@@ -439,7 +450,10 @@ def _launch_streamed(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape,
 
 def _check_out(out, shape, n_obs, n_src, kind, parts):
     if out is None:
-        chunking.refuse_if_too_large(n_obs, n_src, kind, np.float64, parts)
+        # a served request's output stays on the device: the serving loop
+        # admits it against its device-memory budget instead of the host ceiling
+        if not getattr(_defer, "on", False):
+            chunking.refuse_if_too_large(n_obs, n_src, kind, np.float64, parts)
         return
     if _is_torch(out):
         torch = _torch()
@@ -582,16 +596,8 @@ def _rows(rows, n_rec: int):
     return lo, hi
 
 
-def interaction_matrix(tris, material, eps, *, receiver=("strike", "dip", "normal"),
-                       source=("strike", "dip", "tensile"), obs_tris=None, obs_pts=None, order=0,
-                       shrink=COLLOCATION_SHRINK, subtract_eigenstress=True,
-                       layout="discontinuous", shared=None, rows=None, out=None, fold=True,
-                       precision="fp64"):
-    """On-fault interaction ``(n_rec_dof, n_src_dof, n_a, n_b)``: traction on
-    each receiver dof's own plane resolved on its (strike, dip, tensile)
-    frame from unit slip along each source frame direction
-    (mhs/matrices.py:378-480)."""
-    like = (tris,)
+def _interaction_setup(tris, material, eps, receiver, source, obs_tris, obs_pts, order, shrink,
+                       layout, shared, rows):
     tri = _as_np(tris).reshape(-1, 3, 3)
     p = _order(order)
     K = n_nodes(p)
@@ -624,11 +630,97 @@ def interaction_matrix(tris, material, eps, *, receiver=("strike", "dip", "norma
     obs, tri, mu, lam, eps_arr = _coerce(np.asarray(pts, float)[lo:hi], tri, material, eps)
     rec = tdcs.component_index(receiver)
     src = tdcs.component_index(source)
-    shape = (hi - lo, n_src_dof, len(rec), len(src))
-    _check_out(out, shape, hi - lo, n_src_dof, (len(rec), len(src)), False)
     rec_basis = np.ascontiguousarray(rec_frame[lo:hi][:, rec, :])
     src_basis = np.ascontiguousarray(src_frame[:, src, :])
     normals = np.ascontiguousarray(rec_frame[lo:hi, 2, :])
-    return _launch(_native.INTERACTION, obs, tri, mu, lam, eps_arr, p, ids, n_src_dof, shape,
-                   out, fold, subtract=subtract_eigenstress, normals=normals,
-                   rec_basis=rec_basis, src_basis=src_basis, precision=precision, like=like)
+    return dict(obs=obs, tri=tri, mu=mu, lam=lam, eps_arr=eps_arr, p=p, ids=ids,
+                n_src_dof=n_src_dof, lo=lo, hi=hi, rec=rec, src=src, rec_basis=rec_basis,
+                src_basis=src_basis, normals=normals)
+
+
+def interaction_matrix(tris, material, eps, *, receiver=("strike", "dip", "normal"),
+                       source=("strike", "dip", "tensile"), obs_tris=None, obs_pts=None, order=0,
+                       shrink=COLLOCATION_SHRINK, subtract_eigenstress=True,
+                       layout="discontinuous", shared=None, rows=None, out=None, fold=True,
+                       precision="fp64"):
+    """On-fault interaction ``(n_rec_dof, n_src_dof, n_a, n_b)``: traction on
+    each receiver dof's own plane resolved on its (strike, dip, tensile)
+    frame from unit slip along each source frame direction
+    (mhs/matrices.py:378-480)."""
+    g = _interaction_setup(tris, material, eps, receiver, source, obs_tris, obs_pts, order,
+                           shrink, layout, shared, rows)
+    shape = (g["hi"] - g["lo"], g["n_src_dof"], len(g["rec"]), len(g["src"]))
+    _check_out(out, shape, g["hi"] - g["lo"], g["n_src_dof"], (len(g["rec"]), len(g["src"])), False)
+    return _launch(_native.INTERACTION, g["obs"], g["tri"], g["mu"], g["lam"], g["eps_arr"], g["p"],
+                   g["ids"], g["n_src_dof"], shape, out, fold, subtract=subtract_eigenstress,
+                   normals=g["normals"], rec_basis=g["rec_basis"], src_basis=g["src_basis"],
+                   precision=precision, like=(tris,))
+
+
+# ------------------------------------------------------------ apply mode
+def _slip_arg(slip, n_dof, n_s, name):
+    a = slip.detach().cpu().numpy() if _is_torch(slip) else np.asarray(slip, float)
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.shape != (n_dof, n_s):
+        raise ValueError(f"{name}: slip must have shape ({n_dof}, {n_s}), got {a.shape}")
+    return a
+
+
+def interaction_matvec(tris, material, eps, slip, *, receiver=("strike", "dip", "normal"),
+                       source=("strike", "dip", "tensile"), obs_tris=None, obs_pts=None, order=0,
+                       shrink=COLLOCATION_SHRINK, subtract_eigenstress=True,
+                       layout="discontinuous", shared=None, rows=None, fold=True,
+                       precision="fp64"):
+    """``interaction_matrix(...)`` contracted with a slip vector without
+    storing the matrix: ``y[r, a] = sum_{c, b} K[r, c, a, b] slip[c, b]``,
+    slip ``(n_src_dof, n_b)``, result ``(n_rec_dof, n_a)`` -- the traction a
+    slip distribution puts on every receiver dof (the product a cycle or
+    cascade model reads; studies/active_fractal/kernel.py:1-30 stores K
+    for it)."""
+    g = _interaction_setup(tris, material, eps, receiver, source, obs_tris, obs_pts, order,
+                           shrink, layout, shared, rows)
+    s = _slip_arg(slip, g["n_src_dof"], len(g["src"]), "interaction_matvec")
+    shape = (g["hi"] - g["lo"], len(g["rec"]))
+    return _launch(_native.INTERACTION, g["obs"], g["tri"], g["mu"], g["lam"], g["eps_arr"], g["p"],
+                   g["ids"], g["n_src_dof"], shape, None, fold, subtract=subtract_eigenstress,
+                   normals=g["normals"], rec_basis=g["rec_basis"], src_basis=g["src_basis"],
+                   precision=precision, like=(tris, slip), slip=s)
+
+
+def _field_matvec(kind, comps, name, obs_pts, tris, material, eps, slip, order, layout, shared,
+                  fold, precision, subtract=True, normals=None):
+    obs, tri, mu, lam, eps_arr = _coerce(obs_pts, tris, material, eps)
+    p = _order(order)
+    ids, n_dof, _ = _columns(tri, p, layout, shared)
+    s = _slip_arg(slip, n_dof, 3, name)
+    nrm = None if normals is None else _coerce_normals(normals, obs.shape[0])
+    shape = (obs.shape[0],) + comps
+    return _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, shape, None, fold,
+                   subtract=subtract, normals=nrm, precision=precision,
+                   like=(obs_pts, tris, slip), slip=s)
+
+
+def disp_matvec(obs_pts, tris, material, eps, slip, *, order=0, layout="discontinuous",
+                shared=None, fold=True, precision="fp64"):
+    """``disp_matrix(...)`` contracted with Cartesian slip ``(n_dof, 3)``:
+    the displacement ``(n_obs, 3)`` of that slip distribution."""
+    return _field_matvec(_native.DISP, (3,), "disp_matvec", obs_pts, tris, material, eps, slip,
+                         order, layout, shared, fold, precision)
+
+
+def stress_matvec(obs_pts, tris, material, eps, slip, *, subtract_eigenstress=True, order=0,
+                  layout="discontinuous", shared=None, fold=True, precision="fp64"):
+    """``stress_matrix(...)`` contracted with Cartesian slip ``(n_dof, 3)``:
+    the stress ``(n_obs, 3, 3)`` of that slip distribution."""
+    return _field_matvec(_native.STRESS, (3, 3), "stress_matvec", obs_pts, tris, material, eps,
+                         slip, order, layout, shared, fold, precision,
+                         subtract=subtract_eigenstress)
+
+
+def traction_matvec(obs_pts, obs_normals, tris, material, eps, slip, *, subtract_eigenstress=True,
+                    order=0, layout="discontinuous", shared=None, fold=True, precision="fp64"):
+    """``traction_matrix(...)`` contracted with Cartesian slip
+    ``(n_dof, 3)``: the traction ``(n_obs, 3)`` of that slip distribution."""
+    return _field_matvec(_native.TRACTION, (3,), "traction_matvec", obs_pts, tris, material, eps,
+                         slip, order, layout, shared, fold, precision,
+                         subtract=subtract_eigenstress, normals=obs_normals)

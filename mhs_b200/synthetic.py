@@ -188,3 +188,50 @@ def batched_requests(n: int = 64, seed: int = 0, tri_range=(50, 5000), obs_range
         reqs.append(dict(kind=kind, order=order, obs=obs, tris=tris, normals=nrm, mu=30.0,
                          lam=float(rng.uniform(20.0, 40.0)), eps=0.1))
     return reqs
+
+
+def serving_requests(n: int, seed: int = 0, rate_per_s: float = 20.0, tri_range=(100, 20000),
+                     obs_range=(100, 50000), strike_strike=(10000, 20000)):
+    """The serving stream: Poisson arrivals at `rate_per_s`; per request
+    (seeded) kind uniform in {disp, stress, traction, interaction}, triangle
+    count log-uniform in `tri_range`, observer count log-uniform in
+    `obs_range`, order in {0, 1, 2}, a planar rectangular fault as in
+    batched_requests, eps per triangle 0.3 x its mean edge.  The stream also
+    carries scalar strike/strike interaction requests at each size of
+    `strike_strike` (placed at evenly spaced positions in the stream).
+    Returns a list of dicts with 'arrival_s' (seconds after the first)."""
+    rng0 = np.random.default_rng([seed, 10 ** 6])
+    gaps = rng0.exponential(1.0 / rate_per_s, n)
+    arrival = np.concatenate([[0.0], np.cumsum(gaps[1:])])
+    big_at = {int(round((k + 1) * n / (len(strike_strike) + 1))): sz
+              for k, sz in enumerate(strike_strike)}
+    kinds = ("disp", "stress", "traction", "interaction")
+    reqs = []
+    for i in range(n):
+        rng = np.random.default_rng([seed, i])
+        if i in big_at:
+            n_tri, kind, order = big_at[i], "interaction", 0
+        else:
+            n_tri = int(round(math.exp(rng.uniform(math.log(tri_range[0]), math.log(tri_range[1])))))
+            kind = kinds[int(rng.integers(0, len(kinds)))]
+            order = int(rng.integers(0, 3))
+        n_obs = int(round(math.exp(rng.uniform(math.log(obs_range[0]), math.log(obs_range[1])))))
+        dip = float(rng.uniform(15.0, 90.0))
+        top = -float(rng.uniform(0.0, 5.0))
+        cells = max(1, n_tri // 2)
+        nv = max(1, int(round(math.sqrt(cells / 2.0))))
+        nu = max(1, int(round(cells / nv)))
+        tris = planar_fault(0.0, dip, float(nu), float(nv), top, nu, nv)
+        ext = 3.0 * max(nu, nv)
+        obs = np.column_stack([rng.uniform(-ext / 2, ext / 2, n_obs),
+                               rng.uniform(-ext / 2, ext / 2, n_obs),
+                               -rng.uniform(0.0, ext / 2, n_obs)])
+        nrm = rng.standard_normal((n_obs, 3))
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        r = dict(kind=kind, order=order, obs=obs, tris=tris, normals=nrm, mu=30.0,
+                 lam=float(rng.uniform(20.0, 40.0)), eps=0.3 * mean_edge(tris),
+                 arrival_s=float(arrival[i]))
+        if i in big_at:
+            r.update(receiver=("strike",), source=("strike",))
+        reqs.append(r)
+    return reqs

@@ -144,3 +144,45 @@ def test_fold_off_equals_lift_outside_band(cuda):
     A = m.stress_matrix(deep, c["tris"], mat, c["eps"])
     B = m.stress_matrix(deep, c["tris"], mat, c["eps"], fold=False)
     assert np.array_equal(A, B)
+
+
+# ------------------------------------------------------------ apply mode
+@pytest.mark.parametrize("layout", ["discontinuous", "continuous"])
+def test_matvec_equals_matrix_times_slip(cuda, layout):
+    """The apply mode (the matrix contracted with a slip vector, never
+    stored) against the FP64 matrix contracted on the host."""
+    import mhs_b200 as m
+    from conftest import golden
+    d = golden("continuous")
+    mat = m.Material(float(d["mu"]), float(d["lam"]))
+    kw = dict(order=2, layout=layout) if layout == "continuous" else dict(order=1)
+    rng = np.random.default_rng(3)
+    K = m.interaction_matrix(d["tris"], mat, 0.1, source=("strike", "dip"), **kw)
+    slip = rng.standard_normal((K.shape[1], 2))
+    y = m.interaction_matvec(d["tris"], mat, 0.1, slip, source=("strike", "dip"), **kw)
+    ref = np.einsum("rcab,cb->ra", K, slip)
+    assert y.shape == ref.shape
+    assert relmax(y, ref) < 1e-12
+    sl3 = rng.standard_normal((K.shape[1], 3))
+    T = m.traction_matrix(d["obs"], d["obs_normals"], d["tris"], mat, 0.1, **kw)
+    t = m.traction_matvec(d["obs"], d["obs_normals"], d["tris"], mat, 0.1, sl3, **kw)
+    assert relmax(t, np.einsum("oicm,cm->oi", T, sl3)) < 1e-12
+    S = m.stress_matrix(d["obs"], d["tris"], mat, 0.1, **kw)
+    st = m.stress_matvec(d["obs"], d["tris"], mat, 0.1, sl3, **kw)
+    assert relmax(st, np.einsum("oijcm,cm->oij", S, sl3)) < 1e-12
+    U = m.disp_matrix(d["obs"], d["tris"], mat, 0.1, **kw)
+    u = m.disp_matvec(d["obs"], d["tris"], mat, 0.1, sl3, **kw)
+    assert relmax(u, np.einsum("oicm,cm->oi", U, sl3)) < 1e-12
+
+
+def test_matvec_with_the_fold_and_rows(cuda):
+    import mhs_b200 as m
+    from conftest import golden
+    d = golden("c2_rows")
+    mat = m.Material(float(d["mu"]), float(d["lam"]))
+    rng = np.random.default_rng(9)
+    slip = rng.standard_normal((d["tris"].shape[0], 3))
+    r0 = int(d["rows"][0])
+    y = m.interaction_matvec(d["tris"], mat, d["eps"], slip, rows=(r0, r0 + 1))
+    ref = np.einsum("cab,cb->a", d["K"][0], slip)
+    assert relmax(y[0], ref) < 1e-12
