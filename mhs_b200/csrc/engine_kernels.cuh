@@ -194,16 +194,19 @@ MHS_HD void szz_coefficient(const Frame& f, double eps, const Material& m, int l
 // ----------------------------------------------------------- direct term
 // One source triangle at one observer, all K nodes: near field by the
 // closed-form recursion (sqrt(|x - c|^2 + eps^2) <= D_STAR L), far field by
-// the 12x12 (8x8 beyond D_STAR_DISTANT L) product rule
-// (mhs/fullspace/moments.py:551-601, mhs/fullspace/kernels.py:126-215).
-// R_FAR is the arithmetic type of the far-field quadrature.
+// the product rule r12 (12 x 12), r8 (8 x 8) beyond far_switch_l L
+// (D_STAR_DISTANT: mhs/fullspace/moments.py:551-601,
+// mhs/fullspace/kernels.py:126-215).  R_FAR is the arithmetic type of the
+// far-field quadrature; the mixed form passes its own float rules and
+// switch distance.
 // The node loops are fully unrolled so that every output offset is a
 // compile-time constant: a -O3 device build with them kept rolled returned
 // wrong P >= 1 tensors where this function is inlined into the fold kernels.
 template <int P, int WANT, class R_FAR = double, class Q = QuadRule>
 MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
                         const double* x, double eps, const Material& m,
-                        double* U, double* H, double* E, double near_l = cst::D_STAR) {
+                        double* U, double* H, double* E, double near_l = cst::D_STAR,
+                        double far_switch_l = cst::D_STAR_DISTANT) {
   using S = DirectSpec<P, WANT>;
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
@@ -230,7 +233,7 @@ MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
       if (WANT & W_E) E[k] = e4 * W[sp.w_off[nslot(7)]];
     }
   } else {
-    const Q& q = (D > cst::D_STAR_DISTANT * f.L) ? r8 : r12;
+    const Q& q = (D > far_switch_l * f.L) ? r8 : r12;
     double W[K * NW] = {};
     weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
 #pragma unroll
@@ -324,6 +327,23 @@ MHS_HD void contract_dg(const double* DG, const double* nrm, const Material& m, 
 
 // DDG (i, j, p, m) -> displacement gradient -> symmetric Hooke stress
 // (mhs/kernels/image.py:138-161).
+// H from the traction-operator image S[i][p][k] of DDG: the symmetric part
+// in (i, p) through Hooke's law, per slip component k.
+MHS_HD void hooke_from_traction(const double (&S)[3][3][3], const Material& m, double* H) {
+  for (int k = 0; k < 3; ++k) {
+    double e[3][3];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) e[a][b] = 0.5 * (S[a][b][k] + S[b][a][k]);
+    const double tr = e[0][0] + e[1][1] + e[2][2];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double v = 2.0 * m.mu * e[a][b];
+        if (a == b) v += m.lam * tr;
+        H[9 * a + 3 * b + k] = v;
+      }
+  }
+}
+
 MHS_HD void contract_ddg(const double* DDG, const double* nrm, const Material& m, double* H) {
   double S[3][3][3];
   for (int i = 0; i < 3; ++i)
@@ -339,18 +359,7 @@ MHS_HD void contract_ddg(const double* DDG, const double* nrm, const Material& m
         S[i][p][k] = m.mu * s1 + m.mu * s2 + m.lam * nrm[k] * trm;
       }
     }
-  for (int k = 0; k < 3; ++k) {
-    double e[3][3];
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) e[a][b] = 0.5 * (S[a][b][k] + S[b][a][k]);
-    const double tr = e[0][0] + e[1][1] + e[2][2];
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) {
-        double v = 2.0 * m.mu * e[a][b];
-        if (a == b) v += m.lam * tr;
-        H[9 * a + 3 * b + k] = v;
-      }
-  }
+  hooke_from_traction(S, m, H);
 }
 
 // --------------------------------------------------------- image R-family
@@ -361,7 +370,8 @@ template <int P, int WANT, class R_FAR = double, class Q = QuadRule>
 MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
                          const Q& r12, const Q& r8, const double* x, double eps,
                          const Material& m, const ImageCoef& ic, double* U, double* H,
-                         double near_l = cst::D_STAR) {
+                         double near_l = cst::D_STAR,
+                         double far_switch_l = cst::D_STAR_DISTANT) {
   using S = SpecImg<P>;
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
@@ -383,7 +393,7 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
     shape_coeffs<P>(fi, X0, X1, c);
     for (int k = 0; k < K; ++k) weight_closed<S, P>(T, c, k, Wall + k * NW);
   } else {
-    const Q& q = (D > cst::D_STAR_DISTANT * fi.L) ? r8 : r12;
+    const Q& q = (D > far_switch_l * fi.L) ? r8 : r12;
     weight_far<S, P, R_FAR>(q, X0, X1, h2, Wall);
   }
 #pragma unroll 1
@@ -527,15 +537,87 @@ MHS_HD void build_qrule(const Frame& f, const double* glx, const double* glw, in
 
 // Q-family moments by quadrature, contracted (image.py:315-432).
 //
-// One pass per node k.  The basis sums B_m = sum_t wN_t[k] D1^a D2^b D3^c /
-// (R2^n Q^q) of exactly the monomials the contraction reads are kept in
-// registers: the generated lists spell every monomial's exponents as
+// Per node k, the basis sums B_m = sum_t wN_t[k] D1^a D2^b D3^c / (R2^n Q^q)
+// of exactly the monomials the contraction reads, in passes over ranges of
+// the monomial index: a pass keeps its range's sums in registers through the
+// point loop (the generated lists spell every monomial's exponents as
 // literals, so the products and the record-by-record contraction are
-// straight-line code.  Each monomial is formed as the ordered product
-// p1[a] p2[b] p3[c] pr[n] pq[q] with p[0] = 1 (a factor of one is exact), the
-// points are summed in rule order and the records in table order, as mhs
-// does.  Rule: count() and node(t, y, wN[K]) in the arithmetic type R of
-// the point sums (double; float for the mixed form's far pairs).
+// straight-line code) and then contracts that range's records.  Each
+// monomial is formed as the ordered product p1[a] p2[b] p3[c] pr[n] pq[q]
+// with p[0] = 1 (a factor of one is exact), the points are summed in rule
+// order, and -- the records being sorted by monomial -- passes in
+// increasing range add the records in table order, as mhs does.  Rule:
+// count() and node(t, y, wN[K]) in the arithmetic type R of the point sums
+// (double; float for the mixed form's far pairs).
+//
+// The stress readout contracts each DDG record straight into the 27 entries
+// of its traction-operator image S[i][p][k] = mu sum_l n_l (DDG[i,k,p,l] +
+// DDG[i,l,p,k]) + lam n_k sum_j DDG[i,j,p,j] (contract_ddg), so a pass holds
+// 27 accumulators instead of 81: with mun = mu n and lamn = lam n, record
+// slot (i, a, p, b) adds mun[b] v to S[i][p][a], mun[a] v to S[i][p][b] and,
+// when a = b, lamn[k] v to every S[i][p][k].  D is DG (27) for the
+// displacement readout, S (27, as 9 i + 3 p + k) for the stress readout.
+template <int P, int WANT, int LO, int HI, class Rule, class R>
+MHS_HD void image_q_pass(const Rule& q, int k, R x0, R x1, R x2, R e2, const ImageCoef& ic,
+                         double* D, const double* mun, const double* lamn) {
+  constexpr int K = n_nodes(P);
+  R bs[HI - LO];
+#define MHS_QZ(i, a, b, c, n, qq) \
+  if constexpr ((i) >= LO && (i) < HI) bs[(i) - LO] = R(0);
+  if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QZ) }
+  else { MHS_Q_MONO_DDG(MHS_QZ) }
+#undef MHS_QZ
+  const int nq = q.count();
+#pragma unroll 1
+  for (int t = 0; t < nq; ++t) {
+    R y[3], wN[K];
+    q.node(t, y, wN);
+    const R d1 = x0 - y[0];
+    const R d2 = x1 - y[1];
+    const R d3 = x2 + y[2];
+    const R r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
+    const R ir = R(1) / r2, iq = R(1) / (r2 - d3);
+    R p1[5], p2[5], p3[5], pr[8], pq[5];
+    p1[0] = R(1); p2[0] = R(1); p3[0] = R(1); pr[0] = R(1); pq[0] = R(1);
+    p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
+#pragma unroll
+    for (int i = 2; i < 5; ++i) {
+      p1[i] = p1[i - 1] * d1;
+      p2[i] = p2[i - 1] * d2;
+      p3[i] = p3[i - 1] * d3;
+      pq[i] = pq[i - 1] * iq;
+    }
+#pragma unroll
+    for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
+    const R w = wN[k];
+#define MHS_QA(i, a, b, c, n, qq) \
+  if constexpr ((i) >= LO && (i) < HI) \
+    bs[(i) - LO] += ((((p1[a] * p2[b]) * p3[c]) * pr[n]) * pq[qq]) * w;
+    if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QA) }
+    else { MHS_Q_MONO_DDG(MHS_QA) }
+#undef MHS_QA
+  }
+#define MHS_QTD(r, mi, slot)                                                     \
+  if constexpr ((mi) >= LO && (mi) < HI) {                                      \
+    const double v = ic.q_ddg[r] * bs[(mi) - LO];                                \
+    constexpr int qi = (slot) / 27, qa = ((slot) / 9) % 3, qp = ((slot) / 3) % 3; \
+    constexpr int qb = (slot) % 3;                                               \
+    D[9 * qi + 3 * qp + qa] += mun[qb] * v;                                      \
+    D[9 * qi + 3 * qp + qb] += mun[qa] * v;                                      \
+    if constexpr (qa == qb) {                                                    \
+      D[9 * qi + 3 * qp + 0] += lamn[0] * v;                                     \
+      D[9 * qi + 3 * qp + 1] += lamn[1] * v;                                     \
+      D[9 * qi + 3 * qp + 2] += lamn[2] * v;                                     \
+    }                                                                            \
+  }
+#define MHS_QTU(r, mi, slot) \
+  if constexpr ((mi) >= LO && (mi) < HI) D[slot] += ic.q_dg[r] * bs[(mi) - LO];
+  if constexpr (WANT == W_U) { MHS_Q_TERMS_DG(MHS_QTU) }
+  else { MHS_Q_TERMS_DDG(MHS_QTD) }
+#undef MHS_QTD
+#undef MHS_QTU
+}
+
 template <int P, int WANT, class Rule, class R = double>
 MHS_HD void image_q_eval(const Rule& q, const double* nrm, const double* x, double eps,
                          const Material& m, const ImageCoef& ic, double* U, double* H) {
@@ -543,55 +625,31 @@ MHS_HD void image_q_eval(const Rule& q, const double* nrm, const double* x, doub
   constexpr int K = n_nodes(P);
   const R e2 = R(eps * eps);
   const R x0 = R(x[0]), x1 = R(x[1]), x2 = R(x[2]);
-  const int nq = q.count();
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    R bs[MHS_Q_NMONO];
-#define MHS_QZ(i, a, b, c, n, qq) bs[i] = R(0);
-    if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QZ) }
-    else { MHS_Q_MONO_DDG(MHS_QZ) }
-#undef MHS_QZ
+  const double mun[3] = {m.mu * nrm[0], m.mu * nrm[1], m.mu * nrm[2]};
+  const double lamn[3] = {m.lam * nrm[0], m.lam * nrm[1], m.lam * nrm[2]};
 #pragma unroll 1
-    for (int t = 0; t < nq; ++t) {
-      R y[3], wN[K];
-      q.node(t, y, wN);
-      const R d1 = x0 - y[0];
-      const R d2 = x1 - y[1];
-      const R d3 = x2 + y[2];
-      const R r2 = sqrt(((d1 * d1 + d2 * d2) + d3 * d3) + e2);
-      const R ir = R(1) / r2, iq = R(1) / (r2 - d3);
-      R p1[5], p2[5], p3[5], pr[8], pq[5];
-      p1[0] = R(1); p2[0] = R(1); p3[0] = R(1); pr[0] = R(1); pq[0] = R(1);
-      p1[1] = d1; p2[1] = d2; p3[1] = d3; pr[1] = ir; pq[1] = iq;
-#pragma unroll
-      for (int i = 2; i < 5; ++i) {
-        p1[i] = p1[i - 1] * d1;
-        p2[i] = p2[i - 1] * d2;
-        p3[i] = p3[i - 1] * d3;
-        pq[i] = pq[i - 1] * iq;
-      }
-#pragma unroll
-      for (int i = 2; i < 8; ++i) pr[i] = pr[i - 1] * ir;
-      const R w = wN[k];
-#define MHS_QA(i, a, b, c, n, qq) bs[i] += ((((p1[a] * p2[b]) * p3[c]) * pr[n]) * pq[qq]) * w;
-      if constexpr (WANT == W_U) { MHS_Q_MONO_DG(MHS_QA) }
-      else { MHS_Q_MONO_DDG(MHS_QA) }
-#undef MHS_QA
-    }
+  for (int k = 0; k < K; ++k) {
     if constexpr (WANT == W_U) {
       double DG[27] = {};
-#define MHS_QT(r, mi, slot) DG[slot] += ic.q_dg[r] * bs[mi];
-      MHS_Q_TERMS_DG(MHS_QT)
-#undef MHS_QT
+      // two ranges of 34-35 of the 69 monomials
+      image_q_pass<P, WANT, 0, 73>(q, k, x0, x1, x2, e2, ic, DG, mun, lamn);
+      image_q_pass<P, WANT, 73, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, DG, mun, lamn);
       for (int i = 0; i < 27; ++i) DG[i] *= m.scale_c;
       contract_dg(DG, nrm, m, U + 9 * k);
     } else {
-      double DDG[81] = {};
-#define MHS_QT(r, mi, slot) DDG[slot] += ic.q_ddg[r] * bs[mi];
-      MHS_Q_TERMS_DDG(MHS_QT)
-#undef MHS_QT
-      for (int i = 0; i < 81; ++i) DDG[i] *= m.scale_c;
-      contract_ddg(DDG, nrm, m, H + 27 * k);
+      double Sf[27] = {};
+      // six ranges of 27-28 of the 167 monomials
+      image_q_pass<P, WANT, 0, 55>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      image_q_pass<P, WANT, 55, 107>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      image_q_pass<P, WANT, 107, 144>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      image_q_pass<P, WANT, 144, 180>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      image_q_pass<P, WANT, 180, 208>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      image_q_pass<P, WANT, 208, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      double S[3][3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int p = 0; p < 3; ++p)
+          for (int c = 0; c < 3; ++c) S[i][p][c] = Sf[9 * i + 3 * p + c] * m.scale_c;
+      hooke_from_traction(S, m, H + 27 * k);
     }
   }
 }

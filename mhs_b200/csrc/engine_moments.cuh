@@ -709,68 +709,4 @@ MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, double* Wout
 }
 
 
-// weight_far for two points at once against the same rule (constant slip,
-// P = 0): each rule node is loaded once for both, and the two sums are
-// independent chains.  Same arithmetic per point as weight_far.
-template <class S, class R, class Q = QuadRule>
-MHS_HD void weight_far2(const Q& q, double X0a, double X1a, double h2a, double X0b, double X1b,
-                        double h2b, double* Wa, double* Wb) {
-  constexpr Spec sp = S::spec;
-  constexpr int NW = sp.w_off[NS];
-  constexpr int DM = spec_max_need0(sp);
-  static_assert(sp.order == 0, "two-point far rule for constant slip only");
-  R acc[2][NW];
-#pragma unroll
-  for (int h = 0; h < 2; ++h)
-#pragma unroll
-    for (int i = 0; i < NW; ++i) acc[h][i] = R(0);
-  const R xa0 = R(X0a), xa1 = R(X1a), ha = R(h2a);
-  const R xb0 = R(X0b), xb1 = R(X1b), hb = R(h2b);
-#pragma unroll 2
-  for (int t = 0; t < q.nq; ++t) {
-    const R e0 = R(q.eta0[t]), e1 = R(q.eta1[t]), wq = R(q.wq[t]);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const R xi0 = e0 - (h ? xb0 : xa0), xi1 = e1 - (h ? xb1 : xa1);
-      const R R2 = xi0 * xi0 + xi1 * xi1 + (h ? hb : ha);
-      const R inv = rsqrt_r(R2);
-      const R inv2 = inv * inv;
-      R ws[NS];
-      {
-        R cur = wq * inv;
-#pragma unroll
-        for (int s = 1; s < NS; ++s) {
-          ws[s] = cur;
-          cur = cur * inv2;
-        }
-      }
-      R p0[DM + 1], p1[DM + 1];
-      p0[0] = R(1);
-      p1[0] = R(1);
-#pragma unroll
-      for (int i = 1; i <= DM; ++i) {
-        p0[i] = p0[i - 1] * xi0;
-        p1[i] = p1[i - 1] * xi1;
-      }
-#pragma unroll
-      for (int a = 0; a <= DM; ++a)
-#pragma unroll
-        for (int b = 0; a + b <= DM; ++b) {
-          const R mono = (a && b) ? p0[a] * p1[b] : a ? p0[a] : b ? p1[b] : R(1);
-#pragma unroll
-          for (int s = 0; s < NS; ++s) {
-            if (sp.need0[s] < a + b) continue;
-            const R v = (a || b) ? ws[s] * mono : ws[s];
-            acc[h][sp.w_off[s] + tri_idx(a, b)] += v;
-          }
-        }
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < NW; ++i) {
-    Wa[i] = double(acc[0][i]);
-    Wb[i] = double(acc[1][i]);
-  }
-}
-
 }  // namespace mhs

@@ -136,10 +136,7 @@ k_src(int j0, int nj, const int* __restrict__ st_src, const SrcPrep* __restrict_
     for (int c = 0; c < 3; ++c) d.slc.coef[c][threadIdx.x] = col[c];
   }
   if (threadIdx.x == NLIFT) surface_load_ezz(sp.f, sp.eps, m, d.slc);
-  if constexpr (std::is_same<RF, float>::value) {
-    __syncthreads();
-    float_rules<P>(d.rd, d.fr, threadIdx.x, blockDim.x);
-  }
+  if constexpr (std::is_same<RF, float>::value) build_float_rules<P>(sp.f, d.fr, threadIdx.x, blockDim.x);
 }
 
 // ------------------------------------------------------------- the plan
@@ -541,20 +538,21 @@ k_scatter(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls, int* __
   }
 }
 
-// Far loads: one thread per node of the far lists (two consecutive list
-// entries per thread at constant slip, sharing each rule node's loads when
-// they belong to the same source and rule).
+// Far loads: one thread per node of the far lists.  The FP64 form takes
+// mhs's rules (12 x 12; 8 x 8 for the far-8 class, beyond D_STAR_DISTANT L);
+// the mixed form takes its float MIXED_GAUSS_N_FAR rule for both classes (every
+// far node lies beyond D_STAR L).
 template <int P, int KC, class RF>
 __device__ __forceinline__ QuadRuleT<RF> far_rule(const Src<P, RF>& d, bool r8) {
-  constexpr int K = n_nodes(P), N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
-  constexpr int N8 = cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
-  const int off = r8 ? N12 : 0;
-  if constexpr (std::is_same<RF, float>::value)
-    return QuadRuleT<float>{r8 ? N8 : N12, d.fr.e0 + off, d.fr.e1 + off, d.fr.wq + off,
-                            d.fr.Nq + off * K};
-  else
+  if constexpr (std::is_same<RF, float>::value) {
+    return float_rule_far<P>(d.fr);
+  } else {
+    constexpr int K = n_nodes(P), N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
+    constexpr int N8 = cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
+    const int off = r8 ? N12 : 0;
     return QuadRuleT<double>{r8 ? N8 : N12, d.rd.e0 + off, d.rd.e1 + off, d.rd.wq + off,
                              d.rd.Nq + off * K};
+  }
 }
 
 template <int P, int KC, class RF>
@@ -564,68 +562,24 @@ k_far(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* 
       const int* __restrict__ pair_st, int j0, const int* __restrict__ st_src,
       const SrcPrep* __restrict__ prep, const Src<P, RF>* __restrict__ srcs,
       double* __restrict__ load, long long cap) {
-  using S = SurfaceSpec<P>;
-  constexpr Spec spc = S::spec;
-  constexpr int NW = spc.w_off[NS];
   constexpr int K = n_nodes(P);
   constexpr int NJ = 3 * K;
-  constexpr int STEP = 1;   // one node per thread (two-node blocking measured slower)
   const long long a = hdr->cls_off[CLS_FAR12], b = hdr->cls_off[CLS_FAR8 + 1];
   const long long r8_from = hdr->cls_off[CLS_FAR8];
-  for (long long e = a + STEP * ((long long)blockIdx.x * blockDim.x + threadIdx.x); e < b;
-       e += (long long)STEP * gridDim.x * blockDim.x) {
+  for (long long e = a + (long long)blockIdx.x * blockDim.x + threadIdx.x; e < b;
+       e += (long long)gridDim.x * blockDim.x) {
     const int u = nlist[e];
     const int j = pair_st[npair[u]];
     const SrcPrep& sp = prep[st_src[j]];
     const Src<P, RF>& d = srcs[j - j0];
-    const bool r8 = e >= r8_from;
     const double xx[3] = {npx[u], npy[u], 0.0};
     double z, X0, X1;
     to_plane(sp.f, xx, z, X0, X1);
     const double h2 = z * z + sp.eps * sp.eps;
-    if constexpr (STEP == 2) {
-      // the entry after this one, when it shares source and rule
-      int u2 = -1;
-      if (e + 1 < b && ((e + 1 >= r8_from) == r8)) {
-        const int v = nlist[e + 1];
-        if (pair_st[npair[v]] == j) u2 = v;
-      }
-      double sa[NJ] = {}, sb[NJ] = {};
-      if (u2 >= 0) {
-        const double xy[3] = {npx[u2], npy[u2], 0.0};
-        double z2, Y0, Y1;
-        to_plane(sp.f, xy, z2, Y0, Y1);
-        double Wa[NW], Wb[NW];
-        weight_far2<S, RF>(far_rule<P, KC, RF>(d, r8), X0, X1, h2, Y0, Y1,
-                           z2 * z2 + sp.eps * sp.eps, Wa, Wb);
-        surface_load_node<S>(d.slc, Wa, z, sa);
-        surface_load_node<S>(d.slc, Wb, z2, sb);
+    double sl[NJ] = {};
+    surface_load_far<P, RF>(far_rule<P, KC, RF>(d, e >= r8_from), d.slc, z, X0, X1, h2, sl);
 #pragma unroll
-        for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u2] = sb[jj];
-      } else {
-        surface_load_far<P, RF>(far_rule<P, KC, RF>(d, r8), d.slc, z, X0, X1, h2, sa);
-        if (e + 1 < b) {  // the next entry on its own
-          const int v = nlist[e + 1];
-          const int jv = pair_st[npair[v]];
-          const SrcPrep& spv = prep[st_src[jv]];
-          const Src<P, RF>& dv = srcs[jv - j0];
-          const double xy[3] = {npx[v], npy[v], 0.0};
-          double z2, Y0, Y1;
-          to_plane(spv.f, xy, z2, Y0, Y1);
-          surface_load_far<P, RF>(far_rule<P, KC, RF>(dv, e + 1 >= r8_from), dv.slc, z2, Y0, Y1,
-                                  z2 * z2 + spv.eps * spv.eps, sb);
-#pragma unroll
-          for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + v] = sb[jj];
-        }
-      }
-#pragma unroll
-      for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sa[jj];
-    } else {
-      double sl[NJ] = {};
-      surface_load_far<P, RF>(far_rule<P, KC, RF>(d, r8), d.slc, z, X0, X1, h2, sl);
-#pragma unroll
-      for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sl[jj];
-    }
+    for (int jj = 0; jj < NJ; ++jj) load[(size_t)jj * cap + u] = sl[jj];
   }
 }
 
@@ -941,7 +895,7 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
   // budgets of the variable part
   const size_t rest = region_bytes - off;
   const size_t b_src = rest / 10, b_pair = rest * 3 / 20, b_pan = rest * 3 / 20;
-  const size_t b_node = rest - b_src - b_pair - b_pan - 8 * 256;
+  const size_t b_node = rest - b_src - b_pair - b_pan - 24 * 256;   // 18 aligned carves below
   const long long cap_src = (long long)(b_src / Z::per_src);
   const long long cap_pair = (long long)(b_pair / Z::per_pair) - 2;
   const long long cap_pan = (long long)(b_pan / Z::per_panel) - 2;

@@ -58,33 +58,24 @@ struct SmemRules {
   __device__ QuadRule r8() const { return QuadRule{N8, e0 + N12, e1 + N12, wq + N12, Nq + N12 * K}; }
 };
 
-// Float copies of the element's far rules for the mixed form.
+// The mixed form's far rules, in float: MIXED_GAUSS_N x MIXED_GAUSS_N for
+// MIXED_NEAR_L L < D <= D_STAR L, MIXED_GAUSS_N_FAR x MIXED_GAUSS_N_FAR beyond.
 template <int P>
 struct FloatRules {
-  static constexpr int N = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N +
-                           cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT;
+  static constexpr int NM = MIXED_GAUSS_N * MIXED_GAUSS_N;
+  static constexpr int NF = MIXED_GAUSS_N_FAR * MIXED_GAUSS_N_FAR;
+  static constexpr int N = NM + NF;
   float e0[N], e1[N], wq[N], Nq[N * n_nodes(P)];
 };
 struct NoRules {};
 
-// Float copies of a block's rules (the mixed form), as QuadRuleT<float>.
-template <int P>
-__device__ void float_rules(const SmemRules<P>& rd, FloatRules<P>& fr, int tid, int nthr) {
-  constexpr int N = FloatRules<P>::N, K = n_nodes(P);
-  for (int t = tid; t < N; t += nthr) {
-    fr.e0[t] = (float)rd.e0[t];
-    fr.e1[t] = (float)rd.e1[t];
-    fr.wq[t] = (float)rd.wq[t];
-  }
-  for (int t = tid; t < N * K; t += nthr) fr.Nq[t] = (float)rd.Nq[t];
-}
-// Float rules built directly (nodes formed in double, then rounded).
+// Nodes formed in double, then rounded.
 template <int P>
 __device__ void build_float_rules(const Frame& f, FloatRules<P>& fr, int tid, int nthr) {
-  constexpr int N12 = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N, K = n_nodes(P);
+  constexpr int NM = FloatRules<P>::NM, K = n_nodes(P);
   for (int t = tid; t < FloatRules<P>::N; t += nthr) {
-    const int n = t < N12 ? cst::FAR_GAUSS_N : cst::FAR_GAUSS_N_DISTANT;
-    const int q = t < N12 ? t : t - N12;
+    const int n = t < NM ? MIXED_GAUSS_N : MIXED_GAUSS_N_FAR;
+    const int q = t < NM ? t : t - NM;
     double e0, e1, wq, Nq[K];
     rule_node<P>(f, n, q, e0, e1, wq, Nq);
     fr.e0[t] = (float)e0;
@@ -95,14 +86,14 @@ __device__ void build_float_rules(const Frame& f, FloatRules<P>& fr, int tid, in
 }
 
 template <int P>
-__device__ QuadRuleT<float> float_r12(const FloatRules<P>& fr) {
-  return QuadRuleT<float>{cst::FAR_GAUSS_N * cst::FAR_GAUSS_N, fr.e0, fr.e1, fr.wq, fr.Nq};
+__device__ QuadRuleT<float> float_rule_mid(const FloatRules<P>& fr) {
+  return QuadRuleT<float>{FloatRules<P>::NM, fr.e0, fr.e1, fr.wq, fr.Nq};
 }
 template <int P>
-__device__ QuadRuleT<float> float_r8(const FloatRules<P>& fr) {
-  constexpr int O = cst::FAR_GAUSS_N * cst::FAR_GAUSS_N;
-  return QuadRuleT<float>{cst::FAR_GAUSS_N_DISTANT * cst::FAR_GAUSS_N_DISTANT, fr.e0 + O, fr.e1 + O,
-                          fr.wq + O, fr.Nq + O * n_nodes(P)};
+__device__ QuadRuleT<float> float_rule_far(const FloatRules<P>& fr) {
+  constexpr int O = FloatRules<P>::NM;
+  return QuadRuleT<float>{FloatRules<P>::NF, fr.e0 + O, fr.e1 + O, fr.wq + O,
+                          fr.Nq + O * n_nodes(P)};
 }
 
 // ---------------------------------------------------------------- k_coef
@@ -233,7 +224,8 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
   double* row = T + ((oc * n_src + s) * K) * NR;
   if constexpr (KC == KD_E) {
     double E[K] = {};
-    if constexpr (F32) direct_eval<P, W_E, RF>(sp.f, float_r12<P>(rdf), float_r8<P>(rdf), x, eps, m, nullptr, nullptr, E, near_l);
+    if constexpr (F32) direct_eval<P, W_E, RF>(sp.f, float_rule_mid<P>(rdf), float_rule_far<P>(rdf), x, eps, m,
+                                          nullptr, nullptr, E, near_l, cst::D_STAR);
     else direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
     for (int k = 0; k < K; ++k) {
       row[k * NR + 0] = E[k];
@@ -244,11 +236,12 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
     constexpr int C = comps_of(KC);
     double A[K * C] = {}, E[K] = {};
     if constexpr (F32) {
-      const QuadRuleT<float> f12 = float_r12<P>(rdf), f8 = float_r8<P>(rdf);
+      const QuadRuleT<float> f12 = float_rule_mid<P>(rdf), f8 = float_rule_far<P>(rdf);
       if constexpr (KC == KD_DISP)
-        direct_eval<P, W_U, RF>(sp.f, f12, f8, x, eps, m, A, nullptr, nullptr, near_l);
+        direct_eval<P, W_U, RF>(sp.f, f12, f8, x, eps, m, A, nullptr, nullptr, near_l, cst::D_STAR);
       else
-        direct_eval<P, W_H | W_E, RF>(sp.f, f12, f8, x, eps, m, nullptr, A, E, near_l);
+        direct_eval<P, W_H | W_E, RF>(sp.f, f12, f8, x, eps, m, nullptr, A, E, near_l,
+                                      cst::D_STAR);
     } else {
       if constexpr (KC == KD_DISP)
         direct_eval<P, W_U, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, A, nullptr, nullptr);
@@ -260,11 +253,13 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
       double B[K * C] = {};
       const ImageCoef ic = image_coef_view(coef);
       if constexpr (F32) {
-        const QuadRuleT<float> i12 = float_r12<P>(rif), i8 = float_r8<P>(rif);
+        const QuadRuleT<float> i12 = float_rule_mid<P>(rif), i8 = float_rule_far<P>(rif);
         if constexpr (KC == KD_DISP)
-          image_r_eval<P, W_U, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, B, nullptr, near_l);
+          image_r_eval<P, W_U, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, B, nullptr, near_l,
+                                      cst::D_STAR);
         else
-          image_r_eval<P, W_H, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, nullptr, B, near_l);
+          image_r_eval<P, W_H, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, nullptr, B, near_l,
+                                      cst::D_STAR);
       } else {
         if constexpr (KC == KD_DISP)
           image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
@@ -319,10 +314,13 @@ struct QRuleFly {
   }
 };
 
+#ifndef MHS_IMAGEQ_MINB
+#define MHS_IMAGEQ_MINB 1
+#endif
 // RF = float (the mixed form): pairs at the floor order -- at least about an
 // element from the image triangle -- sum their points in float.
 template <int P, int KC, class RF>
-__global__ void __launch_bounds__(TB)
+__global__ void __launch_bounds__(TB, MHS_IMAGEQ_MINB)
 k_imageq(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq) {
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);

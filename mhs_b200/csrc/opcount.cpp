@@ -1,4 +1,5 @@
-// Algorithmic operation counts of the fold's work units, for the roofline.
+// Algorithmic operation counts of the fold's work units and of one ordinary
+// pair's direct and image terms, for the roofline.
 //
 // The engine headers are compiled here with `double` replaced by CountD, a
 // scalar that performs the same IEEE arithmetic and counts every operation:
@@ -317,6 +318,111 @@ int oc_pair(int P, int want_h, const double* tri, double eps, double mu, double 
   if (nb > 1) fold_panel_rule(fp, br[0], br[1], A);
   take(panel_ops);
   return nb;
+}
+
+}  // extern "C"
+
+namespace {
+// The per-material coefficient block in ImageCoef's layout (values only:
+// built before the counted evaluation).
+constexpr int OC_COEF_SIZE = 3 * (MHS_R_NDG + MHS_R_NDDG) + MHS_Q_NDG + MHS_Q_NDDG;
+void oc_image_coef(const Material& m, CountD* out) {
+  const CountD nup[3] = {1.0, m.nu_i, m.nu_i * m.nu_i};
+  CountD* p = out;
+  for (int r = 0; r < MHS_R_NDG; ++r)
+    for (int pz = 0; pz < 3; ++pz) {
+      CountD v = 0.0;
+      for (int k = 0; k < 3; ++k) v += tab_h::mhs_r_dg_c[r][pz][k] * nup[k];
+      *p++ = v * m.scale_c;
+    }
+  for (int r = 0; r < MHS_R_NDDG; ++r)
+    for (int pz = 0; pz < 3; ++pz) {
+      CountD v = 0.0;
+      for (int k = 0; k < 3; ++k) v += tab_h::mhs_r_ddg_c[r][pz][k] * nup[k];
+      *p++ = v * m.scale_c;
+    }
+  for (int r = 0; r < MHS_Q_NDG; ++r) {
+    CountD v = 0.0;
+    for (int k = 0; k < 3; ++k) v += tab_h::mhs_q_dg_c[r][k] * nup[k];
+    *p++ = v;
+  }
+  for (int r = 0; r < MHS_Q_NDDG; ++r) {
+    CountD v = 0.0;
+    for (int k = 0; k < 3; ++k) v += tab_h::mhs_q_ddg_c[r][k] * nup[k];
+    *p++ = v;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+// One ordinary (observer, source) pair as the pair kernels evaluate it:
+// the direct term (closed form within D_STAR L, else the 12 x 12 rule, 8 x 8
+// beyond D_STAR_DISTANT L), the image R-family on the reflected element and
+// the image Q-family at the pair's Gauss order (nodes precomputed, as the
+// device holds the floor order's per source).  *band = 1 when the receiver
+// lies in the fold band of a straddling source: the image terms are then
+// replaced by the fold and are not evaluated (their counts are zero).
+int oc_pair_terms(int P, int want_h, const double* tri, double eps, double mu, double lam,
+                  const double* x, long long* direct_ops, long long* image_r_ops,
+                  long long* image_q_ops, int* q_order, int* band) {
+  ensure_gl();
+  CountD tt[9], ti[9], xx[3] = {x[0], x[1], x[2]};
+  for (int i = 0; i < 9; ++i) {
+    tt[i] = tri[i];
+    ti[i] = (i % 3 == 2) ? -tri[i] : tri[i];
+  }
+  Frame f, fi;
+  make_frame(tt, f);
+  make_frame(ti, fi);
+  const Material m = make_material(CountD(mu), CountD(lam));
+  CountD centre[2], r_f;
+  fold_crease(tt, CountD(eps), centre, &r_f);
+  const bool in_band = fold_straddles(tt, CountD(eps)) && fold_band(xx, centre, CountD(eps));
+  *band = in_band ? 1 : 0;
+  long long scratch[4];
+#define OC_TERMS(PP)                                                                         \
+  {                                                                                          \
+    constexpr int K = n_nodes(PP);                                                           \
+    static Rules<PP> rd, ri;                                                                 \
+    rd.build(f);                                                                             \
+    ri.build(fi);                                                                            \
+    static CountD G[G_SIZE], coef[OC_COEF_SIZE];                                          \
+    build_basis_products(fi, G);                                                             \
+    oc_image_coef(m, coef);                                                                  \
+    const ImageCoef ic = image_coef_view(coef);                                              \
+    take(scratch);                                                                           \
+    CountD A[27 * 6], E[6];                                                                  \
+    if (want_h) direct_eval<PP, W_H | W_E>(f, rd.r12, rd.r8, xx, CountD(eps), m, nullptr, A, E); \
+    else direct_eval<PP, W_U>(f, rd.r12, rd.r8, xx, CountD(eps), m, A, nullptr, nullptr);    \
+    take(direct_ops);                                                                        \
+    for (int i = 0; i < 4; ++i) image_r_ops[i] = image_q_ops[i] = 0;                         \
+    *q_order = 0;                                                                            \
+    if (!in_band) {                                                                          \
+      CountD B[27 * 6];                                                                      \
+      if (want_h) image_r_eval<PP, W_H>(fi, G, f.n, ri.r12, ri.r8, xx, CountD(eps), m, ic,   \
+                                        nullptr, B);                                         \
+      else image_r_eval<PP, W_U>(fi, G, f.n, ri.r12, ri.r8, xx, CountD(eps), m, ic, B,       \
+                                 nullptr);                                                   \
+      take(image_r_ops);                                                                     \
+      CountD tv[9];                                                                          \
+      for (int a = 0; a < 3; ++a)                                                            \
+        for (int b = 0; b < 3; ++b) tv[3 * a + b] = fi.v[a][b];                              \
+      const int n = q_gauss_order(xx, tv, CountD(eps), f.L, PP);                             \
+      *q_order = n;                                                                          \
+      static CountD qy[3 * GL_MAX * GL_MAX], qw[6 * GL_MAX * GL_MAX];                        \
+      build_qrule<PP>(f, g_glx, g_glw, n, qy, qw);                                           \
+      const QRule<PP> q{n * n, qy, qw};                                                      \
+      take(scratch);                                                                         \
+      if (want_h) image_q_eval<PP, W_H>(q, f.n, xx, CountD(eps), m, ic, nullptr, B);         \
+      else image_q_eval<PP, W_U>(q, f.n, xx, CountD(eps), m, ic, B, nullptr);                \
+      take(image_q_ops);                                                                     \
+      (void)K;                                                                               \
+    }                                                                                        \
+  }
+  if (P == 0) OC_TERMS(0) else if (P == 1) OC_TERMS(1) else OC_TERMS(2)
+#undef OC_TERMS
+  return 0;
 }
 
 }  // extern "C"

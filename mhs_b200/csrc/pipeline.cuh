@@ -47,10 +47,18 @@ struct SrcPrep {
 };
 
 constexpr int TB = 128;          // threads per block for pair-parallel kernels
-// The mixed form takes the closed-form near field only within this many
-// element lengths (sqrt(|x - c|^2 + eps^2) <= MIXED_NEAR_L * L) and the float
-// 12 x 12 rule beyond, out to D_STAR; the FP64 form uses D_STAR throughout.
+// The mixed form's far field: the pair kernel takes the closed-form near
+// field only within MIXED_NEAR_L element lengths (sqrt(|x - c|^2 + eps^2)
+// <= MIXED_NEAR_L * L), a float MIXED_GAUSS_N x MIXED_GAUSS_N product rule
+// out to D_STAR L and a float MIXED_GAUSS_N_FAR x MIXED_GAUSS_N_FAR rule
+// beyond (the fold's far surface loads, all beyond D_STAR L, take the
+// latter).  At those distances these orders already resolve the kernels:
+// at P2 the 8 x 8 rule at 3 L and the 6 x 6 rule at 10 L agree with a
+// 40 x 40 rule to 2e-13 of the largest entry, far below float rounding.
+// The FP64 form keeps mhs's rules (12 x 12, 8 x 8 beyond D_STAR_DISTANT L).
 constexpr double MIXED_NEAR_L = 3.0;
+constexpr int MIXED_GAUSS_N = 8;
+constexpr int MIXED_GAUSS_N_FAR = 6;
 constexpr int QFLOOR = cst::IMAGE_Q_GAUSS_MIN;
 
 enum : int { KD_DISP = 0, KD_HE = 1, KD_E = 2 };   // what the stages compute

@@ -1,4 +1,5 @@
-"""Algorithmic flops of the fold stage, for the roofline.
+"""Algorithmic flops of the fold stage and of the pair kernels, for the
+roofline.
 
 Two measurements multiply:
 
@@ -16,6 +17,11 @@ Two measurements multiply:
 The per-unit counts are taken on representative inputs of each unit; every
 unit except the per-pair breakpoint sort is branch-free straight-line
 arithmetic in its form, so the counts do not depend on the inputs.
+
+The pair kernels' work depends on each pair's geometry (closed form or
+quadrature, edge forms, the image Q order), so ``pair_flops`` counts a
+seeded uniform sample of (observer, source) pairs exactly and scales the
+sample mean to all pairs.
 """
 from __future__ import annotations
 
@@ -129,3 +135,44 @@ def fold_flops(census: dict, order: int, want_h: bool, **kw) -> dict:
     tot["per_unit"] = u
     tot["nodes"] = nodes
     return tot
+
+
+def pair_flops(obs, tris, eps, mu: float, lam: float, order: int, want_h: bool,
+               samples: int = 4096, seed: int = 0) -> dict:
+    """Algorithmic flops of the pair kernels over all (observer, source)
+    pairs, from a seeded uniform sample counted exactly: the direct term
+    (``k_pair``, every pair), the image R-family (``k_pair``, pairs outside
+    a fold band) and the image Q-family (``k_imageq``, likewise).  Returns
+    totals per kernel and the sample's share of fold-band pairs."""
+    lib = _load()
+    obs = np.ascontiguousarray(obs, dtype=np.float64)
+    tris = np.ascontiguousarray(tris, dtype=np.float64)
+    eps = np.broadcast_to(np.asarray(eps, dtype=np.float64), (tris.shape[0],))
+    n_obs, n_src = obs.shape[0], tris.shape[0]
+    rng = np.random.default_rng(seed)
+    oi = rng.integers(0, n_obs, samples)
+    si = rng.integers(0, n_src, samples)
+    keys = ("flop", "div", "sqrt", "special")
+    acc = {k: {q: 0 for q in keys} for k in ("direct", "image_r", "image_q")}
+    n_band = 0
+    qo = ctypes.c_int()
+    band = ctypes.c_int()
+    for o, s_ in zip(oi, si):
+        t = np.ascontiguousarray(tris[s_])
+        x = np.ascontiguousarray(obs[o])
+        od, orr, oq = _ops(), _ops(), _ops()
+        lib.oc_pair_terms(order, 1 if want_h else 0, t.ctypes.data_as(ctypes.c_void_p),
+                          _D(float(eps[s_])), _D(mu), _D(lam), x.ctypes.data_as(ctypes.c_void_p),
+                          od, orr, oq, ctypes.byref(qo), ctypes.byref(band))
+        n_band += band.value
+        for name, o_ in (("direct", od), ("image_r", orr), ("image_q", oq)):
+            for i, q in enumerate(keys):
+                acc[name][q] += int(o_[i])
+    scale = n_obs * n_src / samples
+    out = {name: {q: v * scale for q, v in d.items()} for name, d in acc.items()}
+    out["k_pair"] = {q: out["direct"][q] + out["image_r"][q] for q in keys}
+    out["k_imageq"] = out["image_q"]
+    out["samples"] = samples
+    out["band_share"] = n_band / samples
+    return out
+

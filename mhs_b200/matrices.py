@@ -309,7 +309,8 @@ class Pending:
         if bits.value & _native.DEV_FOLD_GRID_OVERFLOW:
             raise RuntimeError("a fold polar grid exceeded its capacity (FOLD_MAX_BREAKS); "
                                "the source is far larger than its eps")
-        return self.out
+        out, self.out = self.out, None      # the caller's reference is the only one
+        return out
 
 
 def _launch(kind, obs, tri, mu, lam, eps_arr, p, ids, n_dof, out_shape, out, fold,

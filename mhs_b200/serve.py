@@ -18,8 +18,14 @@ admitted, not when the current group ends).  Every request computes exactly
 what a direct call computes -- the kernels are deterministic and requests
 share no scratch -- so a result is the same alone and in the mix.
 
-A request larger than the whole budget is refused with MemoryError, the
-way mhs refuses a matrix above its byte ceiling.  ``stats()`` returns the
+A result keeps counting against the budget, with its output bytes, until
+the caller drops the last reference to it (the device memory is in use
+until then), so a client that holds results slows admission instead of
+running the device out of memory.  When nothing is in flight and only held
+results keep the next request out, it is admitted if the device's free
+memory holds it, and otherwise fails with MemoryError (the caller's results
+fill the device).  A request larger than the whole budget is refused with
+MemoryError, the way mhs refuses a matrix above its byte ceiling.  ``stats()`` returns the
 latency percentiles (submit to result ready, host clock) and throughput.
 """
 from __future__ import annotations
@@ -27,6 +33,7 @@ from __future__ import annotations
 import collections
 import threading
 import time
+import weakref
 from concurrent.futures import Future
 
 from . import matrices
@@ -56,13 +63,14 @@ class Server:
         self.queue = collections.deque()
         self.in_flight = []          # (pending, future, stream index, event, t_submit)
         self.in_flight_bytes = 0
-        self.peak_bytes = 0          # most device bytes ever admitted at once
+        self.held_bytes = 0          # outputs handed out and still referenced
+        self.peak_bytes = 0          # most device bytes ever in flight at once
         self.peak_in_flight = 0      # most requests ever in flight at once
         self.lat = []
         self.entries = 0
         self.t_first = None
         self.t_last = None
-        self.cv = threading.Condition()
+        self.cv = threading.Condition(threading.RLock())
         self.running = True
         self.error = None
         self.thread = threading.Thread(target=self._loop, name="mhs-serve", daemon=True)
@@ -127,6 +135,17 @@ class Server:
                 "entries_per_s": (self.entries / span) if span else None,
                 "req_per_s": (n / span) if span else None}
 
+    def _device_room(self) -> int:
+        torch = self.torch
+        free, _ = torch.cuda.mem_get_info(self.device)
+        return int(free + torch.cuda.memory_reserved(self.device)
+                   - torch.cuda.memory_allocated(self.device))
+
+    def _release(self, nbytes: int) -> None:
+        with self.cv:
+            self.held_bytes -= nbytes
+            self.cv.notify_all()
+
     # -------------------------------------------------------- dispatcher
     def _loop(self):
         torch = self.torch
@@ -139,8 +158,20 @@ class Server:
                 while self.queue and self.free_streams:
                     pend, fut, t0 = self.queue[0]
                     need = pend.device_bytes
-                    if not admissible(need, self.in_flight_bytes, len(self.in_flight) + len(admit),
-                                      self.budget, self.slots):
+                    n_now = len(self.in_flight) + len(admit)
+                    ok = admissible(need, self.in_flight_bytes + self.held_bytes, n_now,
+                                    self.budget, self.slots)
+                    if not ok and n_now == 0 and self.held_bytes > 0:
+                        # only results the caller still holds keep it out
+                        ok = need <= self._device_room()
+                        if not ok:
+                            self.queue.popleft()
+                            fut.set_exception(MemoryError(
+                                f"request needs {need / 2**30:.2f} GiB on the device; results "
+                                f"still held by the caller ({self.held_bytes / 2**30:.2f} GiB) "
+                                f"leave no room"))
+                            continue
+                    if not ok:
                         break
                     self.queue.popleft()
                     self.in_flight_bytes += need
@@ -178,6 +209,9 @@ class Server:
                         res.record_stream(pend.consumer)
                     t1 = time.perf_counter()
                     with self.cv:
+                        if res is not None:
+                            self.held_bytes += pend.out_bytes
+                            weakref.finalize(res, self._release, pend.out_bytes)
                         self.lat.append(t1 - t0)
                         self.entries += pend.entries
                         self.t_last = t1
@@ -188,6 +222,10 @@ class Server:
                     self.in_flight_bytes -= need
                     self.free_streams.append(si)
                     self.cv.notify_all()
-            if not admit and not done:
+            idle = not admit and not done
+            # drop this pass's references, so that a result lives only as long
+            # as the caller keeps it
+            admit = done = item = pend = fut = res = None
+            if idle:
                 with self.cv:
                     self.cv.wait(self.poll_s)

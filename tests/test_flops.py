@@ -51,3 +51,33 @@ def test_fold_flops_combines_a_census():
         + 300 * u["edge_large"]["flop"] + 1500 * u["node"]["flop"] + 2 * u["pair"]["flop"] \
         + 40 * u["panel"]["flop"]
     assert tot["flop"] == expect
+
+
+def test_pair_terms_counts():
+    """The pair kernels' counts: every pair runs the direct term; a pair in a
+    fold band runs no image term; a far pair's direct term takes the 12 x 12
+    rule (a fixed count), and the image Q-family costs in proportion to its
+    order's points."""
+    import ctypes
+    import numpy as np
+    from mhs_b200 import flops
+    lib = flops._load()
+    tri = np.ascontiguousarray([[0.0, 0.0, -0.02], [1.0, 0.0, -0.6], [0.0, 1.0, -0.4]])
+
+    def terms(x):
+        od, orr, oq = flops._ops(), flops._ops(), flops._ops()
+        qo, band = ctypes.c_int(), ctypes.c_int()
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        lib.oc_pair_terms(0, 1, tri.ctypes.data_as(ctypes.c_void_p), flops._D(0.05),
+                          flops._D(30.0), flops._D(30.0), x.ctypes.data_as(ctypes.c_void_p),
+                          od, orr, oq, ctypes.byref(qo), ctypes.byref(band))
+        return flops._as(od), flops._as(orr), flops._as(oq), qo.value, band.value
+
+    d, r, q, n, band = terms([0.3, 0.3, -0.01])          # in the band of a straddler
+    assert band == 1 and d["flop"] > 0 and r["flop"] == 0 and q["flop"] == 0
+    far_a = terms([25.0, 3.0, -4.0])
+    far_b = terms([-20.0, 14.0, -9.0])
+    assert far_a[4] == 0 and far_a[0]["flop"] == far_b[0]["flop"] > 0
+    assert far_a[3] == far_b[3] == 8 and far_a[2]["flop"] == far_b[2]["flop"]
+    near = terms([0.4, 0.2, -0.8])
+    assert near[4] == 0 and near[3] > 8 and near[2]["flop"] > far_a[2]["flop"] * (near[3] / 8) ** 2 * 0.9

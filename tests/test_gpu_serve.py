@@ -77,3 +77,35 @@ def test_byte_budget_admission_and_refusal(cuda):
     with serve.Server(cuda, budget_bytes=sizes[big] - 1, slots=2) as srv:
         with pytest.raises(MemoryError, match="serving budget"):
             srv.submit(reqs[big][0], *reqs[big][1], **reqs[big][2])
+
+
+def test_held_results_count_until_dropped(cuda):
+    import torch
+    from mhs_b200 import matrices, serve
+    reqs = _requests(torch, cuda)[:3]
+    with matrices.deferred():
+        outs = [fn(*a, **k).out_bytes for fn, a, k in reqs]
+    with serve.Server(cuda, slots=4) as srv:
+        r0 = srv.submit(reqs[0][0], *reqs[0][1], **reqs[0][2]).result(timeout=300)
+        srv.drain()
+        assert srv.held_bytes == outs[0]
+        futs = [srv.submit(fn, *a, **k) for fn, a, k in reqs[1:]]
+        res = [f.result(timeout=300) for f in futs]
+        srv.drain()
+        assert srv.held_bytes == sum(outs)
+        del futs, res
+        assert _settles(srv, outs[0])
+        del r0
+        assert _settles(srv, 0)
+
+
+def _settles(srv, want, seconds=5.0):
+    import gc
+    import time
+    t = time.perf_counter()
+    while time.perf_counter() - t < seconds:
+        gc.collect()
+        if srv.held_bytes == want:
+            return True
+        time.sleep(0.01)
+    return False
