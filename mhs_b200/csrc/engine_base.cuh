@@ -79,6 +79,17 @@ constexpr double PI = 3.141592653589793;
 }  // namespace cst
 
 // Largest Gauss-Legendre order any rule asks for (the Q-family ceiling).
+// The array behind p stays in (local) memory: once its address has passed
+// through an opaque move the compiler can no longer promote the array to
+// registers.  For per-thread arrays too large to live in registers.
+template <class T>
+MHS_FI T* in_memory(T* p) {
+#if defined(__CUDA_ARCH__)
+  asm volatile("mov.b64 %0, %0;" : "+l"(p));
+#endif
+  return p;
+}
+
 constexpr int GL_MAX = cst::IMAGE_Q_GAUSS_MAX;
 // Offset of order n's nodes in the packed 1-D rule table (orders 1..GL_MAX).
 MHS_FI constexpr int gl_offset(int n) { return (n - 1) * n / 2; }

@@ -9,6 +9,7 @@
 
 #include "engine_moments.cuh"
 #include "tables_q.inc"
+#include "tables_r.inc"
 
 namespace mhs {
 
@@ -234,7 +235,8 @@ MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
     }
   } else {
     const Q& q = (D > far_switch_l * f.L) ? r8 : r12;
-    double W[K * NW] = {};
+    double Wbuf[K * NW] = {};
+    double* W = P > 0 ? in_memory(Wbuf) : Wbuf;   // K * NW doubles at P >= 1
     weight_far<S, P, R_FAR>(q, X0, X1, h2, W);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -325,8 +327,6 @@ MHS_HD void contract_dg(const double* DG, const double* nrm, const Material& m, 
   }
 }
 
-// DDG (i, j, p, m) -> displacement gradient -> symmetric Hooke stress
-// (mhs/kernels/image.py:138-161).
 // H from the traction-operator image S[i][p][k] of DDG: the symmetric part
 // in (i, p) through Hooke's law, per slip component k.
 MHS_HD void hooke_from_traction(const double (&S)[3][3][3], const Material& m, double* H) {
@@ -344,6 +344,8 @@ MHS_HD void hooke_from_traction(const double (&S)[3][3][3], const Material& m, d
   }
 }
 
+// DDG (i, j, p, m) -> displacement gradient -> symmetric Hooke stress
+// (mhs/kernels/image.py:138-161).
 MHS_HD void contract_ddg(const double* DDG, const double* nrm, const Material& m, double* H) {
   double S[3][3][3];
   for (int i = 0; i < 3; ++i)
@@ -363,6 +365,90 @@ MHS_HD void contract_ddg(const double* DDG, const double* nrm, const Material& m
 }
 
 // --------------------------------------------------------- image R-family
+// Cartesian monomial moment mi, D1^a D2^b D3^c / R2^n, of one node from the
+// basis products G and the weighted table W (mhs/kernels/image.py:456-480):
+// sum over t of (-1)^t zp^(r - t) sum_al G[al, t - al] W_n[al, t - al].
+template <class S>
+MHS_FI double r_moment(int mi, const double* G, const double* W, const double* zpow) {
+  constexpr Spec sp = S::spec;
+  const int a = MHS_TAB(mhs_r_mono)[mi][0], b = MHS_TAB(mhs_r_mono)[mi][1],
+            c = MHS_TAB(mhs_r_mono)[mi][2], n = MHS_TAB(mhs_r_mono)[mi][3];
+  const int r = a + b + c;
+  const double* g = G + g_off(a, b, c);
+  const double* Wn = W + sp.w_off[nslot(n)];
+  double acc = 0.0;
+  for (int t = 0; t <= r; ++t) {
+    double part = 0.0;
+    for (int al = 0; al <= t; ++al) part += g[tri_idx(al, t - al)] * Wn[tri_idx(al, t - al)];
+    const double v = zpow[r - t] * part;
+    acc += (t & 1) ? -v : v;
+  }
+  return acc;
+}
+
+// The records of one node: the monomial moments in monomial order, each
+// followed by its own records (sorted by monomial, so every slot receives
+// its records in table order) with coefficient c(z) = c0 + z (c1 + z c2) at
+// the observer's depth.  The displacement readout accumulates DG (27
+// slots); the stress readout contracts each DDG record straight into the
+// traction-operator image S[i][p][k] (27 entries, as 9 i + 3 p + k): record
+// slot (i, a, p, b) adds mun[b] v to S[i][p][a], mun[a] v to S[i][p][b] and,
+// when a = b, lamn[k] v to every S[i][p][k] (mun = mu n, lamn = lam n; the
+// scale is already in the coefficients).  The monomial loop runs at run
+// time and dispatches to one case per monomial whose records are straight-
+// line code with literal slots, so only the moment and the 27 accumulators
+// are live and nothing is addressed at run time but the tables.
+template <class S, int WANT, int MI>
+MHS_FI void r_mono_records(double tm, double zo, const ImageCoef& ic, double* D,
+                           const double* mun, const double* lamn) {
+  if constexpr (WANT == W_U) {
+#define MHS_RTU(r, mi, slot)                                           \
+  if constexpr ((mi) == MI) {                                          \
+    const double* cz = ic.r_dg + 3 * (r);                              \
+    D[slot] += (cz[0] + zo * (cz[1] + zo * cz[2])) * tm;               \
+  }
+    MHS_R_TERMS_DG(MHS_RTU)
+#undef MHS_RTU
+  } else {
+#define MHS_RTD(r, mi, slot)                                                        \
+  if constexpr ((mi) == MI) {                                                       \
+    const double* cz = ic.r_ddg + 3 * (r);                                          \
+    const double v = (cz[0] + zo * (cz[1] + zo * cz[2])) * tm;                      \
+    constexpr int qi = (slot) / 27, qa = ((slot) / 9) % 3, qp = ((slot) / 3) % 3;  \
+    constexpr int qb = (slot) % 3;                                                  \
+    D[9 * qi + 3 * qp + qa] += mun[qb] * v;                                         \
+    D[9 * qi + 3 * qp + qb] += mun[qa] * v;                                         \
+    if constexpr (qa == qb) {                                                       \
+      D[9 * qi + 3 * qp + 0] += lamn[0] * v;                                        \
+      D[9 * qi + 3 * qp + 1] += lamn[1] * v;                                        \
+      D[9 * qi + 3 * qp + 2] += lamn[2] * v;                                        \
+    }                                                                               \
+  }
+    MHS_R_TERMS_DDG(MHS_RTD)
+#undef MHS_RTD
+  }
+}
+
+template <class S, int WANT>
+MHS_FI void image_r_records(const double* G, const double* W, const double* zpow, double zo,
+                            const ImageCoef& ic, double* D, const double* mun,
+                            const double* lamn) {
+#pragma unroll 1
+  for (int mi = 0; mi < MHS_R_NMONO; ++mi) {
+    const double tm = r_moment<S>(mi, G, W, zpow);
+    switch (mi) {
+#define MHS_RCASE(mi_, a, b, c, n)                                  \
+  case mi_:                                                         \
+    r_mono_records<S, WANT, mi_>(tm, zo, ic, D, mun, lamn);         \
+    break;
+      MHS_R_MONO(MHS_RCASE)
+#undef MHS_RCASE
+      default:
+        break;
+    }
+  }
+}
+
 // The closed-form R-family on the reflected element (mhs/kernels/image.py:
 // 435-497): weighted tables of the image frame, Cartesian monomial moments
 // D1^a D2^b D3^c / R2^n from the basis products G, then the generated records.
@@ -385,7 +471,8 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
   double zpow[G_RMAX + 1];
   zpow[0] = 1.0;
   for (int i = 1; i <= G_RMAX; ++i) zpow[i] = zpow[i - 1] * zp;
-  double Wall[K * NW] = {};
+  double Wbuf[K * NW] = {};
+  double* Wall = P > 0 ? in_memory(Wbuf) : Wbuf;   // K * NW doubles at P >= 1
   if (D <= cst::D_STAR * fi.L && D <= near_l * fi.L) {
     MomentTable<S> T;
     closed_moments<S>(fi, X0, X1, h2, T);
@@ -396,48 +483,24 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
     const Q& q = (D > far_switch_l * fi.L) ? r8 : r12;
     weight_far<S, P, R_FAR>(q, X0, X1, h2, Wall);
   }
+  const double mun[3] = {m.mu * nrm[0], m.mu * nrm[1], m.mu * nrm[2]};
+  const double lamn[3] = {m.lam * nrm[0], m.lam * nrm[1], m.lam * nrm[2]};
 #pragma unroll 1
   for (int k = 0; k < K; ++k) {
     const double* W = Wall + k * NW;
-    // Cartesian monomial moments
-    double Tm[MHS_R_NMONO];
-#pragma unroll 1
-    for (int mi = 0; mi < MHS_R_NMONO; ++mi) {
-      const int a = MHS_TAB(mhs_r_mono)[mi][0], b = MHS_TAB(mhs_r_mono)[mi][1],
-                c = MHS_TAB(mhs_r_mono)[mi][2], n = MHS_TAB(mhs_r_mono)[mi][3];
-      const int r = a + b + c, s = nslot(n);
-      const double* g = G + g_off(a, b, c);
-      const double* Wn = W + sp.w_off[s];
-      double acc = 0.0;
-      for (int t = 0; t <= r; ++t) {
-        double part = 0.0;
-        for (int al = 0; al <= t; ++al) part += g[tri_idx(al, t - al)] * Wn[tri_idx(al, t - al)];
-        const double v = zpow[r - t] * part;
-        acc += (t & 1) ? -v : v;
-      }
-      Tm[mi] = acc;
-    }
-    if (WANT & W_U) {
-      double DG[27];
-      for (int i = 0; i < 27; ++i) DG[i] = 0.0;
-#pragma unroll 1
-      for (int r = 0; r < MHS_R_NDG; ++r) {
-        const int mi = MHS_TAB(mhs_r_dg_idx)[r][0], slot = MHS_TAB(mhs_r_dg_idx)[r][1];
-        const double* cz = ic.r_dg + 3 * r;
-        DG[slot] += (cz[0] + zo * (cz[1] + zo * cz[2])) * Tm[mi];
-      }
+    if constexpr ((WANT & W_U) != 0) {
+      double DG[27] = {};
+      image_r_records<S, W_U>(G, W, zpow, zo, ic, DG, mun, lamn);
       contract_dg(DG, nrm, m, U + 9 * k);
     }
-    if (WANT & W_H) {
-      double DDG[81];
-      for (int i = 0; i < 81; ++i) DDG[i] = 0.0;
-#pragma unroll 1
-      for (int r = 0; r < MHS_R_NDDG; ++r) {
-        const int mi = MHS_TAB(mhs_r_ddg_idx)[r][0], slot = MHS_TAB(mhs_r_ddg_idx)[r][1];
-        const double* cz = ic.r_ddg + 3 * r;
-        DDG[slot] += (cz[0] + zo * (cz[1] + zo * cz[2])) * Tm[mi];
-      }
-      contract_ddg(DDG, nrm, m, H + 27 * k);
+    if constexpr ((WANT & W_H) != 0) {
+      double Sf[27] = {};
+      image_r_records<S, W_H>(G, W, zpow, zo, ic, Sf, mun, lamn);
+      double St[3][3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int p = 0; p < 3; ++p)
+          for (int c = 0; c < 3; ++c) St[i][p][c] = Sf[9 * i + 3 * p + c];
+      hooke_from_traction(St, m, H + 27 * k);
     }
   }
 }
@@ -629,22 +692,34 @@ MHS_HD void image_q_eval(const Rule& q, const double* nrm, const double* x, doub
   const double lamn[3] = {m.lam * nrm[0], m.lam * nrm[1], m.lam * nrm[2]};
 #pragma unroll 1
   for (int k = 0; k < K; ++k) {
+    // float sums take half the registers: fewer, wider passes
+    constexpr bool F32 = std::is_same<R, float>::value;
     if constexpr (WANT == W_U) {
       double DG[27] = {};
-      // two ranges of 34-35 of the 69 monomials
-      image_q_pass<P, WANT, 0, 73>(q, k, x0, x1, x2, e2, ic, DG, mun, lamn);
-      image_q_pass<P, WANT, 73, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, DG, mun, lamn);
+      if constexpr (F32) {
+        image_q_pass<P, WANT, 0, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, DG, mun, lamn);
+      } else {
+        // two ranges of 34-35 of the 69 monomials
+        image_q_pass<P, WANT, 0, 73>(q, k, x0, x1, x2, e2, ic, DG, mun, lamn);
+        image_q_pass<P, WANT, 73, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, DG, mun, lamn);
+      }
       for (int i = 0; i < 27; ++i) DG[i] *= m.scale_c;
       contract_dg(DG, nrm, m, U + 9 * k);
     } else {
       double Sf[27] = {};
-      // six ranges of 27-28 of the 167 monomials
-      image_q_pass<P, WANT, 0, 55>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
-      image_q_pass<P, WANT, 55, 107>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
-      image_q_pass<P, WANT, 107, 144>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
-      image_q_pass<P, WANT, 144, 180>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
-      image_q_pass<P, WANT, 180, 208>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
-      image_q_pass<P, WANT, 208, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      if constexpr (F32) {
+        // two ranges of 84 and 83 of the 167 monomials
+        image_q_pass<P, WANT, 0, 144>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+        image_q_pass<P, WANT, 144, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      } else {
+        // six ranges of 27-28 of the 167 monomials
+        image_q_pass<P, WANT, 0, 55>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+        image_q_pass<P, WANT, 55, 107>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+        image_q_pass<P, WANT, 107, 144>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+        image_q_pass<P, WANT, 144, 180>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+        image_q_pass<P, WANT, 180, 208>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+        image_q_pass<P, WANT, 208, MHS_Q_NMONO>(q, k, x0, x1, x2, e2, ic, Sf, mun, lamn);
+      }
       double S[3][3][3];
       for (int i = 0; i < 3; ++i)
         for (int p = 0; p < 3; ++p)

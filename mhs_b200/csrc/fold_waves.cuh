@@ -688,8 +688,15 @@ struct AccumShape {
 
 constexpr int ACCUM_WARPS = 4;
 
+#ifndef MHS_ACCUM_MINB
+#define MHS_ACCUM_MINB 1
+#endif
+#ifndef MHS_ACCUM_UNROLL
+#define MHS_ACCUM_UNROLL 2
+#endif
+constexpr int ACCUM_UNROLL = MHS_ACCUM_UNROLL;
 template <int P, int KC>
-__global__ void __launch_bounds__(32 * ACCUM_WARPS)
+__global__ void __launch_bounds__(32 * ACCUM_WARPS, MHS_ACCUM_MINB)
 k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restrict__ pair_oc,
         const long long* __restrict__ pair_poff, const long long* __restrict__ pan_noff,
         const Hdr* __restrict__ hdr, const double* __restrict__ npx,
@@ -721,7 +728,7 @@ k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restric
 #pragma unroll
       for (int t = 0; t < NJG; ++t) pt[c][t] = 0.0;
     const long long ua = pan_noff[q] - n0, ub = pan_noff[q + 1] - n0;
-#pragma unroll 2
+#pragma unroll ACCUM_UNROLL
     for (long long u = ua + gl; u < ub; u += LANES) {
       const double px = npx[u], py = npy[u], w = nw[u];
       double Bv[NC];

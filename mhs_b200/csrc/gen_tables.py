@@ -96,9 +96,11 @@ def main(src: str) -> None:
         rows.sort(key=lambda r: (r[0], r[1]))
         return rows
 
+    rlists = {}
     for name, records, nix in (("DG", t["DG_RECORDS"], 3),
                                ("DDG", t["DDG_RECORDS"], 4)):
         rows = rrecs(records, nix)
+        rlists[name] = rows
         lines.append(f"#define MHS_R_N{name} {len(rows)}")
         lines.append(f"// (monomial, slot) sorted by monomial; slot = flattened "
                      f"{'(i,j,m)' if nix == 3 else '(i,j,p,m)'}")
@@ -179,6 +181,18 @@ def main(src: str) -> None:
         ql += [f"  X({r}, {m}, {sl}) \\" for r, (m, sl, _) in enumerate(qlists[name])]
         ql.append("")
     (HERE / "tables_q.inc").write_text("\n".join(ql) + "\n")
+    # X-macro lists of the R family: every monomial (index, exponents) and
+    # each contraction's records in table order (record, monomial, slot).
+    rl = ["// GENERATED by gen_tables.py -- do not edit by hand.",
+          "// R-family lists as X-macros over the records of tables.inc.", ""]
+    rl.append("#define MHS_R_MONO(X) \\")
+    rl += [f"  X({i}, {a}, {b}, {c}, {n}) \\" for i, (a, b, c, n) in enumerate(rmono)]
+    rl.append("")
+    for name in ("DG", "DDG"):
+        rl.append(f"#define MHS_R_TERMS_{name}(X) \\")
+        rl += [f"  X({r}, {m}, {sl}) \\" for r, (m, sl, _) in enumerate(rlists[name])]
+        rl.append("")
+    (HERE / "tables_r.inc").write_text("\n".join(rl) + "\n")
     print(f"wrote {HERE / 'tables.inc'}: R {len(rmono)} monomials, "
           f"Q {len(qmono)} monomials")
 

@@ -200,6 +200,11 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
   __shared__ std::conditional_t<F32, NoRules, SmemRules<P>> rd;
   __shared__ std::conditional_t<F32 || !IMG, NoRules, SmemRules<IMG ? P : 0>> ri;
   __shared__ double sG[IMG ? G_SIZE : 1];
+  // the R-family coefficients of the request's material, read record by
+  // record by the image term (from shared memory where the block's static
+  // shared memory has room for them: P0 and P1)
+  constexpr bool STAGE_RC = IMG && P < 2;
+  __shared__ double sRc[STAGE_RC ? 3 * (MHS_R_NDG + MHS_R_NDDG) : 1];
   __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rdf;
   __shared__ std::conditional_t<F32 && IMG, FloatRules<IMG ? P : 0>, NoRules> rif;
   if (threadIdx.x == 0) sp = prep[s];
@@ -211,8 +216,11 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
     rd.build(sp.f, threadIdx.x, blockDim.x);
     if constexpr (IMG) ri.build(sp.fi, threadIdx.x, blockDim.x);
   }
-  if (IMG)
+  if (IMG) {
     for (int i = threadIdx.x; i < G_SIZE; i += blockDim.x) sG[i] = Gall[s * G_SIZE + i];
+    if (STAGE_RC)
+      for (int i = threadIdx.x; i < 3 * (MHS_R_NDG + MHS_R_NDDG); i += blockDim.x) sRc[i] = coef[i];
+  }
   __syncthreads();
   const double near_l = F32 ? near_l_mixed : cst::D_STAR;
   const int64_t oc = tile * (int64_t)blockDim.x + threadIdx.x;
@@ -234,7 +242,9 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
     return;
   } else {
     constexpr int C = comps_of(KC);
-    double A[K * C] = {}, E[K] = {};
+    double Abuf[K * C] = {}, E[K] = {};
+    // at P >= 1 the node tensors stay in memory (K * C doubles)
+    double* A = P > 0 ? in_memory(Abuf) : Abuf;
     if constexpr (F32) {
       const QuadRuleT<float> f12 = float_rule_mid<P>(rdf), f8 = float_rule_far<P>(rdf);
       if constexpr (KC == KD_DISP)
@@ -250,8 +260,13 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
     }
     const bool band = sp.straddle && fold_band(x, sp.centre, eps);
     if (!band) {
-      double B[K * C] = {};
-      const ImageCoef ic = image_coef_view(coef);
+      double Bbuf[K * C] = {};
+      double* B = P > 0 ? in_memory(Bbuf) : Bbuf;
+      ImageCoef ic = image_coef_view(coef);
+      if (STAGE_RC) {
+        ic.r_dg = sRc;
+        ic.r_ddg = sRc + 3 * MHS_R_NDG;
+      }
       if constexpr (F32) {
         const QuadRuleT<float> i12 = float_rule_mid<P>(rif), i8 = float_rule_far<P>(rif);
         if constexpr (KC == KD_DISP)
