@@ -336,6 +336,41 @@ __device__ __forceinline__ int panel_pair(const long long* pair_poff, int np, lo
   return a;
 }
 
+// Edge-form counts (small-|u| series, large-|u| series) of a near node, in
+// float: the counts only group nodes into warp-uniform lists -- k_near
+// recomputes every edge's form in double -- so a node whose float test lands
+// on the other side of a form threshold costs some divergence, not accuracy.
+MHS_FI void near_signature_f(const Frame& f, double px, double py, double eps, int& ns, int& nl) {
+  const float d0 = (float)(px - f.c[0]), d1 = (float)(py - f.c[1]), d2 = (float)(0.0 - f.c[2]);
+  const float z = d0 * (float)f.n[0] + d1 * (float)f.n[1] + d2 * (float)f.n[2];
+  const float X0 = d0 * (float)f.e1[0] + d1 * (float)f.e1[1] + d2 * (float)f.e1[2];
+  const float X1 = d0 * (float)f.e2[0] + d1 * (float)f.e2[1] + d2 * (float)f.e2[2];
+  const float h2 = z * z + (float)(eps * eps);
+  float pr[3][2];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    pr[k][0] = (float)f.p[k][0] - X0;
+    pr[k][1] = (float)f.p[k][1] - X1;
+  }
+  const float s2 = (float)cst::SMALL_U_OVER_RHO_SQ, l2 = (float)cst::SERIES_U_OVER_RHO_SQ;
+  ns = 0;
+  nl = 0;
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const int e2 = e == 2 ? 0 : e + 1;
+    const float ev0 = pr[e2][0] - pr[e][0], ev1 = pr[e2][1] - pr[e][1];
+    const float iL = rsqrtf(ev0 * ev0 + ev1 * ev1);
+    const float s1 = ev0 * iL, sy = ev1 * iL;
+    const float dp = pr[e][0] * sy - pr[e][1] * s1;
+    const float ua = pr[e][0] * s1 + pr[e][1] * sy, ub = pr[e2][0] * s1 + pr[e2][1] * sy;
+    const float rho2 = dp * dp + h2;
+    const float a2 = ua * ua, b2 = ub * ub;
+    const float umax2 = a2 > b2 ? a2 : b2, umin2 = a2 < b2 ? a2 : b2;
+    if (umax2 <= s2 * rho2) ++ns;
+    else if (ua * ub > 0.0f && umin2 >= l2 * rho2) ++nl;
+  }
+}
+
 // Nodes of the wave's panels: position, weight, pair, class.  One warp per
 // panel (grid-stride over the wave's panels): each lane takes angular nodes
 // j (one sincos each) and writes the panel's six radial nodes at j, in the
@@ -400,20 +435,8 @@ k_nodes(double near_l, int np, int64_t lo, const double* __restrict__ obs,
           if (D > near_l * sp.f.L) cls = SL_FAR12;
         }
         if (cls == SL_NEAR) {
-          const double xx[3] = {px, py, 0.0};
-          double z, X0, X1;
-          to_plane(sp.f, xx, z, X0, X1);
-          const double h2 = z * z + sp.eps * sp.eps;
-          double pr[3][2];
-          foot_vertices(sp.f, X0, X1, pr);
-          int ns = 0, nl = 0;
-#pragma unroll
-          for (int e = 0; e < 3; ++e) {
-            const EdgeGeom g = edge_geom_rcp(pr, e, h2);
-            const int form = edge_regime_sq(g.ua, g.ub, g.rho2);
-            ns += form == EDGE_SMALL;
-            nl += form == EDGE_LARGE;
-          }
+          int ns, nl;
+          near_signature_f(sp.f, px, py, sp.eps, ns, nl);
           cls = near_sig(ns, nl);
         } else {
           cls = cls == SL_FAR8 ? CLS_FAR8 : CLS_FAR12;
@@ -446,11 +469,9 @@ k_count(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls) {
     for (int k = 0; k < SCAT_PER_THREAD; ++k) {
       const long long u = t0 + (long long)k * blockDim.x + threadIdx.x;
       const int cls = u < n ? ncls[u] : -1;
-#pragma unroll 1
-      for (int c = 0; c < NCLS; ++c) {
-        const unsigned m = __ballot_sync(0xffffffffu, cls == c);
-        if (m && (threadIdx.x & 31) == 0) atomicAdd(&s_cnt[c], __popc(m));
-      }
+      // lanes of one class: the lowest adds their count
+      const unsigned m = __match_any_sync(0xffffffffu, cls);
+      if (cls >= 0 && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&s_cnt[cls], __popc(m));
     }
   }
   __syncthreads();
@@ -503,15 +524,14 @@ k_scatter(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls, int* __
       cls[k] = u < n ? ncls[u] : -1;
       mk[k] = 0;
     }
-    // per warp, per sub-tile: count of each class, and this lane's mask
+    // per warp, per sub-tile: count of each class, and this lane's peers
 #pragma unroll
-    for (int k = 0; k < SCAT_PER_THREAD; ++k)
-#pragma unroll 1
-      for (int c = 0; c < NCLS; ++c) {
-        const unsigned m = __ballot_sync(0xffffffffu, cls[k] == c);
-        if (cls[k] == c) mk[k] = m;
-        if (lane == 0) w_cnt[k][wid][c] = __popc(m);
-      }
+    for (int k = 0; k < SCAT_PER_THREAD; ++k) {
+      if (lane < NCLS) w_cnt[k][wid][lane] = 0;
+      mk[k] = __match_any_sync(0xffffffffu, cls[k]);
+      __syncwarp();
+      if (cls[k] >= 0 && lane == __ffs(mk[k]) - 1) w_cnt[k][wid][cls[k]] = __popc(mk[k]);
+    }
     __syncthreads();
     if (threadIdx.x < NCLS) {
       const int c = threadIdx.x;
@@ -555,8 +575,18 @@ __device__ __forceinline__ QuadRuleT<RF> far_rule(const Src<P, RF>& d, bool r8) 
   }
 }
 
+// Launch bounds of the load and accumulation kernels at P0, from timing them
+// on config 2 (FP64): k_far at 5 blocks of 128 per SM (96 registers; asking
+// for one block lets it take 248 and runs 30 % slower), k_near at 5 (96
+// registers, 10 % faster than 4 despite a few spills), k_accum at 6 (80
+// registers; 20 % faster than its unbounded 132).  P1 and P2 keep their
+// registers (bounding them spills).
+constexpr int FAR_MIN_BLOCKS = 5;
+constexpr int NEAR_MIN_BLOCKS_P0 = 5;
+constexpr int ACCUM_MIN_BLOCKS = 6;
+
 template <int P, int KC, class RF>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, P == 0 ? FAR_MIN_BLOCKS : 1)
 k_far(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* __restrict__ npx,
       const double* __restrict__ npy, const int* __restrict__ npair,
       const int* __restrict__ pair_st, int j0, const int* __restrict__ st_src,
@@ -589,7 +619,7 @@ k_far(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* 
 // edges are visited small-series ones first, then large-series ones, then
 // closed-form ones.
 template <int P, int KC>
-__global__ void __launch_bounds__(128, P == 0 ? 4 : 1)
+__global__ void __launch_bounds__(128, P == 0 ? NEAR_MIN_BLOCKS_P0 : 1)
 k_near(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double* __restrict__ npx,
        const double* __restrict__ npy, const int* __restrict__ npair,
        const int* __restrict__ pair_st, int j0, const int* __restrict__ st_src,
@@ -688,15 +718,8 @@ struct AccumShape {
 
 constexpr int ACCUM_WARPS = 4;
 
-#ifndef MHS_ACCUM_MINB
-#define MHS_ACCUM_MINB 1
-#endif
-#ifndef MHS_ACCUM_UNROLL
-#define MHS_ACCUM_UNROLL 2
-#endif
-constexpr int ACCUM_UNROLL = MHS_ACCUM_UNROLL;
 template <int P, int KC>
-__global__ void __launch_bounds__(32 * ACCUM_WARPS, MHS_ACCUM_MINB)
+__global__ void __launch_bounds__(32 * ACCUM_WARPS, P == 0 ? ACCUM_MIN_BLOCKS : 1)
 k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restrict__ pair_oc,
         const long long* __restrict__ pair_poff, const long long* __restrict__ pan_noff,
         const Hdr* __restrict__ hdr, const double* __restrict__ npx,
@@ -728,7 +751,7 @@ k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restric
 #pragma unroll
       for (int t = 0; t < NJG; ++t) pt[c][t] = 0.0;
     const long long ua = pan_noff[q] - n0, ub = pan_noff[q + 1] - n0;
-#pragma unroll ACCUM_UNROLL
+#pragma unroll 2
     for (long long u = ua + gl; u < ub; u += LANES) {
       const double px = npx[u], py = npy[u], w = nw[u];
       double Bv[NC];
