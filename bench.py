@@ -324,7 +324,8 @@ def run_ours(a, rank, world, legs):
     # the pair kernels: a seeded sample of this rank's pairs counted exactly
     pts = mhs.collocation_points(tris)[lo:hi]
     pf = _flops.pair_flops(pts, tris, eps, mu, lam, order=0, want_h=True, samples=4096)
-    parts["pair"] = pf["k_pair"]["flop"]
+    parts["pair_direct"] = pf["direct"]["flop"]
+    parts["pair_image_r"] = pf["image_r"]["flop"]
     parts["imageq"] = pf["k_imageq"]["flop"]
     per_kernel = {}
     for k, f in parts.items():
@@ -346,7 +347,8 @@ def run_ours(a, rank, world, legs):
                            "frac": fl["flop"] / (fold_ms * 1e-3) / 1e12 / peak if fold_ms else None},
             "kernels": per_kernel,
             "pair_kernels": {"samples": pf["samples"], "band_share": pf["band_share"],
-                             "k_pair": pf["k_pair"], "k_imageq": pf["k_imageq"],
+                             "k_pair (direct)": pf["direct"], "k_image_r": pf["image_r"],
+                             "k_imageq": pf["k_imageq"],
                              "counting": "seeded uniform sample of (observer, source) pairs, "
                                          "each counted exactly by the op-counting build, scaled "
                                          "to all pairs"},

@@ -221,7 +221,7 @@ int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, c
  * tracing. */
 enum mhs_stage {
   MHS_STAGE_PREP = 0,    /* per-material coefficients, per-source frames */
-  MHS_STAGE_PAIR = 1,    /* direct term + image R-family */
+  MHS_STAGE_PAIR = 1,    /* direct term + image R-family (two kernels) */
   MHS_STAGE_IMAGEQ = 2,  /* image Q-family */
   MHS_STAGE_FOLD = 3,    /* band lists + folded image */
   MHS_STAGE_FINAL = 4,   /* eigenstress, contraction, layout stores */
@@ -231,7 +231,10 @@ enum mhs_stage {
   MHS_STAGE_FOLD_FAR = 7,    /* far-field surface loads (12 x 12, 8 x 8 rules) */
   MHS_STAGE_FOLD_NEAR = 8,   /* near-field surface loads (closed form) */
   MHS_STAGE_FOLD_ACCUM = 9,  /* point-load products, panel sums, disk term */
-  MHS_N_STAGES = 10
+  /* parts of the pair stage (their time is inside MHS_STAGE_PAIR's) */
+  MHS_STAGE_PAIR_DIRECT = 10,   /* direct term */
+  MHS_STAGE_PAIR_IMAGE_R = 11,  /* image R-family */
+  MHS_N_STAGES = 12
 };
 int mhs_profile_enable(int on);
 int mhs_profile_read(double* ms, int* launches);

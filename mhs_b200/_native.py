@@ -132,7 +132,7 @@ def load() -> ctypes.CDLL:
 
 
 STAGES = ("prep", "pair", "imageq", "fold", "final", "fold_plan", "fold_nodes", "fold_far",
-          "fold_near", "fold_accum")
+          "fold_near", "fold_accum", "pair_direct", "pair_image_r")
 
 
 def profile(on: bool) -> None:

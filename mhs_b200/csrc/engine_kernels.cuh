@@ -471,23 +471,27 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
   double zpow[G_RMAX + 1];
   zpow[0] = 1.0;
   for (int i = 1; i <= G_RMAX; ++i) zpow[i] = zpow[i - 1] * zp;
-  double Wbuf[K * NW] = {};
-  double* Wall = P > 0 ? in_memory(Wbuf) : Wbuf;   // K * NW doubles at P >= 1
-  if (D <= cst::D_STAR * fi.L && D <= near_l * fi.L) {
+  // The closed form's tables of every node come from one moment table, so
+  // they are formed together; the far field forms each node's table by its
+  // own pass over the rule just before that node's records (at P >= 1 only
+  // one node's table is live then).
+  const bool closed = D <= cst::D_STAR * fi.L && D <= near_l * fi.L;
+  double Wbuf[(P > 0 ? K : 1) * NW] = {};
+  double* Wall = P > 0 ? in_memory(Wbuf) : Wbuf;
+  if (closed) {
     MomentTable<S> T;
     closed_moments<S>(fi, X0, X1, h2, T);
     double c[K][ntri(P)];
     shape_coeffs<P>(fi, X0, X1, c);
     for (int k = 0; k < K; ++k) weight_closed<S, P>(T, c, k, Wall + k * NW);
-  } else {
-    const Q& q = (D > far_switch_l * fi.L) ? r8 : r12;
-    weight_far<S, P, R_FAR>(q, X0, X1, h2, Wall);
   }
+  const Q& q = (D > far_switch_l * fi.L) ? r8 : r12;
   const double mun[3] = {m.mu * nrm[0], m.mu * nrm[1], m.mu * nrm[2]};
   const double lamn[3] = {m.lam * nrm[0], m.lam * nrm[1], m.lam * nrm[2]};
 #pragma unroll 1
   for (int k = 0; k < K; ++k) {
-    const double* W = Wall + k * NW;
+    double* W = Wall + (closed ? k * NW : 0);
+    if (!closed) weight_far_nodes<S, P, R_FAR, 1>(q, R_FAR(X0), R_FAR(X1), R_FAR(h2), k, 0, W);
     if constexpr ((WANT & W_U) != 0) {
       double DG[27] = {};
       image_r_records<S, W_U>(G, W, zpow, zo, ic, DG, mun, lamn);

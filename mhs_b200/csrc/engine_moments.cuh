@@ -644,18 +644,20 @@ MHS_HD void build_rule(const Frame& f, const double* glx, const double* glw, int
 // W_k[n](a, b) by quadrature of N_k xi_1^a xi_2^b R^-n at the constant-slip
 // degrees (mhs/fullspace/moments.py:427-498).  R is float or double: the
 // mixed-precision form runs this in float with float accumulation.
-template <class S, int P, class R, class Q = QuadRule>
-MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, double* Wout) {
+// weight_far_nodes evaluates nodes [k0, k0 + KG) into tables out0, out0 + 1,
+// ... of Wout: every accumulator adds its point terms in rule order,
+// whichever group of nodes it is taken with.
+template <class S, int P, class R, int KG, class Q>
+MHS_HD void weight_far_nodes(const Q& q, R x0, R x1, R hh, int k0, int out0, double* Wout) {
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
   constexpr int NW = sp.w_off[NS];
   constexpr int DM = spec_max_need0(sp);
-  R acc[K][NW];
+  R acc[KG][NW];
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+  for (int k = 0; k < KG; ++k)
 #pragma unroll
     for (int i = 0; i < NW; ++i) acc[k][i] = R(0);
-  const R x0 = R(X0), x1 = R(X1), hh = R(h2);
 #pragma unroll 2
   for (int t = 0; t < q.nq; ++t) {
     const R xi0 = R(q.eta0[t]) - x0, xi1 = R(q.eta1[t]) - x1;
@@ -681,9 +683,9 @@ MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, double* Wout
       p0[i] = p0[i - 1] * xi0;
       p1[i] = p1[i - 1] * xi1;
     }
-    R Nk[K];
+    R Nk[KG];
 #pragma unroll
-    for (int k = 0; k < K; ++k) Nk[k] = R(q.Nq[t * K + k]);
+    for (int k = 0; k < KG; ++k) Nk[k] = R(q.Nq[t * K + k0 + k]);
 #pragma unroll
     for (int a = 0; a <= DM; ++a)
 #pragma unroll
@@ -697,16 +699,36 @@ MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, double* Wout
             acc[0][sp.w_off[s] + tri_idx(a, b)] += v;   // N = 1
           } else {
 #pragma unroll
-            for (int k = 0; k < K; ++k) acc[k][sp.w_off[s] + tri_idx(a, b)] += v * Nk[k];
+            for (int k = 0; k < KG; ++k) acc[k][sp.w_off[s] + tri_idx(a, b)] += v * Nk[k];
           }
         }
       }
   }
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+  for (int k = 0; k < KG; ++k)
 #pragma unroll
-    for (int i = 0; i < NW; ++i) Wout[k * NW + i] = double(acc[k][i]);
+    for (int i = 0; i < NW; ++i) Wout[(out0 + k) * NW + i] = double(acc[k][i]);
 }
 
+// Far-field weighted tables of all K nodes by the product rule q, in
+// passes over the rule of as many nodes as keep at most FAR_ACC_MAX
+// accumulators live (P0 and the smaller specs: one pass); each pass repeats
+// the per-point powers and leaves every sum's order unchanged.
+constexpr int FAR_ACC_MAX = 64;
+
+template <class S, int P, class R, int K0, class Q>
+MHS_HD void weight_far_from(const Q& q, R x0, R x1, R hh, double* Wout) {
+  constexpr int K = n_nodes(P);
+  constexpr int NW = S::spec.w_off[NS];
+  constexpr int KG0 = FAR_ACC_MAX / NW > 0 ? FAR_ACC_MAX / NW : 1;
+  constexpr int KG = (K - K0) < KG0 ? (K - K0) : KG0;
+  weight_far_nodes<S, P, R, KG>(q, x0, x1, hh, K0, K0, Wout);
+  if constexpr (K0 + KG < K) weight_far_from<S, P, R, K0 + KG>(q, x0, x1, hh, Wout);
+}
+
+template <class S, int P, class R, class Q = QuadRule>
+MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, double* Wout) {
+  weight_far_from<S, P, R, 0>(q, R(X0), R(X1), R(h2), Wout);
+}
 
 }  // namespace mhs

@@ -253,7 +253,8 @@ k_panels(int np, int64_t lo, const double* __restrict__ obs, const SrcPrep* __re
          const int* __restrict__ st_src, const int* __restrict__ pair_st,
          const int* __restrict__ pair_oc, const long long* __restrict__ pair_poff,
          const long long* __restrict__ pair_noff, double* __restrict__ pan_ra,
-         double* __restrict__ pan_rb, long long* __restrict__ pan_noff) {
+         double* __restrict__ pan_rb, long long* __restrict__ pan_noff,
+         int* __restrict__ pan_pair) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i > np) return;
   if (i == np) {  // closing entry: the batch's node total
@@ -275,6 +276,7 @@ k_panels(int np, int64_t lo, const double* __restrict__ obs, const SrcPrep* __re
     pan_ra[q] = ra;
     pan_rb[q] = rb;
     pan_noff[q] = u;
+    pan_pair[q] = i;
     u += A.n < 0 ? 0 : (long long)cst::FOLD_N_RADIAL * A.n;
     ++q;
   }
@@ -325,17 +327,6 @@ __global__ void k_wave_begin(long long w, long long span, long long nq,
   }
 }
 
-// Pair of panel q (pair_poff ascending).
-__device__ __forceinline__ int panel_pair(const long long* pair_poff, int np, long long q) {
-  int a = 0, b = np - 1;
-  while (a < b) {
-    const int m = (a + b + 1) >> 1;
-    if (pair_poff[m] <= q) a = m;
-    else b = m - 1;
-  }
-  return a;
-}
-
 // Edge-form counts (small-|u| series, large-|u| series) of a near node, in
 // float: the counts only group nodes into warp-uniform lists -- k_near
 // recomputes every edge's form in double -- so a node whose float test lands
@@ -380,7 +371,7 @@ __global__ void __launch_bounds__(256)
 k_nodes(double near_l, int np, int64_t lo, const double* __restrict__ obs,
         const SrcPrep* __restrict__ prep, const int* __restrict__ st_src,
         const int* __restrict__ pair_st, const int* __restrict__ pair_oc,
-        const long long* __restrict__ pair_poff, const double* __restrict__ pan_ra,
+        const int* __restrict__ pan_pair, const double* __restrict__ pan_ra,
         const double* __restrict__ pan_rb, const long long* __restrict__ pan_noff,
         const Hdr* __restrict__ hdr, double* __restrict__ npx, double* __restrict__ npy,
         double* __restrict__ nw, int* __restrict__ npair, unsigned char* __restrict__ ncls) {
@@ -397,7 +388,7 @@ k_nodes(double near_l, int np, int64_t lo, const double* __restrict__ obs,
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long q = q0 + (long long)blockIdx.x * (blockDim.x >> 5) + wid; q < q1; q += nwarps) {
     if (lane == 0) {
-      const int i = panel_pair(pair_poff, np, q);
+      const int i = pan_pair[q];
       const SrcPrep& sp = prep[st_src[pair_st[i]]];
       FoldPair f;
       pair_geom(obs, lo, pair_oc[i], sp, f);
@@ -721,7 +712,7 @@ constexpr int ACCUM_WARPS = 4;
 template <int P, int KC>
 __global__ void __launch_bounds__(32 * ACCUM_WARPS, P == 0 ? ACCUM_MIN_BLOCKS : 1)
 k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restrict__ pair_oc,
-        const long long* __restrict__ pair_poff, const long long* __restrict__ pan_noff,
+        const int* __restrict__ pan_pair, const long long* __restrict__ pan_noff,
         const Hdr* __restrict__ hdr, const double* __restrict__ npx,
         const double* __restrict__ npy, const double* __restrict__ nw,
         const double* __restrict__ load, long long cap, const double* __restrict__ foot,
@@ -735,7 +726,7 @@ k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restric
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long q = q0 + warp; q < q1; q += nwarps) {
-    const int i = panel_pair(pair_poff, np, q);
+    const int i = pan_pair[q];
     const int64_t o = lo + pair_oc[i];
     const double xh0 = obs[3 * o], xh1 = obs[3 * o + 1];
     const double zeta = -obs[3 * o + 2] > 0.0 ? -obs[3 * o + 2] : 0.0;
@@ -876,7 +867,7 @@ struct Sizes {
   // pair_st, pair_oc (int), pair_poff, pair_noff (scan input and output,
   // one more entry), foot (NJ), acc (NOUT)
   static constexpr size_t per_pair = 4 + 4 + 8 + 8 + 8 * NJ + 8 * NOUT;
-  static constexpr size_t per_panel = 8 + 8 + 8 + 8 * NOUT;   // ra, rb, first node, sums
+  static constexpr size_t per_panel = 8 + 8 + 8 + 4 + 8 * NOUT;   // ra, rb, first node, pair, sums
   static constexpr size_t per_node = 8 * 3 + 4 + 1 + 4 + 8 * NJ;
 };
 
@@ -925,7 +916,7 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
   // budgets of the variable part
   const size_t rest = region_bytes - off;
   const size_t b_src = rest / 10, b_pair = rest * 3 / 20, b_pan = rest * 3 / 20;
-  const size_t b_node = rest - b_src - b_pair - b_pan - 24 * 256;   // 18 aligned carves below
+  const size_t b_node = rest - b_src - b_pair - b_pan - 24 * 256;   // 19 aligned carves below
   const long long cap_src = (long long)(b_src / Z::per_src);
   const long long cap_pair = (long long)(b_pair / Z::per_pair) - 2;
   const long long cap_pan = (long long)(b_pan / Z::per_panel) - 2;
@@ -942,6 +933,7 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
   double* pan_ra = (double*)carve(8 * cap_pan);
   double* pan_rb = (double*)carve(8 * cap_pan);
   long long* pan_noff = (long long*)carve(8 * (cap_pan + 1));
+  int* pan_pair = (int*)carve(4 * cap_pan);
   double* pan_sum = (double*)carve(8 * NOUT * cap_pan);
   double* npx = (double*)carve(8 * cap_node);
   double* npy = (double*)carve(8 * cap_node);
@@ -1004,7 +996,7 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
                                                             r->mu, r->lam, srcs);
       k_panels<<<(np + 1 + 127) / 128, 128, 0, st>>>(np, lo, r->obs, prep, st_src, pair_st,
                                                      pair_oc, pair_poff, pair_noff, pan_ra, pan_rb,
-                                                     pan_noff);
+                                                     pan_noff, pan_pair);
       k_foot<P, KC, RF><<<(np + 127) / 128, 128, 0, st>>>(np, (int)j0, lo, r->obs, prep, st_src,
                                                           pair_st, pair_oc, srcs, foot);
       count_kernels(3);
@@ -1020,7 +1012,7 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
         StageTimer t(MHS_STAGE_FOLD_NODES, st);
         k_wave_begin<<<1, 1, 0, st>>>(w, span, nq, pan_noff, hdr);
         k_nodes<P><<<g_nodes, 256, 0, st>>>(near_l, np, lo, r->obs, prep, st_src, pair_st,
-                                            pair_oc, pair_poff, pan_ra, pan_rb, pan_noff, hdr, npx,
+                                            pair_oc, pan_pair, pan_ra, pan_rb, pan_noff, hdr, npx,
                                             npy, nw, npair, ncls);
         k_count<<<g_scatter, 256, 0, st>>>(hdr, ncls);
         k_wave_classes<<<1, 1, 0, st>>>(hdr, census);
@@ -1042,7 +1034,7 @@ int run_fold(const mhs_request* r, cudaStream_t st, char* region, size_t region_
       }
       {
         StageTimer t(MHS_STAGE_FOLD_ACCUM, st);
-        k_accum<P, KC><<<sms * 16, 32 * ACCUM_WARPS, 0, st>>>(np, lo, r->obs, pair_oc, pair_poff,
+        k_accum<P, KC><<<sms * 16, 32 * ACCUM_WARPS, 0, st>>>(np, lo, r->obs, pair_oc, pan_pair,
                                                              pan_noff, hdr, npx, npy, nw, load,
                                                              cap_node, foot, r->mu, r->lam,
                                                              pan_sum);

@@ -172,16 +172,15 @@ __global__ void k_prep(const ReqDesc* __restrict__ D, const long long* __restric
 }
 
 // ---------------------------------------------------------------- k_pair
-// Direct term and image R-family of one (observer, source) pair.
-// RF: arithmetic type of the far-field quadrature (double; float in the
-// mixed form).
+// Direct term of one (observer, source) pair, stored as the pair's row of
+// the table (the image kernels add to it).  RF: arithmetic type of the
+// far-field quadrature (double; float in the mixed form).
 template <int P, int KC, class RF>
 __global__ void __launch_bounds__(TB)
 k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq,
        double near_l_mixed) {
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);
-  constexpr bool IMG = KC != KD_E;
   const int r = find_req(off, nreq, blockIdx.x);
   const ReqDesc& d = D[r];
   const int64_t lo = d.fa.lo, n_chunk = d.fa.n_chunk, n_src = d.fa.n_src;
@@ -189,38 +188,17 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
   const int64_t s = local % n_src, tile = local / n_src;
   const double* __restrict__ obs = d.obs;
   const SrcPrep* __restrict__ prep = d.prep;
-  const double* __restrict__ Gall = d.G;
-  const double* __restrict__ coef = d.coef;
   const double mu = d.fa.mu, lam = d.fa.lam;
   double* __restrict__ T = d.T;
   constexpr bool F32 = std::is_same<RF, float>::value;
-  // far rules of the element and of its reflection: double, or float only
-  // in the mixed form (whose far field runs in float)
+  // far rules of the element: double, or float only in the mixed form
   __shared__ SrcPrep sp;
   __shared__ std::conditional_t<F32, NoRules, SmemRules<P>> rd;
-  __shared__ std::conditional_t<F32 || !IMG, NoRules, SmemRules<IMG ? P : 0>> ri;
-  __shared__ double sG[IMG ? G_SIZE : 1];
-  // the R-family coefficients of the request's material, read record by
-  // record by the image term (from shared memory where the block's static
-  // shared memory has room for them: P0 and P1)
-  constexpr bool STAGE_RC = IMG && P < 2;
-  __shared__ double sRc[STAGE_RC ? 3 * (MHS_R_NDG + MHS_R_NDDG) : 1];
   __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rdf;
-  __shared__ std::conditional_t<F32 && IMG, FloatRules<IMG ? P : 0>, NoRules> rif;
   if (threadIdx.x == 0) sp = prep[s];
   __syncthreads();
-  if constexpr (F32) {
-    build_float_rules<P>(sp.f, rdf, threadIdx.x, blockDim.x);
-    if constexpr (IMG) build_float_rules<P>(sp.fi, rif, threadIdx.x, blockDim.x);
-  } else {
-    rd.build(sp.f, threadIdx.x, blockDim.x);
-    if constexpr (IMG) ri.build(sp.fi, threadIdx.x, blockDim.x);
-  }
-  if (IMG) {
-    for (int i = threadIdx.x; i < G_SIZE; i += blockDim.x) sG[i] = Gall[s * G_SIZE + i];
-    if (STAGE_RC)
-      for (int i = threadIdx.x; i < 3 * (MHS_R_NDG + MHS_R_NDDG); i += blockDim.x) sRc[i] = coef[i];
-  }
+  if constexpr (F32) build_float_rules<P>(sp.f, rdf, threadIdx.x, blockDim.x);
+  else rd.build(sp.f, threadIdx.x, blockDim.x);
   __syncthreads();
   const double near_l = F32 ? near_l_mixed : cst::D_STAR;
   const int64_t oc = tile * (int64_t)blockDim.x + threadIdx.x;
@@ -232,14 +210,15 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
   double* row = T + ((oc * n_src + s) * K) * NR;
   if constexpr (KC == KD_E) {
     double E[K] = {};
-    if constexpr (F32) direct_eval<P, W_E, RF>(sp.f, float_rule_mid<P>(rdf), float_rule_far<P>(rdf), x, eps, m,
-                                          nullptr, nullptr, E, near_l, cst::D_STAR);
-    else direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
+    if constexpr (F32)
+      direct_eval<P, W_E, RF>(sp.f, float_rule_mid<P>(rdf), float_rule_far<P>(rdf), x, eps, m,
+                              nullptr, nullptr, E, near_l, cst::D_STAR);
+    else
+      direct_eval<P, W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, nullptr, E);
     for (int k = 0; k < K; ++k) {
       row[k * NR + 0] = E[k];
       row[k * NR + 1] = 0.0;
     }
-    return;
   } else {
     constexpr int C = comps_of(KC);
     double Abuf[K * C] = {}, E[K] = {};
@@ -258,37 +237,86 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
       else
         direct_eval<P, W_H | W_E, RF>(sp.f, rd.r12(), rd.r8(), x, eps, m, nullptr, A, E);
     }
-    const bool band = sp.straddle && fold_band(x, sp.centre, eps);
-    if (!band) {
-      double Bbuf[K * C] = {};
-      double* B = P > 0 ? in_memory(Bbuf) : Bbuf;
-      ImageCoef ic = image_coef_view(coef);
-      if (STAGE_RC) {
-        ic.r_dg = sRc;
-        ic.r_ddg = sRc + 3 * MHS_R_NDG;
-      }
-      if constexpr (F32) {
-        const QuadRuleT<float> i12 = float_rule_mid<P>(rif), i8 = float_rule_far<P>(rif);
-        if constexpr (KC == KD_DISP)
-          image_r_eval<P, W_U, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, B, nullptr, near_l,
-                                      cst::D_STAR);
-        else
-          image_r_eval<P, W_H, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, nullptr, B, near_l,
-                                      cst::D_STAR);
-      } else {
-        if constexpr (KC == KD_DISP)
-          image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
-        else
-          image_r_eval<P, W_H>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, nullptr, B);
-      }
-      for (int i = 0; i < K * C; ++i) A[i] += B[i];
-    }
     for (int k = 0; k < K; ++k) {
       for (int c = 0; c < C; ++c) row[k * NR + c] = A[k * C + c];
       row[k * NR + C] = (KC == KD_HE) ? E[k] : 0.0;
       row[k * NR + C + 1] = 0.0;
     }
   }
+}
+
+// --------------------------------------------------------------- k_image_r
+// Image R-family of one (observer, source) pair outside the source's fold
+// band (the fold replaces it there), added to the pair's row.
+template <int P, int KC, class RF>
+__global__ void __launch_bounds__(TB)
+k_image_r(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq,
+          double near_l_mixed) {
+  static_assert(KC != KD_E, "the eigenstress readout has no image term");
+  constexpr int K = n_nodes(P);
+  constexpr int NR = row_of(KC);
+  constexpr int C = comps_of(KC);
+  const int r = find_req(off, nreq, blockIdx.x);
+  const ReqDesc& d = D[r];
+  const int64_t lo = d.fa.lo, n_chunk = d.fa.n_chunk, n_src = d.fa.n_src;
+  const long long local = blockIdx.x - off[r];
+  const int64_t s = local % n_src, tile = local / n_src;
+  const double* __restrict__ obs = d.obs;
+  const SrcPrep* __restrict__ prep = d.prep;
+  const double* __restrict__ Gall = d.G;
+  const double* __restrict__ coef = d.coef;
+  const double mu = d.fa.mu, lam = d.fa.lam;
+  double* __restrict__ T = d.T;
+  constexpr bool F32 = std::is_same<RF, float>::value;
+  // far rules of the reflected element, its basis products, and the
+  // R-family coefficients of the request's material (read record by record,
+  // K times per pair)
+  constexpr bool STAGE_RC = true;
+  __shared__ SrcPrep sp;
+  __shared__ std::conditional_t<F32, NoRules, SmemRules<P>> ri;
+  __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rif;
+  __shared__ double sG[G_SIZE];
+  __shared__ double sRc[STAGE_RC ? 3 * (MHS_R_NDG + MHS_R_NDDG) : 1];
+  if (threadIdx.x == 0) sp = prep[s];
+  __syncthreads();
+  if constexpr (F32) build_float_rules<P>(sp.fi, rif, threadIdx.x, blockDim.x);
+  else ri.build(sp.fi, threadIdx.x, blockDim.x);
+  for (int i = threadIdx.x; i < G_SIZE; i += blockDim.x) sG[i] = Gall[s * G_SIZE + i];
+  if (STAGE_RC)
+    for (int i = threadIdx.x; i < 3 * (MHS_R_NDG + MHS_R_NDDG); i += blockDim.x) sRc[i] = coef[i];
+  __syncthreads();
+  const double near_l = F32 ? near_l_mixed : cst::D_STAR;
+  const int64_t oc = tile * (int64_t)blockDim.x + threadIdx.x;
+  if (oc >= n_chunk) return;
+  const int64_t o = lo + oc;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  const double eps = sp.eps;
+  if (sp.straddle && fold_band(x, sp.centre, eps)) return;
+  const Material m = make_material(mu, lam);
+  double Bbuf[K * C] = {};
+  double* B = P > 0 ? in_memory(Bbuf) : Bbuf;
+  ImageCoef ic = image_coef_view(coef);
+  if (STAGE_RC) {
+    ic.r_dg = sRc;
+    ic.r_ddg = sRc + 3 * MHS_R_NDG;
+  }
+  if constexpr (F32) {
+    const QuadRuleT<float> i12 = float_rule_mid<P>(rif), i8 = float_rule_far<P>(rif);
+    if constexpr (KC == KD_DISP)
+      image_r_eval<P, W_U, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, B, nullptr, near_l,
+                                  cst::D_STAR);
+    else
+      image_r_eval<P, W_H, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, nullptr, B, near_l,
+                                  cst::D_STAR);
+  } else {
+    if constexpr (KC == KD_DISP)
+      image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
+    else
+      image_r_eval<P, W_H>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, nullptr, B);
+  }
+  double* row = T + ((oc * n_src + s) * K) * NR;
+  for (int k = 0; k < K; ++k)
+    for (int c = 0; c < C; ++c) row[k * NR + c] += B[k * C + c];
 }
 
 // -------------------------------------------------------------- k_imageq
@@ -776,9 +804,18 @@ int run_passes(const Pass* ps, int n, void* desc, bool upload, cudaStream_t st,
   }
   {
     StageTimer t(MHS_STAGE_PAIR, st);
-    k_pair<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(D, offs(OFF_PAIR), n,
-                                                                          MIXED_NEAR_L);
-    count_kernels(1);
+    {
+      StageTimer td(MHS_STAGE_PAIR_DIRECT, st);
+      k_pair<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(D, offs(OFF_PAIR), n,
+                                                                            MIXED_NEAR_L);
+      count_kernels(1);
+    }
+    if constexpr (KC != KD_E) {
+      StageTimer ti(MHS_STAGE_PAIR_IMAGE_R, st);
+      k_image_r<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(
+          D, offs(OFF_PAIR), n, MIXED_NEAR_L);
+      count_kernels(1);
+    }
   }
   if constexpr (KC != KD_E) {
     StageTimer t(MHS_STAGE_IMAGEQ, st);

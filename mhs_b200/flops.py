@@ -141,9 +141,9 @@ def pair_flops(obs, tris, eps, mu: float, lam: float, order: int, want_h: bool,
                samples: int = 4096, seed: int = 0) -> dict:
     """Algorithmic flops of the pair kernels over all (observer, source)
     pairs, from a seeded uniform sample counted exactly: the direct term
-    (``k_pair``, every pair), the image R-family (``k_pair``, pairs outside
-    a fold band) and the image Q-family (``k_imageq``, likewise).  Returns
-    totals per kernel and the sample's share of fold-band pairs."""
+    (``k_pair``, every pair), the image R-family (``k_image_r``, pairs
+    outside a fold band) and the image Q-family (``k_imageq``, likewise).
+    Returns totals per kernel and the sample's share of fold-band pairs."""
     lib = _load()
     obs = np.ascontiguousarray(obs, dtype=np.float64)
     tris = np.ascontiguousarray(tris, dtype=np.float64)

@@ -25,8 +25,8 @@ from . import defaults
 
 #: Cost of one fold band pair in units of one ordinary pair (direct + image
 #: terms), measured on the 2,400-triangle interaction workload on a B200:
-#: fold 461 ms for 96,121 band pairs against 75 ms for 5.76 M pairs.
-FOLD_PAIR_COST = 370.0
+#: fold 220 ms for 96,121 band pairs against 55 ms for 5.76 M pairs.
+FOLD_PAIR_COST = 240.0
 
 
 def _straddles(tris: np.ndarray, eps: np.ndarray) -> np.ndarray:
