@@ -326,7 +326,9 @@ def run_ours(a, rank, world, legs):
     pf = _flops.pair_flops(pts, tris, eps, mu, lam, order=0, want_h=True, samples=4096)
     parts["pair_direct"] = pf["direct"]["flop"]
     parts["pair_image_r"] = pf["image_r"]["flop"]
-    parts["imageq"] = pf["k_imageq"]["flop"]
+    # the image Q-family from its census (pairs and rule points counted)
+    qf = _flops.imageq_flops(census, order=0, want_h=True, mu=mu, lam=lam)
+    parts["imageq"] = qf["flop"]
     per_kernel = {}
     for k, f in parts.items():
         t = stage_ms.get(k, 0.0)
@@ -348,10 +350,12 @@ def run_ours(a, rank, world, legs):
             "kernels": per_kernel,
             "pair_kernels": {"samples": pf["samples"], "band_share": pf["band_share"],
                              "k_pair (direct)": pf["direct"], "k_image_r": pf["image_r"],
-                             "k_imageq": pf["k_imageq"],
-                             "counting": "seeded uniform sample of (observer, source) pairs, "
-                                         "each counted exactly by the op-counting build, scaled "
-                                         "to all pairs"},
+                             "k_imageq": qf,
+                             "counting": "k_pair and k_image_r: a seeded uniform sample of "
+                                         "(observer, source) pairs, each counted exactly by the "
+                                         "op-counting build, scaled to all pairs; k_imageq: its "
+                                         "device census of pairs and rule points times the "
+                                         "op-counting build's per-pair and per-point counts"},
             "algorithmic": {"flop_fold": fl["flop"], "div": fl["div"], "sqrt": fl["sqrt"],
                             "special": fl["special"], "census": census,
                             "counting": "op-counting host build of the engine "

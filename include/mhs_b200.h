@@ -243,14 +243,15 @@ int mhs_profile_read(double* ms, int* launches);
  * call; the count is returned and reset.  No counterpart in mhs. */
 int mhs_kernel_count(unsigned long long* n);
 
-/* Fold work census (measurement).  While enabled, the fold kernel counts its
+/* Work census (measurement).  While enabled, the fold kernels count their
  * work units into device counters: band pairs, radial panels, polar-grid
  * nodes per surface-load form (closed form, 12 x 12 rule, 8 x 8 rule) and
  * near-field edge integrals per form (closed, small-|u| series, large-|u|
- * series).  mhs_census_read synchronises the device, returns the
+ * series); the image Q-family kernel counts its pairs and their rule points
+ * (n^2 at Gauss order n).  mhs_census_read synchronises the device, returns the
  * MHS_CENSUS_N counts accumulated since the last read or enable, and clears
  * them.  Multiplied by the per-unit operation counts of the op-counting build
- * (mhs_b200/csrc/opcount.cpp) they give the fold's algorithmic flops.  No
+ * (mhs_b200/csrc/opcount.cpp) they give the algorithmic flops.  No
  * counterpart in mhs. */
 enum mhs_census_item {
   MHS_CENSUS_PAIRS = 0,
@@ -261,7 +262,10 @@ enum mhs_census_item {
   MHS_CENSUS_EDGE_CLOSED = 5,
   MHS_CENSUS_EDGE_SMALL = 6,
   MHS_CENSUS_EDGE_LARGE = 7,
-  MHS_CENSUS_N = 8
+  /* the image Q-family stage: pairs it evaluates and their rule points */
+  MHS_CENSUS_Q_PAIRS = 8,
+  MHS_CENSUS_Q_POINTS = 9,
+  MHS_CENSUS_N = 10
 };
 int mhs_census_enable(int on);
 int mhs_census_read(unsigned long long* counts);

@@ -147,16 +147,17 @@ def profile_read() -> dict:
     return {s: (ms[i], n[i]) for i, s in enumerate(STAGES)}
 
 
-CENSUS = ("pairs", "panels", "near", "far12", "far8", "edge_closed", "edge_small", "edge_large")
+CENSUS = ("pairs", "panels", "near", "far12", "far8", "edge_closed", "edge_small", "edge_large",
+          "q_pairs", "q_points")
 
 
 def census(on: bool) -> None:
-    """Start (clearing the counters) or stop the fold work census."""
+    """Start (clearing the counters) or stop the work census."""
     check(load().mhs_census_enable(1 if on else 0))
 
 
 def census_read() -> dict:
-    """Fold work units counted since the last read (synchronises the device)."""
+    """Work units counted since the last read (synchronises the device)."""
     c = (ctypes.c_ulonglong * len(CENSUS))()
     check(load().mhs_census_read(c))
     return {k: int(c[i]) for i, k in enumerate(CENSUS)}

@@ -569,12 +569,13 @@ __device__ __forceinline__ QuadRuleT<RF> far_rule(const Src<P, RF>& d, bool r8) 
 // Launch bounds of the load and accumulation kernels at P0, from timing them
 // on config 2 (FP64): k_far at 5 blocks of 128 per SM (96 registers; asking
 // for one block lets it take 248 and runs 30 % slower), k_near at 5 (96
-// registers, 10 % faster than 4 despite a few spills), k_accum at 6 (80
-// registers; 20 % faster than its unbounded 132).  P1 and P2 keep their
+// registers, 10 % faster than 4 despite a few spills), k_accum at 5 (96
+// registers, with the next node's loads in flight: 33 % faster than its
+// unbounded 132 registers without the prefetch).  P1 and P2 keep their
 // registers (bounding them spills).
 constexpr int FAR_MIN_BLOCKS = 5;
 constexpr int NEAR_MIN_BLOCKS_P0 = 5;
-constexpr int ACCUM_MIN_BLOCKS = 6;
+constexpr int ACCUM_MIN_BLOCKS = 5;
 
 template <int P, int KC, class RF>
 __global__ void __launch_bounds__(128, P == 0 ? FAR_MIN_BLOCKS : 1)
@@ -695,7 +696,9 @@ k_near(const Hdr* __restrict__ hdr, const int* __restrict__ nlist, const double*
 // strides over the panel's nodes; each group's partials are reduced in a
 // fixed butterfly order) into part[q][c * NJ + jj]; then, per pair, the
 // panel sums added in grid order (k_pair_sum).  Neither order depends on
-// how panels were grouped into waves.
+// how panels were grouped into waves.  The kernel is bound by the latency of
+// its node loads, so each lane loads its next node before it computes the
+// current one.
 template <int P, int KC>
 struct AccumShape {
   static constexpr int K = n_nodes(P);
@@ -742,9 +745,38 @@ k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restric
 #pragma unroll
       for (int t = 0; t < NJG; ++t) pt[c][t] = 0.0;
     const long long ua = pan_noff[q] - n0, ub = pan_noff[q + 1] - n0;
-#pragma unroll 2
-    for (long long u = ua + gl; u < ub; u += LANES) {
-      const double px = npx[u], py = npy[u], w = nw[u];
+    // the next node's data is loaded before this node's products, so each
+    // lane keeps two nodes' loads in flight
+    long long u = ua + gl;
+    double px = 0.0, py = 0.0, w = 0.0, lv[NJG];
+#pragma unroll
+    for (int t = 0; t < NJG; ++t) lv[t] = 0.0;
+    if (u < ub) {
+      px = npx[u];
+      py = npy[u];
+      w = nw[u];
+#pragma unroll
+      for (int t = 0; t < NJG; ++t) {
+        const int jj = grp * NJG + t;
+        lv[t] = jj < NJ ? load[(size_t)jj * cap + u] : 0.0;
+      }
+    }
+#pragma unroll 1
+    for (; u < ub; u += LANES) {
+      const long long un = u + LANES;
+      double pxn = 0.0, pyn = 0.0, wn = 0.0, lvn[NJG];
+#pragma unroll
+      for (int t = 0; t < NJG; ++t) lvn[t] = 0.0;
+      if (un < ub) {
+        pxn = npx[un];
+        pyn = npy[un];
+        wn = nw[un];
+#pragma unroll
+        for (int t = 0; t < NJG; ++t) {
+          const int jj = grp * NJG + t;
+          lvn[t] = jj < NJ ? load[(size_t)jj * cap + un] : 0.0;
+        }
+      }
       double Bv[NC];
       if constexpr (KC == KD_HE) point_stress6_rcp(xh0 - px, xh1 - py, zeta, m.nu_f, Bv);
       else point_disp3_rcp(xh0 - px, xh1 - py, zeta, m.mu, m.nu_f, Bv);
@@ -754,11 +786,16 @@ k_accum(int np, int64_t lo, const double* __restrict__ obs, const int* __restric
       for (int t = 0; t < NJG; ++t) {
         const int jj = grp * NJG + t;
         if (jj < NJ) {
-          const double sv = load[(size_t)jj * cap + u] - sh[t];
+          const double sv = lv[t] - sh[t];
 #pragma unroll
           for (int c = 0; c < NC; ++c) pt[c][t] += Bv[c] * sv;
         }
       }
+      px = pxn;
+      py = pyn;
+      w = wn;
+#pragma unroll
+      for (int t = 0; t < NJG; ++t) lv[t] = lvn[t];
     }
 #pragma unroll
     for (int c = 0; c < NC; ++c)

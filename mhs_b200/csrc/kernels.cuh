@@ -363,7 +363,8 @@ struct QRuleFly {
 // two; the float sums keep their registers.
 template <int P, int KC, class RF>
 __global__ void __launch_bounds__(TB, (P == 0 && std::is_same<RF, double>::value) ? 3 : 1)
-k_imageq(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq) {
+k_imageq(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq,
+         unsigned long long* __restrict__ census) {
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);
   constexpr int C = comps_of(KC);
@@ -407,6 +408,10 @@ k_imageq(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int n
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) ti[3 * i + j] = sp.fi.v[i][j];
   const int n = q_gauss_order(x, ti, eps, sp.f.L, P);
+  if (census) {
+    atomicAdd(&census[MHS_CENSUS_Q_PAIRS], 1ull);
+    atomicAdd(&census[MHS_CENSUS_Q_POINTS], (unsigned long long)n * (unsigned long long)n);
+  }
   double B[K * C] = {};
   constexpr int WANT = KC == KD_DISP ? W_U : W_H;
   bool done = false;
@@ -819,7 +824,8 @@ int run_passes(const Pass* ps, int n, void* desc, bool upload, cudaStream_t st,
   }
   if constexpr (KC != KD_E) {
     StageTimer t(MHS_STAGE_IMAGEQ, st);
-    k_imageq<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(D, offs(OFF_PAIR), n);
+    k_imageq<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(D, offs(OFF_PAIR), n,
+                                                                            census);
     count_kernels(1);
   }
   for (int i = 0; i < n; ++i) {

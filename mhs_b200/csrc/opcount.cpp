@@ -425,4 +425,35 @@ int oc_pair_terms(int P, int want_h, const double* tri, double eps, double mu, d
   return 0;
 }
 
+// The image Q-family of one pair at a given Gauss order n (its work is a
+// fixed part plus a part per rule point, n^2 of them).
+int oc_image_q_n(int P, int want_h, const double* tri, double eps, double mu, double lam,
+                 const double* x, int n, long long* ops) {
+  ensure_gl();
+  if (n < 1 || n > GL_MAX) return -1;
+  CountD tt[9], xx[3] = {x[0], x[1], x[2]};
+  for (int i = 0; i < 9; ++i) tt[i] = tri[i];
+  Frame f;
+  make_frame(tt, f);
+  const Material m = make_material(CountD(mu), CountD(lam));
+  long long scratch[4];
+#define OC_Q(PP)                                                                  \
+  {                                                                               \
+    static CountD coef[OC_COEF_SIZE];                                             \
+    oc_image_coef(m, coef);                                                       \
+    const ImageCoef ic = image_coef_view(coef);                                   \
+    static CountD qy[3 * GL_MAX * GL_MAX], qw[6 * GL_MAX * GL_MAX];               \
+    build_qrule<PP>(f, g_glx, g_glw, n, qy, qw);                                  \
+    const QRule<PP> q{n * n, qy, qw};                                             \
+    CountD B[27 * 6];                                                             \
+    take(scratch);                                                                \
+    if (want_h) image_q_eval<PP, W_H>(q, f.n, xx, CountD(eps), m, ic, nullptr, B); \
+    else image_q_eval<PP, W_U>(q, f.n, xx, CountD(eps), m, ic, B, nullptr);      \
+    take(ops);                                                                    \
+  }
+  if (P == 0) OC_Q(0) else if (P == 1) OC_Q(1) else OC_Q(2)
+#undef OC_Q
+  return 0;
+}
+
 }  // extern "C"

@@ -176,3 +176,27 @@ def pair_flops(obs, tris, eps, mu: float, lam: float, order: int, want_h: bool,
     out["band_share"] = n_band / samples
     return out
 
+
+def imageq_flops(census: dict, order: int, want_h: bool, mu: float = 30.0,
+                 lam: float = 30.0, eps: float = 0.35) -> dict:
+    """Algorithmic flops of the image Q-family kernel from its census: its
+    work per pair is a fixed part plus a part per rule point, taken from the
+    op-counting build at two Gauss orders, times the pairs and the rule
+    points (sum of n^2) the kernel counted."""
+    lib = _load()
+    tri = np.ascontiguousarray(_TRI)
+    x = np.ascontiguousarray([4.0, -3.0, -2.0])
+    per = {}
+    for n in (8, 16):
+        o = _ops()
+        lib.oc_image_q_n(order, 1 if want_h else 0, tri.ctypes.data_as(ctypes.c_void_p), _D(eps),
+                         _D(mu), _D(lam), x.ctypes.data_as(ctypes.c_void_p), n, o)
+        per[n] = _as(o)
+    out = {}
+    for k in ("flop", "div", "sqrt", "special"):
+        b = (per[16][k] - per[8][k]) / (256 - 64)   # per point
+        a = per[8][k] - 64 * b                       # per pair
+        out[k] = a * census["q_pairs"] + b * census["q_points"]
+    out["per_point_flop"] = (per[16]["flop"] - per[8]["flop"]) / (256 - 64)
+    return out
+

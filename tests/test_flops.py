@@ -84,3 +84,34 @@ def test_pair_terms_counts():
     assert far_a[3] == far_b[3] == 8 and far_a[2]["flop"] == far_b[2]["flop"]
     near = terms([0.4, 0.2, -0.8])
     assert near[4] == 0 and near[3] > 8 and near[2]["flop"] > far_a[2]["flop"] * (near[3] / 8) ** 2 * 0.9
+
+
+def test_imageq_flops_from_its_census():
+    """The image Q-family's work is a fixed part per pair plus a part per rule
+    point: doubling the points of a census adds the per-point part."""
+    from mhs_b200 import flops
+    a = flops.imageq_flops({"q_pairs": 10, "q_points": 640}, 0, True)
+    b = flops.imageq_flops({"q_pairs": 10, "q_points": 1280}, 0, True)
+    assert a["per_point_flop"] > 100
+    assert abs((b["flop"] - a["flop"]) - 640 * a["per_point_flop"]) < 1e-6 * b["flop"]
+
+
+def _gpu_census_q(cuda):
+    import mhs_b200 as m
+    from mhs_b200 import _native, synthetic
+    c = synthetic.config2(seed=3, nu=4, nv=2)
+    _native.census(True)
+    m.interaction_matrix(c["tris"], m.Material(c["mu"], c["lam"]), c["eps"])
+    cen = _native.census_read()
+    _native.census(False)
+    return c, cen
+
+
+@pytest.mark.gpu
+def test_gpu_census_counts_image_q_pairs(cuda):
+    """k_imageq counts every pair outside a fold band, each with at least the
+    floor order's 64 points."""
+    c, cen = _gpu_census_q(cuda)
+    n = c["tris"].shape[0]
+    assert 0 < cen["q_pairs"] <= n * n
+    assert cen["q_points"] >= 64 * cen["q_pairs"]
