@@ -96,22 +96,17 @@ def test_imageq_flops_from_its_census():
     assert abs((b["flop"] - a["flop"]) - 640 * a["per_point_flop"]) < 1e-6 * b["flop"]
 
 
-def _gpu_census_q(cuda):
-    import mhs_b200 as m
-    from mhs_b200 import _native, synthetic
-    c = synthetic.config2(seed=3, nu=4, nv=2)
-    _native.census(True)
-    m.interaction_matrix(c["tris"], m.Material(c["mu"], c["lam"]), c["eps"])
-    cen = _native.census_read()
-    _native.census(False)
-    return c, cen
-
-
 @pytest.mark.gpu
 def test_gpu_census_counts_image_q_pairs(cuda):
-    """k_imageq counts every pair outside a fold band, each with at least the
-    floor order's 64 points."""
-    c, cen = _gpu_census_q(cuda)
-    n = c["tris"].shape[0]
-    assert 0 < cen["q_pairs"] <= n * n
-    assert cen["q_points"] >= 64 * cen["q_pairs"]
+    """k_imageq counts every pair outside a fold band (here, a buried fault:
+    all of them), each with at least the floor order's 64 points."""
+    import mhs_b200 as m
+    from mhs_b200 import _native, synthetic
+    tris = synthetic.planar_fault(10.0, 60.0, 6.0, 3.0, -2.0, 6, 3)
+    n = tris.shape[0]
+    _native.census(True)
+    m.interaction_matrix(tris, m.Material(30.0, 30.0), 0.1)
+    cen = _native.census_read()
+    _native.census(False)
+    assert cen["pairs"] == 0 and cen["q_pairs"] == n * n
+    assert cen["q_points"] >= 64 * n * n
