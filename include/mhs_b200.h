@@ -202,6 +202,41 @@ int mhs_read_status(void* workspace, void* stream, int* bits);
 int mhs_column_plan(const int64_t* ids_host, int64_t n_src, int64_t n_cols, int32_t* col_ptr,
                     int32_t* col_ent);
 
+/* The full-space single-triangle API (mhs/fullspace/api.py:90-175): the
+ * nodal influence tensors of ONE triangle at n_obs observers (one thread per
+ * observer), for the kernels in `want` (OR of MHS_FS_*):
+ *   U (n, K, 3, 3)     slip -> displacement       (MHS_FS_U)
+ *   H (n, K, 3, 3, 3)  slip -> TOTAL stress       (MHS_FS_H)
+ *   E (n, K)           eigenstress weight         (MHS_FS_E)
+ *   G (n, K, 3, 3)     force density -> displacement, Kelvin single layer (MHS_FS_G)
+ *   S (n, K, 3, 3, 3)  force density -> stress    (MHS_FS_S)
+ * with K = 1, 3, 6 nodes at order 0, 1, 2 (the nodes of the matrix
+ * functions).  far_field: MHS_FAR_HYBRID (closed form within D_STAR element
+ * lengths, Gauss quadrature beyond, as mhs's default), MHS_FAR_ANALYTIC
+ * (closed form everywhere), MHS_FAR_QUADRATURE (quadrature everywhere).
+ * tri: the vertex rows, by value in the request; obs and the outputs on
+ * the device.  Material by (mu, nu), as mhs's full-space API.  eps >= 0; with
+ * eps = 0 every observer must lie off the triangle's plane (the caller
+ * checks: this engine has no on-plane limit). */
+enum { MHS_FS_U = 1, MHS_FS_H = 2, MHS_FS_E = 4, MHS_FS_G = 8, MHS_FS_S = 16 };
+enum { MHS_FAR_HYBRID = 0, MHS_FAR_ANALYTIC = 1, MHS_FAR_QUADRATURE = 2 };
+typedef struct mhs_fullspace_request {
+  int order;
+  int want;
+  int far_field;
+  int pad;
+  int64_t n_obs;
+  const double* obs;   /* (n_obs, 3), device */
+  double tri[9];       /* vertex rows, by value */
+  double mu, nu, eps;
+  double* U;           /* device outputs; NULL where not wanted */
+  double* H;
+  double* E;
+  double* G;
+  double* S;
+} mhs_fullspace_request;
+int mhs_fullspace_influence(const mhs_fullspace_request* req, void* stream);
+
 /* Diagnostics: one influence term of ONE source at n observers, one thread
  * per observer, as the pipeline evaluates it (term 0 direct, 1 image
  * R-family, 2 image Q-family, 3 folded image; with want_u = 0, 4 and 5 the

@@ -9,8 +9,12 @@ without a CUDA device the matrix functions raise.
     import mhs_b200 as mhs
     mat = mhs.Material(mu=30.0, lam=30.0)
     G = mhs.disp_matrix(obs, tris, mat, eps=0.1)     # (n_obs, 3, n_src, 3)
+
+``mhs_b200.fullspace`` is mhs.fullspace.api's single-triangle calls
+(displacement, stress, eigenstress, force_displacement, force_stress,
+influence) on the device.
 """
-from . import chunking, defaults, tdcs
+from . import chunking, defaults, fullspace, tdcs
 from .materials import Material
 from .matrices import (
     collocation_points,
@@ -46,6 +50,7 @@ __all__ = [
     "SharedNodes",
     "chunking",
     "defaults",
+    "fullspace",
     "tdcs",
 ]
 

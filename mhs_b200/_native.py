@@ -63,7 +63,16 @@ EXPORTS = ("mhs_workspace_bytes", "mhs_assemble", "mhs_read_status", "mhs_column
            "mhs_fp_peak", "mhs_debug_terms", "mhs_assemble_noalloc", "mhs_census_enable",
            "mhs_census_read", "mhs_kernel_count", "mhs_batch_create", "mhs_batch_workspace_bytes",
            "mhs_batch_bind", "mhs_submit_batch", "mhs_poll", "mhs_batch_destroy", "mhs_autotune",
-           "mhs_set_tune", "mhs_get_tune", "mhs_batch_pass_bytes")
+           "mhs_set_tune", "mhs_get_tune", "mhs_batch_pass_bytes", "mhs_fullspace_influence")
+
+class FullspaceRequest(ctypes.Structure):
+    """struct mhs_fullspace_request (include/mhs_b200.h)."""
+    _fields_ = [("order", ctypes.c_int), ("want", ctypes.c_int), ("far_field", ctypes.c_int),
+                ("pad", ctypes.c_int), ("n_obs", ctypes.c_int64), ("obs", ctypes.c_void_p),
+                ("tri", ctypes.c_double * 9), ("mu", ctypes.c_double), ("nu", ctypes.c_double),
+                ("eps", ctypes.c_double), ("U", ctypes.c_void_p), ("H", ctypes.c_void_p),
+                ("E", ctypes.c_void_p), ("G", ctypes.c_void_p), ("S", ctypes.c_void_p)]
+
 
 _lib = None
 
@@ -120,6 +129,8 @@ def load() -> ctypes.CDLL:
     lib.mhs_batch_destroy.argtypes = [V]
     lib.mhs_batch_pass_bytes.argtypes = [R, ctypes.POINTER(ctypes.c_size_t),
                                          ctypes.POINTER(ctypes.c_size_t)]
+    lib.mhs_fullspace_influence.argtypes = [ctypes.POINTER(FullspaceRequest), V]
+    lib.mhs_fullspace_influence.restype = ctypes.c_int
     lib.mhs_autotune.argtypes = [R, V, ctypes.POINTER(Tune), ctypes.POINTER(ctypes.c_double)]
     lib.mhs_set_tune.argtypes = [R, ctypes.POINTER(Tune)]
     lib.mhs_get_tune.argtypes = [R, ctypes.POINTER(Tune)]

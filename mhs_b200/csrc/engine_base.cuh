@@ -232,11 +232,14 @@ MHS_FI constexpr Spec make_spec(int d1, int d3, int d5, int d7, int d9, int orde
 
 // Constant-slip degrees per readout (mhs/fullspace/moments.py:63-91):
 //   U -> {3: 1, 5: 3};  H (and H + E) -> {3: 0, 5: 2, 7: 4};  E -> {7: 0};
-// the image R-family reads {3: 1, 5: 3, 7: 4, 9: 5} (its generated table).
+// the image R-family reads {3: 1, 5: 3, 7: 4, 9: 5} (its generated table);
+// the force source G -> {1: 0, 3: 2}, S -> {3: 1, 5: 3}.
 template <int P> struct SpecU { static constexpr Spec spec = make_spec(-1, 1, 3, -1, -1, P); };
 template <int P> struct SpecH { static constexpr Spec spec = make_spec(-1, 0, 2, 4, -1, P); };
 template <int P> struct SpecE { static constexpr Spec spec = make_spec(-1, -1, -1, 0, -1, P); };
 template <int P> struct SpecImg { static constexpr Spec spec = make_spec(-1, 1, 3, 4, 5, P); };
+// the force (Kelvin single-layer) source: G reads {1: 0, 3: 2}, S the U degrees
+template <int P> struct SpecF { static constexpr Spec spec = make_spec(0, 2, 3, -1, -1, P); };
 
 // ------------------------------------------------------------------ frames
 struct Frame {

@@ -13,7 +13,7 @@
 
 namespace mhs {
 
-enum : int { W_U = 1, W_H = 2, W_E = 4 };
+enum : int { W_U = 1, W_H = 2, W_E = 4, W_G = 8, W_S = 16 };
 
 // Spec of the direct term for a readout mask.
 template <int P, int WANT> struct DirectSpec {
@@ -61,11 +61,12 @@ MHS_HD void rotate3(const Frame& f, const double in[3][3][3], double* out) {
         out[9 * a + 3 * b + c] = t2[a][b][0] * B[0][c] + t2[a][b][1] * B[1][c] + t2[a][b][2] * B[2][c];
 }
 
-// Slip -> displacement (mhs/fullspace/kernels.py:148-163), evaluated in the
-// element frame where the normal is e3, then rotated.
+// The integrated gradient G1[i][j][k] of the mollified Kelvin solution over
+// the element (mhs/fullspace/kernels.py:148-157), in the element frame where
+// the normal is e3: read by the slip displacement and the force stress.
 template <class S>
-MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, const Material& m,
-                     double* U) {
+MHS_HD void g1_local(const double* W, double z, double eps, const Material& m,
+                     double G1[3][3][3]) {
   double zp[4] = {1.0, z, z * z, z * z * z};
   const int s5 = nslot(5);
   constexpr Spec sp = S::spec;
@@ -74,7 +75,6 @@ MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, cons
   const double V5[3] = {-W[o5 + tri_idx(1, 0)], -W[o5 + tri_idx(0, 1)], z * W[o5]};
   const double e2 = eps * eps;
   const double f6 = 6.0 * m.one_m_nu * e2;
-  double G1[3][3][3];
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j)
       for (int k = 0; k < 3; ++k) {
@@ -87,6 +87,15 @@ MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, cons
         g = g - (i == j ? f6 * V5[k] : 0.0);
         G1[i][j][k] = g * m.C1;
       }
+}
+
+// Slip -> displacement (mhs/fullspace/kernels.py:159-163), evaluated in the
+// element frame, then rotated.
+template <class S>
+MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, const Material& m,
+                     double* U) {
+  double G1[3][3][3];
+  g1_local<S>(W, z, eps, m, G1);
   double Ul[3][3];
   for (int i = 0; i < 3; ++i) {
     const double tr = G1[i][0][0] + G1[i][1][1] + G1[i][2][2];
@@ -94,6 +103,46 @@ MHS_HD void kernel_U(const Frame& f, const double* W, double z, double eps, cons
       Ul[i][j] = -(m.mu * G1[i][j][2] + (j == 2 ? m.lam_d * tr : 0.0) + m.mu * G1[i][2][j]);
   }
   rotate2(f, Ul, U);
+}
+
+// Force density -> displacement, the Kelvin single layer (mhs/fullspace/
+// kernels.py:165-173): C1 [(3 - 4 nu) I1 delta_ij + T23_ij + 2 (1 - nu)
+// eps^2 I3 delta_ij], in the element frame, then rotated.
+template <class S>
+MHS_HD void kernel_G(const Frame& f, const double* W, double z, double eps, const Material& m,
+                     double* G) {
+  const double zp[3] = {1.0, z, z * z};
+  constexpr Spec sp = S::spec;
+  const double I1 = W[sp.w_off[nslot(1)]], I3 = W[sp.w_off[nslot(3)]];
+  const double f2 = 2.0 * m.one_m_nu * (eps * eps);
+  double Gl[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const int ca = (i == 0) + (j == 0), cb = (i == 1) + (j == 1);
+      double g = (i == j ? m.c34 * I1 : 0.0);
+      g = g + lift_local<S>(W, nslot(3), ca, cb, 2 - ca - cb, zp);
+      g = g + (i == j ? f2 * I3 : 0.0);
+      Gl[i][j] = m.C1 * g;
+    }
+  rotate2(f, Gl, G);
+}
+
+// Force density -> stress (mhs/fullspace/kernels.py:175-181):
+// S[i][j][c] = lam delta_ij G1[a][c][a] + mu (G1[i][c][j] + G1[j][c][i]),
+// in the element frame, then rotated in all three indices.
+template <class S>
+MHS_HD void kernel_S(const Frame& f, const double* W, double z, double eps, const Material& m,
+                     double* Sout) {
+  double G1[3][3][3];
+  g1_local<S>(W, z, eps, m, G1);
+  double Sl[3][3][3];
+  for (int c = 0; c < 3; ++c) {
+    const double tr = G1[0][c][0] + G1[1][c][1] + G1[2][c][2];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        Sl[i][j][c] = (i == j ? m.lam_d * tr : 0.0) + m.mu * G1[i][c][j] + m.mu * G1[j][c][i];
+  }
+  rotate3(f, Sl, Sout);
 }
 
 // Lifted local-frame quantities of the stress kernel, one vector per node:
@@ -218,9 +267,10 @@ MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
   to_plane(f, x, z, X0, X1);
   const double h2 = z * z + eps * eps;
   const double e4 = 15.0 * (eps * eps) * (eps * eps) / (8.0 * cst::PI);
-  // closed form within D_STAR element lengths (near_l < D_STAR: the mixed
-  // form's narrower closed-form zone, the far rule beyond it)
-  if (D <= cst::D_STAR * f.L && D <= near_l * f.L) {
+  // closed form within near_l element lengths: D_STAR (mhs's hybrid split),
+  // the mixed form's narrower zone, or (the full-space API's far_field
+  // options) everywhere / nowhere; the far rule beyond
+  if (D <= near_l * f.L) {
     MomentTable<S> T;
     closed_moments<S>(f, X0, X1, h2, T);
     double c[K][ntri(P)];
@@ -243,6 +293,48 @@ MHS_HD void direct_eval(const Frame& f, const Q& r12, const Q& r8,
       if (WANT & W_U) kernel_U<S>(f, W + k * NW, z, eps, m, U + 9 * k);
       if (WANT & W_H) kernel_H<S>(f, W + k * NW, z, eps, m, H + 27 * k);
       if (WANT & W_E) E[k] = e4 * W[k * NW + sp.w_off[nslot(7)]];
+    }
+  }
+}
+
+// Force (Kelvin single-layer) source of one triangle at one observer, all K
+// nodes: G[k] (9) and / or S[k] (27), from the force source's weighted
+// tables with the same near / far split as direct_eval (node loops fully
+// unrolled, as there).
+template <int P, int WANT, class Q = QuadRule>
+MHS_HD void force_eval(const Frame& f, const Q& r12, const Q& r8, const double* x, double eps,
+                       const Material& m, double* G, double* S, double near_l = cst::D_STAR,
+                       double far_switch_l = cst::D_STAR_DISTANT) {
+  using Sp = SpecF<P>;
+  constexpr Spec sp = Sp::spec;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = sp.w_off[NS];
+  const double d0 = x[0] - f.c[0], d1 = x[1] - f.c[1], d2 = x[2] - f.c[2];
+  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
+  double z, X0, X1;
+  to_plane(f, x, z, X0, X1);
+  const double h2 = z * z + eps * eps;
+  if (D <= near_l * f.L) {
+    MomentTable<Sp> T;
+    closed_moments<Sp>(f, X0, X1, h2, T);
+    double c[K][ntri(P)];
+    shape_coeffs<P>(f, X0, X1, c);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double W[NW] = {};
+      weight_closed<Sp, P>(T, c, k, W);
+      if (WANT & W_G) kernel_G<Sp>(f, W, z, eps, m, G + 9 * k);
+      if (WANT & W_S) kernel_S<Sp>(f, W, z, eps, m, S + 27 * k);
+    }
+  } else {
+    const Q& q = (D > far_switch_l * f.L) ? r8 : r12;
+    double Wbuf[K * NW] = {};
+    double* W = P > 0 ? in_memory(Wbuf) : Wbuf;
+    weight_far<Sp, P, double>(q, X0, X1, h2, W);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (WANT & W_G) kernel_G<Sp>(f, W + k * NW, z, eps, m, G + 9 * k);
+      if (WANT & W_S) kernel_S<Sp>(f, W + k * NW, z, eps, m, S + 27 * k);
     }
   }
 }
@@ -475,7 +567,7 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
   // they are formed together; the far field forms each node's table by its
   // own pass over the rule just before that node's records (at P >= 1 only
   // one node's table is live then).
-  const bool closed = D <= cst::D_STAR * fi.L && D <= near_l * fi.L;
+  const bool closed = D <= near_l * fi.L;
   double Wbuf[(P > 0 ? K : 1) * NW] = {};
   double* Wall = P > 0 ? in_memory(Wbuf) : Wbuf;
   if (closed) {

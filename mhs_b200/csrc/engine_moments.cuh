@@ -203,7 +203,7 @@ MHS_FI void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
   constexpr int QHI = series_qhi(sp);             // largest s
   constexpr int SMIN = series_qlo(sp) + 2 * (T - 1);   // smallest s
   constexpr int W = QHI - SMIN + 1;               // window width
-  static_assert(QHI <= 2, "large-u series exponent above 2");
+  static_assert(QHI <= 3, "large-u series exponent above 3");
   static_assert(SMIN <= 0, "window shift assumes a negative exponent at t = 0");
   const bool neg = ua < 0.0;
   const double a = neg ? -ub : ua, b = neg ? -ua : ub;
@@ -214,10 +214,11 @@ MHS_FI void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
   const double rm1 = (b - a) / a;     // r - 1
   const double omt = (b - a) / b;     // 1 - 1/r
   const double tt = a / b;            // 1/r
-  double dpos[3] = {0.0, 0.0, 0.0};
+  double dpos[4] = {0.0, 0.0, 0.0, 0.0};
   if constexpr (QHI >= 0) dpos[0] = log_r;
   if constexpr (QHI >= 1) dpos[1] = close ? rm1 : r - 1.0;
   if constexpr (QHI >= 2) dpos[2] = (close ? rm1 * (1.0 + r) : r * r - 1.0) * 0.5;
+  if constexpr (QHI >= 3) dpos[3] = (close ? rm1 * ((1.0 + r) + r * r) : (r * r) * r - 1.0) / 3.0;
   // recurrence over k = -q = 1, 2, ...: dq[-k] = (close ? omt G_k : 1 - t^k) / k
   double gsum = 0.0, tk = 1.0;
   int kc = 0;
@@ -227,7 +228,7 @@ MHS_FI void edge_large(double ua, double ub, double rho2, double P[MS][8]) {
   for (int w = 0; w < W; ++w) {
     const int q = QHI - w;
     if (q >= 0) {
-      win[w] = dpos[q >= 0 && q <= 2 ? q : 0];
+      win[w] = dpos[q >= 0 && q <= 3 ? q : 0];
     } else {
       // generate up to k = -q (k ascending as w grows)
       while (kc < -q) {

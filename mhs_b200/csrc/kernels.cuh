@@ -978,6 +978,67 @@ int debug_terms(int term, int want_u, int n, const double* obs, const double* tr
   return MHS_OK;
 }
 
+// ------------------------------------------------------------ full space
+// The full-space single-triangle API (mhs/fullspace/api.py:90-175): the
+// nodal influence tensors of one triangle at n observers, one thread per
+// observer -- slip source U (K x 9), total stress H (K x 27), eigenstress
+// weight E (K); force source G (K x 9), S (K x 27) -- for the kernels in
+// `want`, with the closed form within near_l element lengths (D_STAR: the
+// hybrid far field; +inf: analytic; -1: quadrature everywhere).
+struct FsTri {
+  double v[9];
+};
+static_assert(MHS_FS_U == W_U && MHS_FS_H == W_H && MHS_FS_E == W_E && MHS_FS_G == W_G &&
+                  MHS_FS_S == W_S,
+              "the ABI's kernel flags are the engine's");
+
+template <int P>
+__global__ void __launch_bounds__(64)
+k_fullspace(int want, double near_l, int64_t n, const double* __restrict__ obs, FsTri tri,
+            double mu, double lam, double eps, double* U, double* H, double* E, double* G,
+            double* S) {
+  constexpr int K = n_nodes(P);
+  __shared__ Frame f;
+  __shared__ SmemRules<P> rd;
+  if (threadIdx.x == 0) make_frame(tri.v, f);
+  __syncthreads();
+  rd.build(f, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
+  const Material m = make_material(mu, lam);
+  const QuadRule r12 = rd.r12(), r8 = rd.r8();
+  if (want & W_U) direct_eval<P, W_U>(f, r12, r8, x, eps, m, U + o * K * 9, nullptr, nullptr, near_l);
+  if ((want & W_H) && (want & W_E))
+    direct_eval<P, W_H | W_E>(f, r12, r8, x, eps, m, nullptr, H + o * K * 27, E + o * K, near_l);
+  else if (want & W_H)
+    direct_eval<P, W_H>(f, r12, r8, x, eps, m, nullptr, H + o * K * 27, nullptr, near_l);
+  else if (want & W_E)
+    direct_eval<P, W_E>(f, r12, r8, x, eps, m, nullptr, nullptr, E + o * K, near_l);
+  if ((want & W_G) && (want & W_S))
+    force_eval<P, W_G | W_S>(f, r12, r8, x, eps, m, G + o * K * 9, S + o * K * 27, near_l);
+  else if (want & W_G)
+    force_eval<P, W_G>(f, r12, r8, x, eps, m, G + o * K * 9, nullptr, near_l);
+  else if (want & W_S)
+    force_eval<P, W_S>(f, r12, r8, x, eps, m, nullptr, S + o * K * 27, near_l);
+}
+
+template <int P>
+int fullspace_run(int want, double near_l, int64_t n, const double* obs, const double* tri,
+                  double mu, double lam, double eps, double* U, double* H, double* E, double* G,
+                  double* S, cudaStream_t st) {
+  if (n <= 0) return MHS_OK;
+  FsTri t;
+  for (int i = 0; i < 9; ++i) t.v[i] = tri[i];
+  const int64_t nb = (n + 63) / 64;
+  if (nb > INT32_MAX) return fail(MHS_ERR_ARG, "fullspace: too many observers");
+  k_fullspace<P><<<(unsigned)nb, 64, 0, st>>>(want, near_l, n, obs, t, mu, lam, eps, U, H, E, G, S);
+  count_kernels(1);
+  MHS_CUDA_TRY(cudaGetLastError());
+  return MHS_OK;
+}
+
 }  // namespace
 }  // namespace pipe
 }  // namespace mhs

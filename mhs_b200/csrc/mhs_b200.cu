@@ -76,6 +76,7 @@ const UnitEntry g_units[] = {MHS_UNIT_LIST(MHS_UNIT_ENTRY)};
 #undef MHS_UNIT_ENTRY
 const UnitInit g_terms_init[3] = {unit_init_terms_0, unit_init_terms_1, unit_init_terms_2};
 const UnitTerms g_terms[3] = {unit_terms_0, unit_terms_1, unit_terms_2};
+const UnitFullspace g_fullspace[3] = {unit_fullspace_0, unit_fullspace_1, unit_fullspace_2};
 
 std::mutex g_init_mu;
 std::vector<int> g_init_done;
@@ -361,6 +362,32 @@ int mhs_debug_terms(int order, int term, int want_u, int n, const double* obs, c
   if (order < 0 || order > 2) return fail(MHS_ERR_ARG, "order");
   return g_terms[order](term, want_u, n, obs, tri, mu, lam, eps, coef_scratch, out,
                         (cudaStream_t)stream);
+}
+
+int mhs_fullspace_influence(const mhs_fullspace_request* q, void* stream) {
+  if (!q) return fail(MHS_ERR_ARG, "fullspace: null request");
+  if (q->order < 0 || q->order > 2) return fail(MHS_ERR_ARG, "fullspace: order must be 0, 1 or 2");
+  const int all = MHS_FS_U | MHS_FS_H | MHS_FS_E | MHS_FS_G | MHS_FS_S;
+  if (q->want == 0 || (q->want & ~all)) return fail(MHS_ERR_ARG, "fullspace: want");
+  if (q->n_obs < 0 || (q->n_obs > 0 && !q->obs)) return fail(MHS_ERR_ARG, "fullspace: obs");
+  if (((q->want & MHS_FS_U) && !q->U) || ((q->want & MHS_FS_H) && !q->H) ||
+      ((q->want & MHS_FS_E) && !q->E) || ((q->want & MHS_FS_G) && !q->G) ||
+      ((q->want & MHS_FS_S) && !q->S))
+    return fail(MHS_ERR_ARG, "fullspace: an output of `want` is NULL");
+  if (!(q->mu > 0.0) || !(q->nu > -1.0 && q->nu < 0.5) || !(q->eps >= 0.0))
+    return fail(MHS_ERR_ARG, "fullspace: mu > 0, -1 < nu < 1/2, eps >= 0");
+  double near_l;
+  switch (q->far_field) {
+    case MHS_FAR_HYBRID: near_l = cst::D_STAR; break;
+    case MHS_FAR_ANALYTIC: near_l = INFINITY; break;
+    case MHS_FAR_QUADRATURE: near_l = -1.0; break;
+    default: return fail(MHS_ERR_ARG, "fullspace: far_field");
+  }
+  int rc = ensure_device_tables();
+  if (rc) return rc;
+  const double lam = 2.0 * q->mu * q->nu / (1.0 - 2.0 * q->nu);
+  return g_fullspace[q->order](q->want, near_l, q->n_obs, q->obs, q->tri, q->mu, lam, q->eps,
+                               q->U, q->H, q->E, q->G, q->S, (cudaStream_t)stream);
 }
 
 int mhs_census_enable(int on) {

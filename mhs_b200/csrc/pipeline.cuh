@@ -237,6 +237,9 @@ using UnitBatch = int (*)(const mhs_request* const* r, const Layout* L, int n, v
 using UnitTerms = int (*)(int term, int want_u, int n, const double* obs, const double* tri,
                           double mu, double lam, double eps, double* coef, double* out,
                           cudaStream_t st);
+using UnitFullspace = int (*)(int want, double near_l, int64_t n, const double* obs,
+                              const double* tri, double mu, double lam, double eps, double* U,
+                              double* H, double* E, double* G, double* S, cudaStream_t st);
 
 #define MHS_UNIT_LIST(X) \
   X(0, 0, 0) X(0, 0, 1) X(0, 1, 0) X(0, 1, 1) X(0, 2, 0) X(0, 2, 1) \
@@ -257,7 +260,10 @@ MHS_UNIT_LIST(MHS_UNIT_DECL)
   int unit_init_terms_##P(const double* glx, const double* glw);                         \
   int unit_terms_##P(int term, int want_u, int n, const double* obs, const double* tri,  \
                      double mu, double lam, double eps, double* coef, double* out,       \
-                     cudaStream_t st);
+                     cudaStream_t st);                                                   \
+  int unit_fullspace_##P(int want, double near_l, int64_t n, const double* obs,          \
+                         const double* tri, double mu, double lam, double eps, double* U, \
+                         double* H, double* E, double* G, double* S, cudaStream_t st);
 MHS_TERMS_DECL(0)
 MHS_TERMS_DECL(1)
 MHS_TERMS_DECL(2)

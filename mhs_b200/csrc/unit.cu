@@ -1,7 +1,8 @@
 // One kernel unit of the library.  The build compiles this file once per
 // (order P, readout class KC, far-field type RF) with
 //   -DMHS_UNIT_P=<0|1|2> -DMHS_UNIT_KC=<0 disp|1 stress+blob|2 blob> -DMHS_UNIT_RF=<0 double|1 float>
-// and once per order with -DMHS_UNIT_TERMS=<P> for the per-term diagnostics,
+// and once per order with -DMHS_UNIT_TERMS=<P> for the per-term diagnostics
+// and the full-space single-triangle API,
 // so the units compile in parallel; the host unit (mhs_b200.cu) dispatches.
 #include "kernels.cuh"
 
@@ -31,6 +32,14 @@ int MHS_CAT2(unit_terms_, MHS_UNIT_TERMS)(int term, int want_u, int n, const dou
                                           const double* tri, double mu, double lam, double eps,
                                           double* coef, double* out, cudaStream_t st) {
   return debug_terms<MHS_UNIT_TERMS>(term, want_u, n, obs, tri, mu, lam, eps, coef, out, st);
+}
+
+int MHS_CAT2(unit_fullspace_, MHS_UNIT_TERMS)(int want, double near_l, int64_t n,
+                                              const double* obs, const double* tri, double mu,
+                                              double lam, double eps, double* U, double* H,
+                                              double* E, double* G, double* S, cudaStream_t st) {
+  return fullspace_run<MHS_UNIT_TERMS>(want, near_l, n, obs, tri, mu, lam, eps, U, H, E, G, S,
+                                       st);
 }
 
 #else

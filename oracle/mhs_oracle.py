@@ -167,6 +167,8 @@ def edge_degrees(deg):
 NEED_U = {3: 1, 5: 3}
 NEED_H = {3: 0, 5: 2, 7: 4}
 NEED_E = {7: 0}
+NEED_G = {1: 0, 3: 2}
+NEED_S = {3: 1, 5: 3}
 NEED_IMG = {3: 1, 5: 3, 7: 4, 9: 5}
 
 
@@ -476,13 +478,14 @@ def _material(mu, lam):
 
 
 def direct(x, tri, P, mu, lam, eps, want):
-    """Full-space Kelvin-Cortez U / H / E of one triangle
-    (fullspace/kernels.py:126-215; (mu, lam) -> nu at assemble.py:58-66)."""
+    """Full-space Kelvin-Cortez U / H / E of one triangle, and the force
+    (Kelvin single-layer) kernels G / S (fullspace/kernels.py:126-215;
+    (mu, lam) -> nu at assemble.py:58-66)."""
     f = Frame(tri)
     nu, lam_d = _material(mu, lam)
     need0 = {}
     for w in want:
-        for n, d in {"U": NEED_U, "H": NEED_H, "E": NEED_E}[w].items():
+        for n, d in {"U": NEED_U, "H": NEED_H, "E": NEED_E, "G": NEED_G, "S": NEED_S}[w].items():
             need0[n] = max(need0.get(n, -1), d)
     W, z = weighted_tables(f, x, eps, P, need0)
     C1 = 1.0 / (16.0 * np.pi * mu * (1.0 - nu))
@@ -491,16 +494,28 @@ def direct(x, tri, P, mu, lam, eps, want):
     n = f.n
     eye = np.eye(3)
     out = {}
-    if "U" in want:
+    if "U" in want or "S" in want:
         V3 = lift(W, z, f, 1, 3)
         V5 = lift(W, z, f, 1, 5)
         T35 = lift(W, z, f, 3, 5)
         G1 = (-c34 * np.einsum("ij,nkm->nkijm", eye, V3) + np.einsum("im,nkj->nkijm", eye, V3)
               + np.einsum("jm,nki->nkijm", eye, V3) - 3.0 * T35
               - 6.0 * (1.0 - nu) * e2 * np.einsum("ij,nkm->nkijm", eye, V5)) * C1
+    if "U" in want:
         out["U"] = -(mu * np.einsum("m,nkijm->nkij", n, G1)
                      + lam_d * np.einsum("j,nkimm->nkij", n, G1)
                      + mu * np.einsum("m,nkimj->nkij", n, G1))
+    if "G" in want:
+        # force density -> displacement: C1 [(3 - 4 nu) I1 delta + T23
+        # + 2 (1 - nu) eps^2 I3 delta]
+        G = (c34 * np.einsum("ij,nk->nkij", eye, W[(1, 0, 0)]) + lift(W, z, f, 2, 3)
+             + 2.0 * (1.0 - nu) * e2 * np.einsum("ij,nk->nkij", eye, W[(3, 0, 0)]))
+        out["G"] = C1 * G
+    if "S" in want:
+        # force density -> stress: S[i, j, c] = C_ijab G1[a, c, b]
+        trG1 = np.einsum("nkaca->nkc", G1)
+        out["S"] = (lam_d * np.einsum("ij,nkc->nkijc", eye, trG1)
+                    + mu * np.einsum("nkicj->nkijc", G1) + mu * np.einsum("nkjci->nkijc", G1))
     if "H" in want:
         I3 = W[(3, 0, 0)]
         I5 = W[(5, 0, 0)]

@@ -52,6 +52,22 @@ void direct_all(const double* obs, int nobs, const double* tri, double mu, doubl
 }
 
 template <int P, int WANT>
+void force_all(const double* obs, int nobs, const double* tri, double mu, double lam, double eps,
+               double near_l, double* G, double* S) {
+  ensure_gl();
+  constexpr int K = n_nodes(P);
+  Frame f;
+  make_frame(tri, f);
+  Rule<P> r12, r8;
+  r12.build(f, cst::FAR_GAUSS_N);
+  r8.build(f, cst::FAR_GAUSS_N_DISTANT);
+  const Material m = make_material(mu, lam);
+  for (int o = 0; o < nobs; ++o)
+    force_eval<P, WANT>(f, r12.q, r8.q, obs + 3 * o, eps, m, G ? G + o * K * 9 : nullptr,
+                        S ? S + o * K * 27 : nullptr, near_l);
+}
+
+template <int P, int WANT>
 void image_r_all(const double* obs, int nobs, const double* tri, double mu, double lam, double eps,
                  double* U, double* H) {
   ensure_gl();
@@ -181,6 +197,15 @@ int hc_direct(int P, int want, const double* obs, int nobs, const double* tri, d
   if (want == W_H) { DISPATCH_P(direct_all, W_H, obs, nobs, tri, mu, lam, eps, U, H, E) }
   if (want == (W_H | W_E)) { DISPATCH_P(direct_all, W_H | W_E, obs, nobs, tri, mu, lam, eps, U, H, E) }
   if (want == W_E) { DISPATCH_P(direct_all, W_E, obs, nobs, tri, mu, lam, eps, U, H, E) }
+  return -2;
+}
+
+// want: 8 = G, 16 = S, 24 = both; near_l: the closed form within near_l L
+int hc_force(int P, int want, const double* obs, int nobs, const double* tri, double mu,
+             double lam, double eps, double near_l, double* G, double* S) {
+  if (want == W_G) { DISPATCH_P(force_all, W_G, obs, nobs, tri, mu, lam, eps, near_l, G, S) }
+  if (want == W_S) { DISPATCH_P(force_all, W_S, obs, nobs, tri, mu, lam, eps, near_l, G, S) }
+  if (want == (W_G | W_S)) { DISPATCH_P(force_all, W_G | W_S, obs, nobs, tri, mu, lam, eps, near_l, G, S) }
   return -2;
 }
 

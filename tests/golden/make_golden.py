@@ -242,10 +242,48 @@ def case_c4_rows():
           rows=rows, n_band=4, n_cols=sn.n, K=K)
 
 
+def case_fullspace():
+    """The full-space single-triangle API (mhs.fullspace.api): nodal influence
+    tensors U, H, E (slip source) and G, S (force source) of two triangles at
+    near and far observers, orders 0-2, hybrid and quadrature far fields, and
+    the contracted calls (displacement, stress, eigenstress,
+    force_displacement, force_stress) for seeded nodal slip and force."""
+    from mhs.fullspace import api
+    rng = np.random.default_rng(21)
+    tris = np.array([[[0.0, 0.0, -1.0], [1.2, 0.2, -1.4], [0.3, 1.1, -0.8]],
+                     [[2.0, -1.0, 0.5], [3.5, -0.6, 1.2], [2.4, 0.8, 0.9]]])
+    obs = np.concatenate([rng.uniform(-1.0, 2.0, (24, 3)), rng.uniform(-40.0, 40.0, (8, 3)),
+                          rng.uniform(-400.0, 400.0, (4, 3))])
+    mu, nu = 30.0, 0.27
+    out = {"tris": tris, "obs": obs, "mu": np.array(mu), "nu": np.array(nu),
+           "eps": np.array([0.1, 0.35])}
+    for t in range(2):
+        for P in (0, 1, 2):
+            K = (P + 1) * (P + 2) // 2
+            for ff in ("hybrid", "quadrature"):
+                inf = api.influence(obs, tris[t], mu, nu, out["eps"][t], order=P,
+                                    want=("U", "H", "E", "G", "S"), far_field=ff)
+                for k in ("U", "H", "E", "G", "S"):
+                    out[f"{k}_{t}_{P}_{ff}"] = getattr(inf, k)
+            slip = rng.standard_normal((K, 3))
+            force = rng.standard_normal((K, 3))
+            e = out["eps"][t]
+            out[f"slip_{t}_{P}"] = slip
+            out[f"force_{t}_{P}"] = force
+            out[f"disp_{t}_{P}"] = api.displacement(obs, tris[t], slip, mu, nu, e)
+            out[f"stress_{t}_{P}"] = api.stress(obs, tris[t], slip, mu, nu, e)
+            out[f"total_{t}_{P}"] = api.stress(obs, tris[t], slip, mu, nu, e,
+                                               subtract_eigenstress=False)
+            out[f"eigen_{t}_{P}"] = api.eigenstress(obs, tris[t], slip, mu, nu, e)
+            out[f"fdisp_{t}_{P}"] = api.force_displacement(obs, tris[t], force, mu, nu, e)
+            out[f"fstress_{t}_{P}"] = api.force_stress(obs, tris[t], force, mu, nu, e)
+    _save("fullspace", **out)
+
+
 CASES = {f.__name__[5:]: f for f in (case_c1_subset, case_orders, case_eps_per_tri,
                                      case_interaction, case_fold, case_continuous,
                                      case_rough_surface, case_signatures, case_c1_full,
-                                     case_c2_rows, case_c4_rows)}
+                                     case_c2_rows, case_c4_rows, case_fullspace)}
 
 if __name__ == "__main__":
     names = sys.argv[1:] or list(CASES)

@@ -169,3 +169,35 @@ def test_fold_finish_form_matches_plain(hc):
         hc.hc_closed_finish(1, _p(pr), ctypes.c_double(h2), _p(bn), _p(b))
         worst = max(worst, np.abs(a[:n] - b[:n]).max() / np.abs(a[:n]).max())
     assert worst < 1e-13
+
+
+@pytest.mark.parametrize("P", [0, 1, 2])
+def test_force_source(hc, P, monkeypatch):
+    """The force (Kelvin single-layer) kernels G and S of the engine against
+    the oracle, with the hybrid split and with quadrature everywhere; and
+    against mhs's own fullspace.influence (golden fixture)."""
+    from conftest import golden
+    c = ctypes.c_double
+    obs = _obs()
+    N, K = obs.shape[0], (P + 1) * (P + 2) // 2
+    for near_l in (10.0, -1.0):
+        monkeypatch.setattr(O, "D_STAR", near_l)
+        ref = O.direct(obs, TRI, P, MU, LAM, EPS, ("G", "S"))
+        G, S = np.zeros((N, K, 3, 3)), np.zeros((N, K, 3, 3, 3))
+        assert hc.hc_force(P, 24, _p(obs), N, _p(TRI.copy()), c(MU), c(LAM), c(EPS), c(near_l),
+                           _p(G), _p(S)) == 0
+        assert relmax(G, ref["G"]) < TOL, near_l
+        assert relmax(S, ref["S"]) < TOL, near_l
+    d = golden("fullspace")
+    mu, nu = float(d["mu"]), float(d["nu"])
+    lam = 2.0 * mu * nu / (1.0 - 2.0 * nu)
+    for t in (0, 1):
+        tri = np.ascontiguousarray(d["tris"][t])
+        o = np.ascontiguousarray(d["obs"])
+        n = o.shape[0]
+        for ff, near_l in (("hybrid", 10.0), ("quadrature", -1.0)):
+            G, S = np.zeros((n, K, 3, 3)), np.zeros((n, K, 3, 3, 3))
+            hc.hc_force(P, 24, _p(o), n, _p(tri), c(mu), c(lam), c(float(d["eps"][t])),
+                        c(near_l), _p(G), _p(S))
+            assert relmax(G, d[f"G_{t}_{P}_{ff}"]) < TOL, (t, ff)
+            assert relmax(S, d[f"S_{t}_{P}_{ff}"]) < TOL, (t, ff)

@@ -53,3 +53,43 @@ def test_request_struct_matches_header_field_order():
         if m:
             flat += [f.strip().lstrip("*") for f in m.group(1).split(",")]
     assert [f[0] for f in _native.Request._fields_] == flat
+
+
+def test_fullspace_struct_matches_header_field_order():
+    from mhs_b200 import _native
+    text = (ROOT / "include" / "mhs_b200.h").read_text()
+    body = text[text.index("typedef struct mhs_fullspace_request"):
+                text.index("} mhs_fullspace_request;")]
+    flat = []
+    for line in body.splitlines():
+        m = re.match(r"\s*(?:const\s+)?[a-z_0-9]+\*?\s+([^;]+);", line.strip() and line or "")
+        if m:
+            flat += [f.strip().lstrip("*").split("[")[0] for f in m.group(1).split(",")]
+    assert [f[0] for f in _native.FullspaceRequest._fields_] == flat
+    assert ctypes.sizeof(_native.FullspaceRequest) == 168
+
+
+def test_fullspace_refusals_before_any_launch():
+    """The full-space API refuses what mhs's refuses, with its messages,
+    before touching a device."""
+    import pytest
+    from mhs_b200 import fullspace as fs
+    tri = np.array([[0.0, 0.0, -1.0], [1.0, 0.0, -1.0], [0.0, 1.0, -1.0]])
+    with pytest.raises(ValueError, match="mu must be > 0"):
+        fs.influence(np.zeros((1, 3)), tri, 0.0, 0.25, 0.1)
+    with pytest.raises(ValueError, match="nu must be in"):
+        fs.influence(np.zeros((1, 3)), tri, 1.0, 0.5, 0.1)
+    with pytest.raises(ValueError, match="eps must be >= 0"):
+        fs.influence(np.zeros((1, 3)), tri, 1.0, 0.25, -0.1)
+    with pytest.raises(ValueError, match="tri must have shape"):
+        fs.influence(np.zeros((1, 3)), tri[:2], 1.0, 0.25, 0.1)
+    with pytest.raises(ValueError, match="degenerate triangle"):
+        fs.influence(np.zeros((1, 3)), np.zeros((3, 3)), 1.0, 0.25, 0.1)
+    with pytest.raises(ValueError, match="slip: 2 nodal values"):
+        fs.displacement(np.zeros((1, 3)), tri, np.zeros((2, 3)), 1.0, 0.25, 0.1)
+    with pytest.raises(ValueError, match="order=1 disagrees"):
+        fs.force_stress(np.zeros((1, 3)), tri, np.zeros((1, 3)), 1.0, 0.25, 0.1, order=1)
+    with pytest.raises(ValueError, match="far_field must be"):
+        fs.influence(np.zeros((1, 3)), tri, 1.0, 0.25, 0.1, far_field="exact")
+    assert np.allclose(fs.nodes(tri, 2)[3], [0.5, 0.0, -1.0])
+    assert np.allclose(fs.traction(np.eye(3), tri), [0.0, 0.0, 1.0])

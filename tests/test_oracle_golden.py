@@ -69,3 +69,21 @@ def test_continuous_traction():
     T = O.traction_matrix(d["obs"], d["obs_normals"], d["tris"], mu, lam, float(d["eps"]), 2,
                           ids=ids, n_dof=n)
     assert relmax(T, d["trac_cont"]) < TOL
+
+
+@pytest.mark.parametrize("t", [0, 1])
+@pytest.mark.parametrize("p", [0, 1, 2])
+def test_fullspace_influence(t, p, monkeypatch):
+    """The oracle's full-space kernels -- slip source U, H, E and force source
+    G, S -- against mhs.fullspace.api.influence, with the hybrid far field
+    and with quadrature everywhere."""
+    d = golden("fullspace")
+    mu, nu = float(d["mu"]), float(d["nu"])
+    lam = 2.0 * mu * nu / (1.0 - 2.0 * nu)
+    eps = float(d["eps"][t])
+    for ff in ("hybrid", "quadrature"):
+        if ff == "quadrature":
+            monkeypatch.setattr(O, "D_STAR", -1.0)
+        got = O.direct(d["obs"], d["tris"][t], p, mu, lam, eps, ("U", "H", "E", "G", "S"))
+        for k in ("U", "H", "E", "G", "S"):
+            assert relmax(got[k], d[f"{k}_{t}_{p}_{ff}"]) < 1e-13, (k, ff)
