@@ -82,6 +82,15 @@ constexpr double PI = 3.141592653589793;
 // The array behind p stays in (local) memory: once its address has passed
 // through an opaque move the compiler can no longer promote the array to
 // registers.  For per-thread arrays too large to live in registers.
+// An int the compiler cannot see through (an opaque move): a loop whose
+// counter passes through it is not unrolled or threaded into its cases.
+MHS_FI int opaque(int v) {
+#if defined(__CUDA_ARCH__)
+  asm volatile("mov.b32 %0, %0;" : "+r"(v));
+#endif
+  return v;
+}
+
 template <class T>
 MHS_FI T* in_memory(T* p) {
 #if defined(__CUDA_ARCH__)
@@ -89,6 +98,16 @@ MHS_FI T* in_memory(T* p) {
 #endif
   return p;
 }
+
+// A table whose entries lie `st` words apart in device memory (the
+// observer index innermost, so one warp's threads touch consecutive words
+// for every entry).  Indexing and offsets count entries, as on a pointer.
+struct StridedTable {
+  double* p;
+  int64_t st;
+  MHS_FI double& operator[](int i) const { return p[(int64_t)i * st]; }
+  MHS_FI StridedTable operator+(int i) const { return {p + (int64_t)i * st, st}; }
+};
 
 constexpr int GL_MAX = cst::IMAGE_Q_GAUSS_MAX;
 // Offset of order n's nodes in the packed 1-D rule table (orders 1..GL_MAX).

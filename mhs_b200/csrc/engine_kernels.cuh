@@ -457,27 +457,6 @@ MHS_HD void contract_ddg(const double* DDG, const double* nrm, const Material& m
 }
 
 // --------------------------------------------------------- image R-family
-// Cartesian monomial moment mi, D1^a D2^b D3^c / R2^n, of one node from the
-// basis products G and the weighted table W (mhs/kernels/image.py:456-480):
-// sum over t of (-1)^t zp^(r - t) sum_al G[al, t - al] W_n[al, t - al].
-template <class S>
-MHS_FI double r_moment(int mi, const double* G, const double* W, const double* zpow) {
-  constexpr Spec sp = S::spec;
-  const int a = MHS_TAB(mhs_r_mono)[mi][0], b = MHS_TAB(mhs_r_mono)[mi][1],
-            c = MHS_TAB(mhs_r_mono)[mi][2], n = MHS_TAB(mhs_r_mono)[mi][3];
-  const int r = a + b + c;
-  const double* g = G + g_off(a, b, c);
-  const double* Wn = W + sp.w_off[nslot(n)];
-  double acc = 0.0;
-  for (int t = 0; t <= r; ++t) {
-    double part = 0.0;
-    for (int al = 0; al <= t; ++al) part += g[tri_idx(al, t - al)] * Wn[tri_idx(al, t - al)];
-    const double v = zpow[r - t] * part;
-    acc += (t & 1) ? -v : v;
-  }
-  return acc;
-}
-
 // The records of one node: the monomial moments in monomial order, each
 // followed by its own records (sorted by monomial, so every slot receives
 // its records in table order) with coefficient c(z) = c0 + z (c1 + z c2) at
@@ -486,10 +465,8 @@ MHS_FI double r_moment(int mi, const double* G, const double* W, const double* z
 // traction-operator image S[i][p][k] (27 entries, as 9 i + 3 p + k): record
 // slot (i, a, p, b) adds mun[b] v to S[i][p][a], mun[a] v to S[i][p][b] and,
 // when a = b, lamn[k] v to every S[i][p][k] (mun = mu n, lamn = lam n; the
-// scale is already in the coefficients).  The monomial loop runs at run
-// time and dispatches to one case per monomial whose records are straight-
-// line code with literal slots, so only the moment and the 27 accumulators
-// are live and nothing is addressed at run time but the tables.
+// scale is already in the coefficients).  One instantiation per monomial:
+// its records are straight-line code with literal slots.
 template <class S, int WANT, int MI>
 MHS_FI void r_mono_records(double tm, double zo, const ImageCoef& ic, double* D,
                            const double* mun, const double* lamn) {
@@ -521,17 +498,49 @@ MHS_FI void r_mono_records(double tm, double zo, const ImageCoef& ic, double* D,
   }
 }
 
-template <class S, int WANT>
-MHS_FI void image_r_records(const double* G, const double* W, const double* zpow, double zo,
+// Cartesian monomial moment D1^A D2^B D3^C / R2^N of one node from the
+// basis products G and the node's weighted table Wr (mhs/kernels/image.py:
+// 456-480): sum over t of (-1)^t zp^(r - t) sum_al G[al, t - al]
+// W_N[al, t - al], with every exponent and table index known at compile time.
+template <class S, int A, int B, int C, int N>
+MHS_FI double r_moment_ct(const double* G, const double* Wr, const double (&zpow)[G_RMAX + 1]) {
+  constexpr Spec sp = S::spec;
+  constexpr int r = A + B + C;
+  constexpr int wo = sp.w_off[nslot(N)];
+  const double* g = G + g_off(A, B, C);
+  double acc = 0.0;
+#pragma unroll
+  for (int t = 0; t <= r; ++t) {
+    double part = 0.0;
+#pragma unroll
+    for (int al = 0; al <= t; ++al) part += g[tri_idx(al, t - al)] * Wr[wo + tri_idx(al, t - al)];
+    const double v = zpow[r - t] * part;
+    acc += (t & 1) ? -v : v;
+  }
+  return acc;
+}
+
+// The records of one node.  The node's table is read once into registers;
+// the monomial loop runs at run time (its counter opaque, so the compiler
+// neither unrolls it nor threads it into its cases) and dispatches to one
+// case per monomial whose moment and records are straight-line code with
+// literal indices: only the table, the 27 sums and the moment are live, and
+// nothing is addressed at run time but the shared tables.
+template <class S, int WANT, class WT>
+MHS_FI void image_r_records(const double* G, WT W, const double (&zpow)[G_RMAX + 1], double zo,
                             const ImageCoef& ic, double* D, const double* mun,
                             const double* lamn) {
+  constexpr int NW = S::spec.w_off[NS];
+  double Wr[NW];
+#pragma unroll
+  for (int j = 0; j < NW; ++j) Wr[j] = W[j];
 #pragma unroll 1
-  for (int mi = 0; mi < MHS_R_NMONO; ++mi) {
-    const double tm = r_moment<S>(mi, G, W, zpow);
-    switch (mi) {
-#define MHS_RCASE(mi_, a, b, c, n)                                  \
-  case mi_:                                                         \
-    r_mono_records<S, WANT, mi_>(tm, zo, ic, D, mun, lamn);         \
+  for (int i = 0; i < MHS_R_NMONO; ++i) {
+    switch (opaque(i)) {
+#define MHS_RCASE(mi_, a, b, c, n)                                                       \
+  case mi_:                                                                              \
+    r_mono_records<S, WANT, mi_>(r_moment_ct<S, a, b, c, n>(G, Wr, zpow), zo, ic, D, mun, \
+                                 lamn);                                                  \
     break;
       MHS_R_MONO(MHS_RCASE)
 #undef MHS_RCASE
@@ -541,9 +550,100 @@ MHS_FI void image_r_records(const double* G, const double* W, const double* zpow
   }
 }
 
+// Powers zp^0..zp^G_RMAX of the observer's height over the reflected
+// element's plane (the moments' sign-alternating z factors).
+MHS_FI void image_r_zpow(const Frame& fi, const double* x, double (&zpow)[G_RMAX + 1]) {
+  double zp, X0, X1;
+  to_plane(fi, x, zp, X0, X1);
+  zpow[0] = 1.0;
+  for (int i = 1; i <= G_RMAX; ++i) zpow[i] = zpow[i - 1] * zp;
+}
+
+// Weighted tables of the image frame for every node k, written to
+// Wall + k NW (a pointer or a StridedTable): the closed form within near_l
+// element lengths (every node's table from one moment table), else the
+// 12 x 12 / 8 x 8 far rules, one pass per node.  PART restricts the call
+// to the observers of one form (TAB_CLOSED, TAB_FAR; others are left
+// untouched), so that each form can run in its own kernel with its own
+// registers.
+enum : int { TAB_BOTH = 0, TAB_CLOSED = 1, TAB_FAR = 2 };
+
+template <int P, class R_FAR = double, int PART = TAB_BOTH, class Q = QuadRule,
+          class WO = double*>
+MHS_HD void image_r_tables(const Frame& fi, const Q& r12, const Q& r8, const double* x,
+                           double eps, WO Wall, double near_l = cst::D_STAR,
+                           double far_switch_l = cst::D_STAR_DISTANT) {
+  using S = SpecImg<P>;
+  constexpr int K = n_nodes(P);
+  constexpr int NW = S::spec.w_off[NS];
+  const double d0 = x[0] - fi.c[0], d1 = x[1] - fi.c[1], d2 = x[2] - fi.c[2];
+  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
+  const bool closed = D <= near_l * fi.L;
+  if ((PART == TAB_CLOSED && !closed) || (PART == TAB_FAR && closed)) return;
+  double zp, X0, X1;
+  to_plane(fi, x, zp, X0, X1);
+  const double h2 = zp * zp + eps * eps;
+  if constexpr (PART != TAB_FAR) {
+    if (closed) {
+      MomentTable<S> T;
+      closed_moments<S>(fi, X0, X1, h2, T);
+      double c[K][ntri(P)];
+      shape_coeffs<P>(fi, X0, X1, c);
+      for (int k = 0; k < K; ++k) weight_closed<S, P>(T, c, k, Wall + k * NW);
+      return;
+    }
+  }
+  if constexpr (PART != TAB_CLOSED) {
+    const Q& q = (D > far_switch_l * fi.L) ? r8 : r12;
+    if constexpr (K == 1 || PART == TAB_BOTH) {
+      weight_far<S, P, R_FAR>(q, X0, X1, h2, Wall);
+    } else {
+      // one pass per node (as weight_far makes them: NW accumulators are
+      // a pass's limit), kept as a loop so that only one pass is live
+#pragma unroll 1
+      for (int k = 0; k < K; ++k) {
+        const int kk = opaque(k);
+        weight_far_nodes<S, P, R_FAR, 1>(q, R_FAR(X0), R_FAR(X1), R_FAR(h2), kk, kk, Wall);
+      }
+    }
+  }
+}
+static_assert(FAR_ACC_MAX / SpecImg<1>::spec.w_off[NS] == 1 &&
+                  FAR_ACC_MAX / SpecImg<2>::spec.w_off[NS] == 1,
+              "the image tables' far passes take one node each");
+
+// The records of one node from its weighted table W (a pointer or a
+// StridedTable), contracted into the node's displacement (U, 9 entries) or
+// total-stress (H, 27 entries) influence.
+template <int P, int WANT, class WT>
+MHS_FI void image_r_node(const double* G, WT W, const double (&zpow)[G_RMAX + 1], double zo,
+                         const double* nrm, const Material& m, const ImageCoef& ic, double* U,
+                         double* H) {
+  using S = SpecImg<P>;
+  const double mun[3] = {m.mu * nrm[0], m.mu * nrm[1], m.mu * nrm[2]};
+  const double lamn[3] = {m.lam * nrm[0], m.lam * nrm[1], m.lam * nrm[2]};
+  if constexpr ((WANT & W_U) != 0) {
+    double DG[27] = {};
+    image_r_records<S, W_U>(G, W, zpow, zo, ic, DG, mun, lamn);
+    contract_dg(DG, nrm, m, U);
+  }
+  if constexpr ((WANT & W_H) != 0) {
+    double Sf[27] = {};
+    image_r_records<S, W_H>(G, W, zpow, zo, ic, Sf, mun, lamn);
+    double St[3][3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int p = 0; p < 3; ++p)
+        for (int c = 0; c < 3; ++c) St[i][p][c] = Sf[9 * i + 3 * p + c];
+    hooke_from_traction(St, m, H);
+  }
+}
+
 // The closed-form R-family on the reflected element (mhs/kernels/image.py:
 // 435-497): weighted tables of the image frame, Cartesian monomial moments
 // D1^a D2^b D3^c / R2^n from the basis products G, then the generated records.
+// The device pipeline runs the two halves as separate kernels over a table
+// buffer (image_r_tables, image_r_node); this composition serves the
+// single-point paths.
 template <int P, int WANT, class R_FAR = double, class Q = QuadRule>
 MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
                          const Q& r12, const Q& r8, const double* x, double eps,
@@ -551,54 +651,17 @@ MHS_HD void image_r_eval(const Frame& fi, const double* G, const double* nrm,
                          double near_l = cst::D_STAR,
                          double far_switch_l = cst::D_STAR_DISTANT) {
   using S = SpecImg<P>;
-  constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
-  constexpr int NW = sp.w_off[NS];
-  const double d0 = x[0] - fi.c[0], d1 = x[1] - fi.c[1], d2 = x[2] - fi.c[2];
-  const double D = sqrt(((d0 * d0 + d1 * d1) + d2 * d2) + eps * eps);
-  double zp, X0, X1;
-  to_plane(fi, x, zp, X0, X1);
-  const double h2 = zp * zp + eps * eps;
-  const double zo = x[2];   // absolute depth of the observer
+  constexpr int NW = S::spec.w_off[NS];
   double zpow[G_RMAX + 1];
-  zpow[0] = 1.0;
-  for (int i = 1; i <= G_RMAX; ++i) zpow[i] = zpow[i - 1] * zp;
-  // The closed form's tables of every node come from one moment table, so
-  // they are formed together; the far field forms each node's table by its
-  // own pass over the rule just before that node's records (at P >= 1 only
-  // one node's table is live then).
-  const bool closed = D <= near_l * fi.L;
-  double Wbuf[(P > 0 ? K : 1) * NW] = {};
+  image_r_zpow(fi, x, zpow);
+  double Wbuf[K * NW];
   double* Wall = P > 0 ? in_memory(Wbuf) : Wbuf;
-  if (closed) {
-    MomentTable<S> T;
-    closed_moments<S>(fi, X0, X1, h2, T);
-    double c[K][ntri(P)];
-    shape_coeffs<P>(fi, X0, X1, c);
-    for (int k = 0; k < K; ++k) weight_closed<S, P>(T, c, k, Wall + k * NW);
-  }
-  const Q& q = (D > far_switch_l * fi.L) ? r8 : r12;
-  const double mun[3] = {m.mu * nrm[0], m.mu * nrm[1], m.mu * nrm[2]};
-  const double lamn[3] = {m.lam * nrm[0], m.lam * nrm[1], m.lam * nrm[2]};
+  image_r_tables<P, R_FAR>(fi, r12, r8, x, eps, Wall, near_l, far_switch_l);
 #pragma unroll 1
-  for (int k = 0; k < K; ++k) {
-    double* W = Wall + (closed ? k * NW : 0);
-    if (!closed) weight_far_nodes<S, P, R_FAR, 1>(q, R_FAR(X0), R_FAR(X1), R_FAR(h2), k, 0, W);
-    if constexpr ((WANT & W_U) != 0) {
-      double DG[27] = {};
-      image_r_records<S, W_U>(G, W, zpow, zo, ic, DG, mun, lamn);
-      contract_dg(DG, nrm, m, U + 9 * k);
-    }
-    if constexpr ((WANT & W_H) != 0) {
-      double Sf[27] = {};
-      image_r_records<S, W_H>(G, W, zpow, zo, ic, Sf, mun, lamn);
-      double St[3][3][3];
-      for (int i = 0; i < 3; ++i)
-        for (int p = 0; p < 3; ++p)
-          for (int c = 0; c < 3; ++c) St[i][p][c] = Sf[9 * i + 3 * p + c];
-      hooke_from_traction(St, m, H + 27 * k);
-    }
-  }
+  for (int k = 0; k < K; ++k)
+    image_r_node<P, WANT>(G, Wall + k * NW, zpow, x[2], nrm, m, ic, U ? U + 9 * k : nullptr,
+                          H ? H + 27 * k : nullptr);
 }
 
 // --------------------------------------------------------- image Q-family

@@ -528,7 +528,7 @@ MHS_FI void recur_slot(const double* BN1, const double* BN2, MomentTable<S>& T) 
 // seeds' divisions by n h^2 as products with 1/h^2 (rounding-level
 // differences).
 template <class S, bool FAST>
-MHS_FI void closed_finish_t(const double pr[3][2], double h2, const double* BN1, const double* BN2,
+MHS_HD void closed_finish_t(const double pr[3][2], double h2, const double* BN1, const double* BN2,
                             const double* BD, MomentTable<S>& T) {
   constexpr Spec sp = S::spec;
   double h, I3, ih2 = 0.0;
@@ -575,8 +575,8 @@ MHS_HD void closed_moments(const Frame& f, double X0, double X1, double h2, Mome
 
 // W_k[n](a, b) = sum_{a'+b'<=P} c_k(a', b') M_n(a + a', b + b'), at the
 // constant-slip degrees (mhs/fullspace/moments.py:370-398).
-template <class S, int P, int s>
-MHS_FI void weight_slot(const MomentTable<S>& T, const double c[][ntri(P)], int k, double* W) {
+template <class S, int P, int s, class WO>
+MHS_FI void weight_slot(const MomentTable<S>& T, const double c[][ntri(P)], int k, WO W) {
   constexpr Spec sp = S::spec;
   if constexpr (s < NS) {
     constexpr int d = sp.need0[s];
@@ -598,8 +598,9 @@ MHS_FI void weight_slot(const MomentTable<S>& T, const double c[][ntri(P)], int 
   }
 }
 
-template <class S, int P>
-MHS_FI void weight_closed(const MomentTable<S>& T, const double c[][ntri(P)], int k, double* W) {
+// W is a pointer or a StridedTable.
+template <class S, int P, class WO = double*>
+MHS_FI void weight_closed(const MomentTable<S>& T, const double c[][ntri(P)], int k, WO W) {
   weight_slot<S, P, 0>(T, c, k, W);
 }
 
@@ -648,8 +649,8 @@ MHS_HD void build_rule(const Frame& f, const double* glx, const double* glw, int
 // weight_far_nodes evaluates nodes [k0, k0 + KG) into tables out0, out0 + 1,
 // ... of Wout: every accumulator adds its point terms in rule order,
 // whichever group of nodes it is taken with.
-template <class S, int P, class R, int KG, class Q>
-MHS_HD void weight_far_nodes(const Q& q, R x0, R x1, R hh, int k0, int out0, double* Wout) {
+template <class S, int P, class R, int KG, class Q, class WO>
+MHS_HD void weight_far_nodes(const Q& q, R x0, R x1, R hh, int k0, int out0, WO Wout) {
   constexpr Spec sp = S::spec;
   constexpr int K = n_nodes(P);
   constexpr int NW = sp.w_off[NS];
@@ -717,8 +718,8 @@ MHS_HD void weight_far_nodes(const Q& q, R x0, R x1, R hh, int k0, int out0, dou
 // the per-point powers and leaves every sum's order unchanged.
 constexpr int FAR_ACC_MAX = 64;
 
-template <class S, int P, class R, int K0, class Q>
-MHS_HD void weight_far_from(const Q& q, R x0, R x1, R hh, double* Wout) {
+template <class S, int P, class R, int K0, class Q, class WO>
+MHS_HD void weight_far_from(const Q& q, R x0, R x1, R hh, WO Wout) {
   constexpr int K = n_nodes(P);
   constexpr int NW = S::spec.w_off[NS];
   constexpr int KG0 = FAR_ACC_MAX / NW > 0 ? FAR_ACC_MAX / NW : 1;
@@ -727,8 +728,8 @@ MHS_HD void weight_far_from(const Q& q, R x0, R x1, R hh, double* Wout) {
   if constexpr (K0 + KG < K) weight_far_from<S, P, R, K0 + KG>(q, x0, x1, hh, Wout);
 }
 
-template <class S, int P, class R, class Q = QuadRule>
-MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, double* Wout) {
+template <class S, int P, class R, class Q = QuadRule, class WO = double*>
+MHS_HD void weight_far(const Q& q, double X0, double X1, double h2, WO Wout) {
   weight_far_from<S, P, R, 0>(q, R(X0), R(X1), R(h2), Wout);
 }
 

@@ -245,13 +245,62 @@ k_pair(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nre
   }
 }
 
-// --------------------------------------------------------------- k_image_r
+// ------------------------------------------------- k_image_w, k_image_r
 // Image R-family of one (observer, source) pair outside the source's fold
-// band (the fold replaces it there), added to the pair's row.
-template <int P, int KC, class RF>
+// band (the fold replaces it there), in two kernels over the request's
+// table buffer Wimg[s][k][j][oc] (observer innermost): k_image_w forms the
+// image frame's weighted tables of every node (one launch for the pairs in
+// closed-form range, one for the far rules), k_image_r reads them back,
+// runs the generated records and adds the result to the pair's row.  Apart,
+// each kernel keeps its own working set in registers: the moment table, the
+// far rule's accumulators or the records' 27 sums.
+template <int P>
+__device__ __forceinline__ StridedTable image_table(const ReqDesc& d, int64_t s, int k,
+                                                    int64_t oc) {
+  const int64_t n_chunk = d.fa.n_chunk;
+  return {d.Wimg + ((s * n_nodes(P) + k) * IMG_NW) * n_chunk + oc, n_chunk};
+}
+
+template <int P, int KC, class RF, int PART>
 __global__ void __launch_bounds__(TB)
-k_image_r(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq,
+k_image_w(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq,
           double near_l_mixed) {
+  static_assert(KC != KD_E, "the eigenstress readout has no image term");
+  const int r = find_req(off, nreq, blockIdx.x);
+  const ReqDesc& d = D[r];
+  const int64_t lo = d.fa.lo, n_chunk = d.fa.n_chunk, n_src = d.fa.n_src;
+  const long long local = blockIdx.x - off[r];
+  const int64_t s = local % n_src, tile = local / n_src;
+  constexpr bool F32 = std::is_same<RF, float>::value;
+  // far rules of the reflected element
+  __shared__ SrcPrep sp;
+  __shared__ std::conditional_t<F32, NoRules, SmemRules<P>> ri;
+  __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rif;
+  if (threadIdx.x == 0) sp = d.prep[s];
+  __syncthreads();
+  if constexpr (PART != TAB_CLOSED) {
+    if constexpr (F32) build_float_rules<P>(sp.fi, rif, threadIdx.x, blockDim.x);
+    else ri.build(sp.fi, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
+  const int64_t oc = tile * (int64_t)blockDim.x + threadIdx.x;
+  if (oc >= n_chunk) return;
+  const int64_t o = lo + oc;
+  const double x[3] = {d.obs[3 * o], d.obs[3 * o + 1], d.obs[3 * o + 2]};
+  const double eps = sp.eps;
+  if (sp.straddle && fold_band(x, sp.centre, eps)) return;
+  const StridedTable W = image_table<P>(d, s, 0, oc);
+  if constexpr (F32) {
+    const QuadRuleT<float> i12 = float_rule_mid<P>(rif), i8 = float_rule_far<P>(rif);
+    image_r_tables<P, float, PART>(sp.fi, i12, i8, x, eps, W, near_l_mixed, cst::D_STAR);
+  } else {
+    image_r_tables<P, double, PART>(sp.fi, ri.r12(), ri.r8(), x, eps, W);
+  }
+}
+
+template <int P, int KC>
+__global__ void __launch_bounds__(TB)
+k_image_r(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int nreq) {
   static_assert(KC != KD_E, "the eigenstress readout has no image term");
   constexpr int K = n_nodes(P);
   constexpr int NR = row_of(KC);
@@ -261,62 +310,38 @@ k_image_r(const ReqDesc* __restrict__ D, const long long* __restrict__ off, int 
   const int64_t lo = d.fa.lo, n_chunk = d.fa.n_chunk, n_src = d.fa.n_src;
   const long long local = blockIdx.x - off[r];
   const int64_t s = local % n_src, tile = local / n_src;
-  const double* __restrict__ obs = d.obs;
-  const SrcPrep* __restrict__ prep = d.prep;
-  const double* __restrict__ Gall = d.G;
-  const double* __restrict__ coef = d.coef;
-  const double mu = d.fa.mu, lam = d.fa.lam;
-  double* __restrict__ T = d.T;
-  constexpr bool F32 = std::is_same<RF, float>::value;
-  // far rules of the reflected element, its basis products, and the
-  // R-family coefficients of the request's material (read record by record,
-  // K times per pair)
-  constexpr bool STAGE_RC = true;
+  // the source's basis products and the R-family coefficients of the
+  // request's material (read record by record, K times per pair)
   __shared__ SrcPrep sp;
-  __shared__ std::conditional_t<F32, NoRules, SmemRules<P>> ri;
-  __shared__ std::conditional_t<F32, FloatRules<P>, NoRules> rif;
   __shared__ double sG[G_SIZE];
-  __shared__ double sRc[STAGE_RC ? 3 * (MHS_R_NDG + MHS_R_NDDG) : 1];
-  if (threadIdx.x == 0) sp = prep[s];
+  __shared__ double sRc[3 * (MHS_R_NDG + MHS_R_NDDG)];
+  if (threadIdx.x == 0) sp = d.prep[s];
+  for (int i = threadIdx.x; i < G_SIZE; i += blockDim.x) sG[i] = d.G[s * G_SIZE + i];
+  for (int i = threadIdx.x; i < 3 * (MHS_R_NDG + MHS_R_NDDG); i += blockDim.x) sRc[i] = d.coef[i];
   __syncthreads();
-  if constexpr (F32) build_float_rules<P>(sp.fi, rif, threadIdx.x, blockDim.x);
-  else ri.build(sp.fi, threadIdx.x, blockDim.x);
-  for (int i = threadIdx.x; i < G_SIZE; i += blockDim.x) sG[i] = Gall[s * G_SIZE + i];
-  if (STAGE_RC)
-    for (int i = threadIdx.x; i < 3 * (MHS_R_NDG + MHS_R_NDDG); i += blockDim.x) sRc[i] = coef[i];
-  __syncthreads();
-  const double near_l = F32 ? near_l_mixed : cst::D_STAR;
   const int64_t oc = tile * (int64_t)blockDim.x + threadIdx.x;
   if (oc >= n_chunk) return;
   const int64_t o = lo + oc;
-  const double x[3] = {obs[3 * o], obs[3 * o + 1], obs[3 * o + 2]};
-  const double eps = sp.eps;
-  if (sp.straddle && fold_band(x, sp.centre, eps)) return;
-  const Material m = make_material(mu, lam);
-  double Bbuf[K * C] = {};
-  double* B = P > 0 ? in_memory(Bbuf) : Bbuf;
-  ImageCoef ic = image_coef_view(coef);
-  if (STAGE_RC) {
-    ic.r_dg = sRc;
-    ic.r_ddg = sRc + 3 * MHS_R_NDG;
-  }
-  if constexpr (F32) {
-    const QuadRuleT<float> i12 = float_rule_mid<P>(rif), i8 = float_rule_far<P>(rif);
+  const double x[3] = {d.obs[3 * o], d.obs[3 * o + 1], d.obs[3 * o + 2]};
+  if (sp.straddle && fold_band(x, sp.centre, sp.eps)) return;
+  const Material m = make_material(d.fa.mu, d.fa.lam);
+  ImageCoef ic = image_coef_view(d.coef);
+  ic.r_dg = sRc;
+  ic.r_ddg = sRc + 3 * MHS_R_NDG;
+  double zpow[G_RMAX + 1];
+  image_r_zpow(sp.fi, x, zpow);
+  double* row = d.T + ((oc * n_src + s) * K) * NR;
+#pragma unroll 1
+  for (int k = 0; k < K; ++k) {
+    double B[C];
     if constexpr (KC == KD_DISP)
-      image_r_eval<P, W_U, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, B, nullptr, near_l,
-                                  cst::D_STAR);
+      image_r_node<P, W_U>(sG, image_table<P>(d, s, k, oc), zpow, x[2], sp.f.n, m, ic, B,
+                           nullptr);
     else
-      image_r_eval<P, W_H, float>(sp.fi, sG, sp.f.n, i12, i8, x, eps, m, ic, nullptr, B, near_l,
-                                  cst::D_STAR);
-  } else {
-    if constexpr (KC == KD_DISP)
-      image_r_eval<P, W_U>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, B, nullptr);
-    else
-      image_r_eval<P, W_H>(sp.fi, sG, sp.f.n, ri.r12(), ri.r8(), x, eps, m, ic, nullptr, B);
+      image_r_node<P, W_H>(sG, image_table<P>(d, s, k, oc), zpow, x[2], sp.f.n, m, ic, nullptr,
+                           B);
+    for (int c = 0; c < C; ++c) row[k * NR + c] += B[c];
   }
-  double* row = T + ((oc * n_src + s) * K) * NR;
-  for (int k = 0; k < K; ++k)
-    for (int c = 0; c < C; ++c) row[k * NR + c] += B[k * C + c];
 }
 
 // -------------------------------------------------------------- k_imageq
@@ -761,6 +786,7 @@ void fill_desc(const Pass& p, ReqDesc& d) {
   d.G = (double*)(ws + p.L->G);
   d.coef = (double*)(ws + p.L->coef);
   d.T = (double*)(ws + p.L->T);
+  d.Wimg = (double*)(ws + p.L->Wimg);
   d.status = (int*)(ws + p.L->status);
   d.fold = r->fold;
   d.pad = 0;
@@ -817,9 +843,12 @@ int run_passes(const Pass* ps, int n, void* desc, bool upload, cudaStream_t st,
     }
     if constexpr (KC != KD_E) {
       StageTimer ti(MHS_STAGE_PAIR_IMAGE_R, st);
-      k_image_r<P, KC, RF><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(
+      k_image_w<P, KC, RF, TAB_CLOSED><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(
           D, offs(OFF_PAIR), n, MIXED_NEAR_L);
-      count_kernels(1);
+      k_image_w<P, KC, RF, TAB_FAR><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(
+          D, offs(OFF_PAIR), n, MIXED_NEAR_L);
+      k_image_r<P, KC><<<(unsigned)total(OFF_PAIR), tune.pair_tb, 0, st>>>(D, offs(OFF_PAIR), n);
+      count_kernels(3);
     }
   }
   if constexpr (KC != KD_E) {
@@ -988,8 +1017,9 @@ int debug_terms(int term, int want_u, int n, const double* obs, const double* tr
 struct FsTri {
   double v[9];
 };
-static_assert(MHS_FS_U == W_U && MHS_FS_H == W_H && MHS_FS_E == W_E && MHS_FS_G == W_G &&
-                  MHS_FS_S == W_S,
+static_assert(int(MHS_FS_U) == int(W_U) && int(MHS_FS_H) == int(W_H) &&
+                  int(MHS_FS_E) == int(W_E) && int(MHS_FS_G) == int(W_G) &&
+                  int(MHS_FS_S) == int(W_S),
               "the ABI's kernel flags are the engine's");
 
 template <int P>

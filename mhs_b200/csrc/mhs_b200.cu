@@ -214,7 +214,9 @@ Layout fit_layout(const mhs_request* r, size_t bytes) {
   return plan(r, lo, fb);
 }
 
-constexpr size_t GOOD_T_BYTES = size_t(2) << 30;
+// Per-chunk pair tables (the pair table and the image tables) of the good
+// workspace size: the 2,400-triangle interaction fits in one chunk.
+constexpr size_t GOOD_T_BYTES = size_t(4) << 30;
 
 // ------------------------------------------- allocation-free scratch
 // Scratch of mhs_assemble_noalloc: one file-scope device array that every

@@ -100,6 +100,7 @@ struct ReqDesc {
   double* G;
   double* coef;
   double* T;
+  double* Wimg;   // the image R-family's weighted tables per pair and node
   int* status;
   int fold, pad;
 };
@@ -136,9 +137,15 @@ struct Tune {
 // Workspace carve-up for a chunk of `chunk` observers plus `fold_bytes`
 // for the fold's plan, pair batches and node waves.
 struct Layout {
-  size_t status, desc, coef, prep, G, cnt, list, T, fold, fold_bytes, total;
+  size_t status, desc, coef, prep, G, cnt, list, T, Wimg, fold, fold_bytes, total;
   int64_t chunk;
 };
+
+// Weighted-table entries per node of the image R-family (the same at every
+// order: its spec's constant-slip degrees do not depend on the order).
+constexpr int IMG_NW = SpecImg<0>::spec.w_off[NS];
+static_assert(IMG_NW == SpecImg<1>::spec.w_off[NS] && IMG_NW == SpecImg<2>::spec.w_off[NS],
+              "image tables per node independent of the order");
 
 inline Layout plan(const mhs_request* r, int64_t chunk, size_t fold_bytes = 0) {
   const int kc = kind_class(r->kind);
@@ -154,6 +161,8 @@ inline Layout plan(const mhs_request* r, int64_t chunk, size_t fold_bytes = 0) {
   L.cnt = off; off = align_up(off + sizeof(int) * (size_t)r->n_src);
   L.list = off; off = align_up(off + sizeof(int) * (size_t)r->n_src * (size_t)chunk);
   L.T = off; off = align_up(off + sizeof(double) * (size_t)chunk * r->n_src * K * row_of(kc));
+  L.Wimg = off;
+  if (kc != KD_E) off = align_up(off + sizeof(double) * (size_t)chunk * r->n_src * K * IMG_NW);
   L.fold = off; off = align_up(off + fold_bytes);
   L.fold_bytes = fold_bytes;
   L.total = off;
