@@ -56,13 +56,12 @@ def test_small_workspace_chunks_equal_one_chunk(cuda, order):
     assert nbytes < good.value
     ws = torch.empty(nbytes, dtype=torch.uint8, device=cuda)
     r.workspace, r.workspace_bytes = ctypes.c_void_p(ws.data_ptr()), nbytes
-    n0 = _native.kernel_count()
+    _native.kernel_count()                                   # the count resets on reading
     assert lib.mhs_assemble(ctypes.byref(r), None) == 0, lib.mhs_last_error()
-    n_small = _native.kernel_count() - n0
-    n0 = _native.kernel_count()
+    n_small = _native.kernel_count()
     m.stress_matrix(obs, tris, mat, eps, order=order)
-    n_one = _native.kernel_count() - n0
-    assert n_small > 4 * n_one // 2, (n_small, n_one)      # several chunks ran
+    n_one = _native.kernel_count()
+    assert n_small > 2 * n_one, (n_small, n_one)              # several chunks ran
     bits = ctypes.c_int(-1)
     assert lib.mhs_read_status(ctypes.c_void_p(ws.data_ptr()), None, ctypes.byref(bits)) == 0
     assert bits.value == 0
