@@ -524,11 +524,17 @@ k_scatter(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls, int* __
       if (cls[k] >= 0 && lane == __ffs(mk[k]) - 1) w_cnt[k][wid][cls[k]] = __popc(mk[k]);
     }
     __syncthreads();
+    // per class, the counts become exclusive prefixes in (sub-tile, warp)
+    // order, and the block's run of the class list is claimed
     if (threadIdx.x < NCLS) {
       const int c = threadIdx.x;
       int tot = 0;
       for (int k = 0; k < SCAT_PER_THREAD; ++k)
-        for (int w = 0; w < nw; ++w) tot += w_cnt[k][w][c];
+        for (int w = 0; w < nw; ++w) {
+          const int v = w_cnt[k][w][c];
+          w_cnt[k][w][c] = tot;
+          tot += v;
+        }
       b_base[c] = tot ? atomicAdd(&hdr->cls_fill[c], tot) : 0;
     }
     __syncthreads();
@@ -536,11 +542,7 @@ k_scatter(Hdr* __restrict__ hdr, const unsigned char* __restrict__ ncls, int* __
     for (int k = 0; k < SCAT_PER_THREAD; ++k) {
       const int c = cls[k];
       if (c >= 0) {
-        int off = b_base[c];
-        for (int kk = 0; kk < k; ++kk)
-          for (int w = 0; w < nw; ++w) off += w_cnt[kk][w][c];
-        for (int w = 0; w < wid; ++w) off += w_cnt[k][w][c];
-        off += __popc(mk[k] & ((1u << lane) - 1u));
+        const int off = b_base[c] + w_cnt[k][wid][c] + __popc(mk[k] & ((1u << lane) - 1u));
         const long long u = t0 + (long long)k * blockDim.x + threadIdx.x;
         nlist[hdr->cls_off[c] + off] = (int)u;
       }
