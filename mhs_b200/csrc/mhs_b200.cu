@@ -475,7 +475,7 @@ int mhs_batch_pass_bytes(const mhs_request* r, size_t* bytes, size_t* limit) {
   q.workspace_bytes = 0;
   int rc = check_request(&q);
   if (rc) return rc;
-  *bytes = plan(&q, q.n_obs, fold_good_bytes(&q)).total;
+  *bytes = plan(&q, q.n_obs, fold_good_bytes(&q, FOLD_BATCH_BYTES)).total;
   if (limit) *limit = BATCH_PASS_MAX;
   return MHS_OK;
 }
@@ -495,7 +495,7 @@ int mhs_batch_create(const mhs_request* reqs, int n, mhs_batch** out) {
       snprintf(msg, sizeof(msg), "%s", mhs_last_error());
       return fail(rc, "batch request %d: %s", i, msg);
     }
-    const Layout L = plan(&r, r.n_obs, fold_good_bytes(&r));
+    const Layout L = plan(&r, r.n_obs, fold_good_bytes(&r, FOLD_BATCH_BYTES));
     if (L.total > BATCH_PASS_MAX)
       return fail(MHS_ERR_WORKSPACE, "batch request %d needs %zu bytes of scratch for one pass, "
                   "above the batch limit of %zu; assemble it alone", i, L.total, BATCH_PASS_MAX);

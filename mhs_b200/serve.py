@@ -71,6 +71,9 @@ class Server:
         self.t_first = None
         self.t_last = None
         self.cv = threading.Condition(threading.RLock())
+        self.outstanding = 0         # submitted requests whose futures are not settled
+        self.oom_wait = False        # admissions wait for a completion (allocator out of memory)
+        self.oom_retries = 0
         self.running = True
         self.error = None
         self.thread = threading.Thread(target=self._loop, name="mhs-serve", daemon=True)
@@ -96,9 +99,16 @@ class Server:
         with self.cv:
             if self.t_first is None:
                 self.t_first = t0
+            self.outstanding += 1
             self.queue.append((pend, fut, t0))
             self.cv.notify()
+        fut.add_done_callback(self._settled)
         return fut
+
+    def _settled(self, fut) -> None:
+        with self.cv:
+            self.outstanding -= 1
+            self.cv.notify_all()
 
     def close(self) -> None:
         with self.cv:
@@ -113,9 +123,10 @@ class Server:
         self.close()
 
     def drain(self) -> None:
-        """Wait until every submitted request has finished."""
+        """Wait until every submitted request's future is settled (its
+        result or error set, its statistics recorded)."""
         with self.cv:
-            while self.queue or self.in_flight:
+            while self.outstanding:
                 self.cv.wait(0.01)
 
     def stats(self) -> dict:
@@ -133,7 +144,7 @@ class Server:
                 "mean_ms": (1e3 * sum(lat) / n) if n else None,
                 "entries": self.entries, "span_s": span,
                 "entries_per_s": (self.entries / span) if span else None,
-                "req_per_s": (n / span) if span else None}
+                "req_per_s": (n / span) if span else None, "oom_retries": self.oom_retries}
 
     def _device_room(self) -> int:
         torch = self.torch
@@ -147,6 +158,16 @@ class Server:
             self.cv.notify_all()
 
     # -------------------------------------------------------- dispatcher
+    def _launch(self, pend, st):
+        """Launch one request; on an allocator out-of-memory, return the
+        cached free blocks to the device and try once more."""
+        torch = self.torch
+        try:
+            pend.launch(st)
+        except torch.OutOfMemoryError:
+            torch.cuda.empty_cache()
+            pend.launch(st)
+
     def _loop(self):
         torch = self.torch
         torch.cuda.set_device(self.device)
@@ -155,7 +176,7 @@ class Server:
                 if not self.running and not self.queue and not self.in_flight:
                     return
                 admit = []
-                while self.queue and self.free_streams:
+                while self.queue and self.free_streams and not self.oom_wait:
                     pend, fut, t0 = self.queue[0]
                     need = pend.device_bytes
                     n_now = len(self.in_flight) + len(admit)
@@ -178,19 +199,37 @@ class Server:
                     admit.append((pend, fut, t0, self.free_streams.pop()))
                     self.peak_bytes = max(self.peak_bytes, self.in_flight_bytes)
                     self.peak_in_flight = max(self.peak_in_flight, len(self.in_flight) + len(admit))
+            requeue = []
             for pend, fut, t0, si in admit:
                 st = self.streams[si]
                 try:
-                    pend.launch(st)
+                    self._launch(pend, st)
                     ev = torch.cuda.Event()
                     ev.record(st)
                     with self.cv:
                         self.in_flight.append((pend, fut, si, ev, t0))
+                except torch.OutOfMemoryError as e:
+                    # the byte budget admitted it, but the allocator's free
+                    # blocks (fragmented across sizes and streams) do not
+                    # hold it: with work in flight, wait for a completion
+                    # and try again; with none, report it
+                    with self.cv:
+                        self.in_flight_bytes -= pend.device_bytes
+                        self.free_streams.append(si)
+                        if self.in_flight:
+                            requeue.append((pend, fut, t0))
+                            self.oom_wait = True
+                            self.oom_retries += 1
+                            continue
+                    fut.set_exception(e)
                 except Exception as e:  # noqa: BLE001 - reported through the future
                     with self.cv:
                         self.in_flight_bytes -= pend.device_bytes
                         self.free_streams.append(si)
                     fut.set_exception(e)
+            if requeue:
+                with self.cv:
+                    self.queue.extendleft(reversed(requeue))
             done = []
             with self.cv:
                 for item in list(self.in_flight):
@@ -221,6 +260,7 @@ class Server:
                 with self.cv:
                     self.in_flight_bytes -= need
                     self.free_streams.append(si)
+                    self.oom_wait = False
                     self.cv.notify_all()
             idle = not admit and not done
             # drop this pass's references, so that a result lives only as long

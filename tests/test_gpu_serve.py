@@ -109,3 +109,53 @@ def _settles(srv, want, seconds=5.0):
             return True
         time.sleep(0.01)
     return False
+
+
+@pytest.mark.parametrize("fails", [1, 10**9])
+def test_allocator_out_of_memory(cuda, monkeypatch, fails):
+    """A launch that the byte budget admitted but the caching allocator
+    cannot place (its free blocks fragmented across sizes and streams) is
+    retried once after the cache is returned to the device, and requeued
+    while other requests are in flight; a request that never fits is
+    reported through its future once nothing else is in flight, and every
+    other request completes unchanged.  The failures are made on the host:
+    the first `fails` launches of the second request to start raise the
+    allocator's out-of-memory error."""
+    import torch
+    from mhs_b200 import matrices, serve
+    reqs = _requests(torch, cuda)
+    alone = [fn(*a, **k) for fn, a, k in reqs]
+    torch.cuda.synchronize()
+    real = matrices.Pending.launch
+    calls = {}       # launch attempts per request, by order of first launch
+
+    def flaky(self, st):
+        # tagged on the object: finished requests are freed, so ids recur
+        if not hasattr(self, "_first_launch"):
+            self._first_launch = len(calls)
+        calls[self._first_launch] = calls.get(self._first_launch, 0) + 1
+        if self._first_launch == 1 and calls[1] <= fails:
+            raise torch.OutOfMemoryError("CUDA out of memory (made by the test)")
+        return real(self, st)
+
+    monkeypatch.setattr(matrices.Pending, "launch", flaky)
+    got = []
+    with serve.Server(cuda, slots=4) as srv:
+        futs = [srv.submit(fn, *a, **k) for fn, a, k in reqs]
+        for f in futs:
+            try:
+                got.append(f.result(timeout=300))
+            except torch.OutOfMemoryError:
+                got.append(None)
+        st = srv.stats()
+    failed = [i for i, g in enumerate(got) if g is None]
+    assert len(calls) == len(reqs)
+    if fails == 1:
+        assert not failed and calls[1] == 2                # the retry after emptying the cache
+    else:
+        assert len(failed) == 1                            # only the request that never fits
+    assert all(n == 1 for k, n in calls.items() if k != 1)
+    for i, (r_alone, r_mix) in enumerate(zip(alone, got)):
+        if i not in failed:
+            assert torch.equal(r_alone, r_mix)
+    assert st["requests"] == len(reqs) - len(failed)
