@@ -366,8 +366,12 @@ MHS_FI void near_signature_f(const Frame& f, double px, double py, double eps, i
 // panel (grid-stride over the wave's panels): each lane takes angular nodes
 // j (one sincos each) and writes the panel's six radial nodes at j, in the
 // grid's order ir * n_ang + j.
+// Three blocks of 256 per SM (80 registers, a few spills): 1.7 ms less per
+// config-2 step than two at 128 registers; the kernel is latency-bound.
+constexpr int NODES_MIN_BLOCKS = 3;
+
 template <int P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, NODES_MIN_BLOCKS)
 k_nodes(double near_l, int np, int64_t lo, const double* __restrict__ obs,
         const SrcPrep* __restrict__ prep, const int* __restrict__ st_src,
         const int* __restrict__ pair_st, const int* __restrict__ pair_oc,
